@@ -1,0 +1,415 @@
+"""ferray_b200 -- B200-native GEMM backend for ferray's matmul path.
+
+Python mirror of ferray-linalg's GEMM interface over the C ABI of
+libferray_b200.so (include/ferray_gpu.h).  Names, argument meaning and error
+behaviour follow the reference:
+
+* ``gemm_f64 / gemm_f32 / gemm_c64 / gemm_c32 / gemm_i8 / gemm_i8_signed /
+  gemm_i16 / quantized_matmul`` keep the signatures of
+  ferray-linalg/src/gemm/mod.rs (m, n, k, scalars, a, b, c[, accumulate]) and
+  return ``True`` like the reference's ``-> bool`` entry points; ``False``
+  means "no kernel for this case" (FG_ERR_UNSUPPORTED).
+* ``matmul`` follows ferray_linalg::matmul (products/mod.rs:362-437) and
+  ``matmul_complex`` (complex.rs:136-264): shape errors raise
+  ``ShapeMismatch``, batch-broadcast errors ``BroadcastFailure`` -- the
+  FerrayError variants of ferray-core/src/error.rs:16-99.
+
+Operands may be host numpy arrays (staged through the device, like the
+reference's slice API) or ``DeviceArray`` objects that stay resident in HBM.
+Every call runs on the GPU; there is no CPU fallback.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+
+__all__ = [
+    "FerrayError", "ShapeMismatch", "BroadcastFailure", "InvalidDtype", "InvalidValue",
+    "OutOfMemory", "BudgetExceeded", "DeviceTimeout", "DeviceError", "Context", "DeviceArray",
+    "default_context", "gemm_f64", "gemm_f32", "gemm_c64", "gemm_c32", "gemm_i8",
+    "gemm_i8_signed", "gemm_i16", "quantized_matmul", "matmul", "matmul_complex",
+    "gemm_batched_strided", "gemm_grouped", "GroupedPlan", "launch_count", "PLAIN", "SPLIT",
+]
+
+PLAIN, SPLIT = "plain", "split"
+
+
+class FerrayError(Exception):
+    """Base class, mirrors ferray_core::FerrayError."""
+
+
+class ShapeMismatch(FerrayError):
+    pass
+
+
+class BroadcastFailure(FerrayError):
+    pass
+
+
+class InvalidDtype(FerrayError):
+    pass
+
+
+class InvalidValue(FerrayError):
+    pass
+
+
+class OutOfMemory(FerrayError):
+    pass
+
+
+class BudgetExceeded(FerrayError):
+    pass
+
+
+class DeviceTimeout(FerrayError):
+    pass
+
+
+class DeviceError(FerrayError):
+    pass
+
+
+_STATUS_EXC = {
+    L.FG_ERR_SHAPE: ShapeMismatch,
+    L.FG_ERR_DTYPE: InvalidDtype,
+    L.FG_ERR_OOM: OutOfMemory,
+    L.FG_ERR_BUDGET: BudgetExceeded,
+    L.FG_ERR_TIMEOUT: DeviceTimeout,
+    L.FG_ERR_DEVICE: DeviceError,
+    L.FG_ERR_INVALID: InvalidValue,
+    L.FG_ERR_BROADCAST: BroadcastFailure,
+}
+
+
+class Unsupported(FerrayError):
+    pass
+
+
+def check(status, what=""):
+    if status == L.FG_OK:
+        return
+    lib = L.load()
+    msg = lib.fg_last_error().decode() or lib.fg_status_string(status).decode()
+    exc = _STATUS_EXC.get(status, Unsupported)
+    raise exc(f"{what}: {msg}" if what else msg)
+
+
+def launch_count():
+    """Kernels launched by libferray_b200.so in this process."""
+    return int(L.load().fg_launch_count())
+
+
+class Context:
+    """A device context (one per GPU); thread-safe."""
+
+    def __init__(self, device=0):
+        self._lib = L.load()
+        h = C.c_void_p()
+        check(self._lib.fg_init(device, C.byref(h)), "fg_init")
+        self.handle = h
+        self.device = device
+
+    def sync(self, stream=None):
+        check(self._lib.fg_sync(self.handle, stream), "fg_sync")
+
+    def info(self):
+        sm, ma, mi, hbm = C.c_int(), C.c_int(), C.c_int(), C.c_size_t()
+        check(self._lib.fg_device_info(self.handle, C.byref(sm), C.byref(ma), C.byref(mi),
+                                       C.byref(hbm)))
+        return {"sm_count": sm.value, "cc": (ma.value, mi.value), "hbm_bytes": hbm.value}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.fg_shutdown(self.handle)
+            self.handle = None
+
+
+_default = None
+
+
+def default_context():
+    global _default
+    if _default is None:
+        _default = Context(0)
+    return _default
+
+
+_NP2FG = {np.dtype(np.float64): L.FG_F64, np.dtype(np.float32): L.FG_F32,
+          np.dtype(np.complex128): L.FG_C64, np.dtype(np.complex64): L.FG_C32,
+          np.dtype(np.int8): L.FG_I8, np.dtype(np.int16): L.FG_I16}
+_OUT_DTYPE = {L.FG_F64: np.float64, L.FG_F32: np.float32, L.FG_C64: np.complex128,
+              L.FG_C32: np.complex64, L.FG_I8: np.int32, L.FG_U8I8: np.int32,
+              L.FG_I16: np.int32}
+
+
+def _mode(mode):
+    if mode in (PLAIN, L.FG_MODE_PLAIN, None):
+        return L.FG_MODE_PLAIN
+    if mode in (SPLIT, L.FG_MODE_SPLIT):
+        return L.FG_MODE_SPLIT
+    raise InvalidValue(f"unknown mode {mode!r}")
+
+
+class DeviceArray:
+    """Row-major array resident in HBM (the device counterpart of
+    ferray_core::Array, ferray-core/src/array/owned.rs:21)."""
+
+    def __init__(self, shape, dtype, ctx=None):
+        self.ctx = ctx or default_context()
+        self.shape = tuple(int(s) for s in shape)
+        self.dtype = np.dtype(dtype)
+        self.nbytes = int(np.prod(self.shape, dtype=np.int64)) * self.dtype.itemsize
+        p = C.c_void_p()
+        check(self.ctx._lib.fg_buffer_alloc(self.ctx.handle, max(self.nbytes, 1), C.byref(p)),
+              "fg_buffer_alloc")
+        self.ptr = p.value
+
+    @classmethod
+    def from_numpy(cls, x, ctx=None):
+        x = np.ascontiguousarray(x)
+        d = cls(x.shape, x.dtype, ctx)
+        check(d.ctx._lib.fg_upload(d.ctx.handle, d.ptr, x.ctypes.data, x.nbytes, None), "upload")
+        d.ctx.sync()
+        return d
+
+    def to_numpy(self):
+        out = np.empty(self.shape, self.dtype)
+        check(self.ctx._lib.fg_download(self.ctx.handle, out.ctypes.data, self.ptr, self.nbytes,
+                                        None), "download")
+        return out
+
+    @property
+    def ndim(self):
+        return len(self.shape)
+
+    def free(self):
+        if self.ptr:
+            self.ctx._lib.fg_buffer_free(self.ctx.handle, self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def _is_dev(x):
+    return isinstance(x, DeviceArray)
+
+
+def _host(x, dtype):
+    return np.ascontiguousarray(x, dtype=dtype)
+
+
+def _run_gemm(dtype, mode, slices, m, n, k, alpha, a, b, beta, c, accumulate, scalar_t):
+    """Shared body of the gemm_* mirrors: device arrays go through the
+    device entry point, host arrays through the staging entry point."""
+    ctx = default_context()
+    lib = ctx._lib
+    al = (scalar_t * len(alpha))(*alpha)
+    be = (scalar_t * len(beta))(*beta)
+    if _is_dev(a) or _is_dev(b) or _is_dev(c):
+        if not (_is_dev(a) and _is_dev(b) and _is_dev(c)):
+            raise InvalidValue("mix of device and host operands")
+        st = lib.fg_gemm(ctx.handle, dtype, _mode(mode), slices, m, n, k, al, a.ptr, k, b.ptr,
+                         n, be, c.ptr, n, int(bool(accumulate)), None)
+        if st == L.FG_ERR_UNSUPPORTED:
+            return False
+        check(st, "gemm")
+        ctx.sync()
+        return True
+    st = lib.fg_gemm_host(ctx.handle, dtype, _mode(mode), slices, m, n, k, al,
+                          a.ctypes.data, b.ctypes.data, be, c.ctypes.data, int(bool(accumulate)))
+    if st == L.FG_ERR_UNSUPPORTED:
+        return False
+    check(st, "gemm")
+    return True
+
+
+def _need(x, count, dtype, name):
+    if _is_dev(x):
+        if x.dtype != np.dtype(dtype):
+            raise InvalidDtype(f"{name}: expected {np.dtype(dtype)}, got {x.dtype}")
+        if x.nbytes < count * np.dtype(dtype).itemsize:
+            raise ShapeMismatch(f"{name}: buffer holds fewer than {count} elements")
+        return x
+    if not isinstance(x, np.ndarray) or x.dtype != np.dtype(dtype) or not x.flags.c_contiguous:
+        raise InvalidDtype(f"{name}: expected a C-contiguous {np.dtype(dtype)} array")
+    if x.size < count:
+        raise ShapeMismatch(f"{name}: fewer than {count} elements")
+    return x
+
+
+def gemm_f64(m, n, k, alpha, a, b, beta, c, mode=PLAIN, ozaki_slices=0):
+    """C = alpha*A@B + beta*C (gemm/mod.rs:197).  mode='split': Ozaki INT8."""
+    _need(a, m * k, np.float64, "a"); _need(b, k * n, np.float64, "b")
+    _need(c, m * n, np.float64, "c")
+    return _run_gemm(L.FG_F64, mode, ozaki_slices, m, n, k, [alpha], a, b, [beta], c, 0,
+                     C.c_double)
+
+
+def gemm_f32(m, n, k, alpha, a, b, beta, c, mode=PLAIN):
+    """C = alpha*A@B + beta*C (gemm/mod.rs:940).  mode='split': 3xBF16."""
+    _need(a, m * k, np.float32, "a"); _need(b, k * n, np.float32, "b")
+    _need(c, m * n, np.float32, "c")
+    return _run_gemm(L.FG_F32, mode, 0, m, n, k, [alpha], a, b, [beta], c, 0, C.c_float)
+
+
+def gemm_c64(m, n, k, alpha_re, alpha_im, a, b, beta_re, beta_im, c, mode=PLAIN,
+             ozaki_slices=0):
+    """Complex<f64> GEMM (gemm/mod.rs:757); a, b, c complex128."""
+    _need(a, m * k, np.complex128, "a"); _need(b, k * n, np.complex128, "b")
+    _need(c, m * n, np.complex128, "c")
+    return _run_gemm(L.FG_C64, mode, ozaki_slices, m, n, k, [alpha_re, alpha_im], a, b,
+                     [beta_re, beta_im], c, 0, C.c_double)
+
+
+def gemm_c32(m, n, k, alpha_re, alpha_im, a, b, beta_re, beta_im, c, mode=PLAIN):
+    """Complex<f32> GEMM (gemm/mod.rs:669); a, b, c complex64."""
+    _need(a, m * k, np.complex64, "a"); _need(b, k * n, np.complex64, "b")
+    _need(c, m * n, np.complex64, "c")
+    return _run_gemm(L.FG_C32, mode, 0, m, n, k, [alpha_re, alpha_im], a, b,
+                     [beta_re, beta_im], c, 0, C.c_float)
+
+
+def gemm_i8_signed(m, n, k, a, b, c, accumulate=False):
+    """i8 x i8 -> i32, wrapping (gemm/mod.rs:414)."""
+    _need(a, m * k, np.int8, "a"); _need(b, k * n, np.int8, "b"); _need(c, m * n, np.int32, "c")
+    return _run_gemm(L.FG_I8, PLAIN, 0, m, n, k, [0.0], a, b, [0.0], c, accumulate, C.c_double)
+
+
+def gemm_i8(m, n, k, a, b, c, accumulate=False):
+    """u8 x i8 -> i32, exact (gemm/mod.rs:601, VNNI semantics)."""
+    _need(a, m * k, np.uint8, "a"); _need(b, k * n, np.int8, "b"); _need(c, m * n, np.int32, "c")
+    return _run_gemm(L.FG_U8I8, PLAIN, 0, m, n, k, [0.0], a, b, [0.0], c, accumulate,
+                     C.c_double)
+
+
+def gemm_i16(m, n, k, a, b, c, accumulate=False):
+    """i16 x i16 -> i32, wrapping (gemm/mod.rs:348)."""
+    _need(a, m * k, np.int16, "a"); _need(b, k * n, np.int16, "b"); _need(c, m * n, np.int32, "c")
+    return _run_gemm(L.FG_I16, PLAIN, 0, m, n, k, [0.0], a, b, [0.0], c, accumulate,
+                     C.c_double)
+
+
+def quantized_matmul(m, n, k, a, a_zp, scale_a, b, b_zp, scale_b, c, accumulate=False):
+    """scale_a*scale_b*sum((a-a_zp)(b-b_zp)) -> f32 (gemm/mod.rs:484)."""
+    _need(a, m * k, np.uint8, "a"); _need(b, k * n, np.int8, "b"); _need(c, m * n, np.float32, "c")
+    ctx = default_context()
+    lib = ctx._lib
+    devs = [_is_dev(x) for x in (a, b, c)]
+    if any(devs) and not all(devs):
+        raise InvalidValue("mix of device and host operands")
+    if all(devs):
+        check(lib.fg_quantized_matmul(ctx.handle, m, n, k, a.ptr, a_zp, scale_a, b.ptr, b_zp,
+                                      scale_b, c.ptr, int(bool(accumulate)), None), "qmm")
+        ctx.sync()
+        return True
+    da, db, dc = (DeviceArray.from_numpy(x) for x in (a, b, c))
+    check(lib.fg_quantized_matmul(ctx.handle, m, n, k, da.ptr, a_zp, scale_a, db.ptr, b_zp,
+                                  scale_b, dc.ptr, int(bool(accumulate)), None), "qmm")
+    ctx.sync()
+    c[...] = dc.to_numpy().reshape(c.shape)
+    return True
+
+
+def matmul(a, b, mode=PLAIN):
+    """NumPy ``@`` on the GPU (products/mod.rs:362 / complex.rs:136).
+
+    a, b: numpy arrays or DeviceArrays of the same dtype (f64, f32, complex128,
+    complex64, int8 -> int32, int16 -> int32).  Returns the same kind.
+    """
+    ctx = default_context()
+    lib = ctx._lib
+    dev = _is_dev(a)
+    if dev != _is_dev(b):
+        raise InvalidValue("mix of device and host operands")
+    if np.dtype(a.dtype) != np.dtype(b.dtype):
+        raise InvalidDtype(f"matmul: dtypes differ ({a.dtype} vs {b.dtype})")
+    dt = _NP2FG.get(np.dtype(a.dtype))
+    if dt is None:
+        raise InvalidDtype(f"matmul: unsupported dtype {a.dtype}")
+    sa = (C.c_int64 * max(len(a.shape), 1))(*a.shape)
+    sb = (C.c_int64 * max(len(b.shape), 1))(*b.shape)
+    os_ = (C.c_int64 * 8)()
+    ond = C.c_int()
+    check(lib.fg_matmul(ctx.handle, dt, _mode(mode), None, len(a.shape), sa, None, len(b.shape),
+                        sb, None, os_, C.byref(ond), None), "matmul")
+    out_shape = tuple(os_[i] for i in range(ond.value))
+    if dev:
+        da, db = a, b
+    else:
+        da, db = DeviceArray.from_numpy(a), DeviceArray.from_numpy(b)
+    dc = DeviceArray(out_shape, _OUT_DTYPE[dt])
+    check(lib.fg_matmul(ctx.handle, dt, _mode(mode), da.ptr, len(a.shape), sa, db.ptr,
+                        len(b.shape), sb, dc.ptr, os_, C.byref(ond), None), "matmul")
+    ctx.sync()
+    return dc if dev else dc.to_numpy()
+
+
+def matmul_complex(a, b, mode=PLAIN):
+    """Complex 2-D matmul (complex.rs:136)."""
+    if not np.issubdtype(np.dtype(a.dtype), np.complexfloating):
+        raise InvalidDtype("matmul_complex: complex operands expected")
+    return matmul(a, b, mode)
+
+
+def gemm_batched_strided(dtype, batch, m, n, k, a, stride_a, b, stride_b, c, stride_c,
+                         alpha=1.0, beta=0.0, mode=PLAIN, accumulate=False):
+    """Stacked GEMM on DeviceArrays; stride 0 broadcasts an operand."""
+    ctx = default_context()
+    dt = _NP2FG[np.dtype(dtype)] if not isinstance(dtype, int) else dtype
+    cplx = dt in (L.FG_C64, L.FG_C32)
+    st_t = C.c_float if dt in (L.FG_F32, L.FG_C32) else C.c_double
+    al = (st_t * 2)(complex(alpha).real, complex(alpha).imag) if cplx else (st_t * 1)(alpha)
+    be = (st_t * 2)(complex(beta).real, complex(beta).imag) if cplx else (st_t * 1)(beta)
+    check(ctx._lib.fg_gemm_batched_strided(ctx.handle, dt, _mode(mode), 0, batch, m, n, k, al,
+                                           a.ptr, k, stride_a, b.ptr, n, stride_b, be, c.ptr, n,
+                                           stride_c, int(bool(accumulate)), None), "batched")
+    ctx.sync()
+
+
+def _table(problems):
+    tab = (L.fg_problem * len(problems))()
+    for i, p in enumerate(problems):
+        m, n, k, a, b, c = p[:6]
+        tab[i] = L.fg_problem(m, n, k, a.ptr if _is_dev(a) else a, b.ptr if _is_dev(b) else b,
+                              c.ptr if _is_dev(c) else c, k, n, n)
+    return tab
+
+
+def gemm_grouped(problems, dtype=np.float32, mode=PLAIN):
+    """One persistent grouped launch over ragged problems
+    [(m, n, k, A, B, C), ...] (DeviceArrays or raw device pointers)."""
+    ctx = default_context()
+    dt = L.FG_I8 if np.dtype(dtype) == np.int8 else L.FG_F32
+    tab = _table(problems)
+    check(ctx._lib.fg_gemm_grouped(ctx.handle, dt, _mode(mode), tab, len(problems), None),
+          "grouped")
+    ctx.sync()
+
+
+class GroupedPlan:
+    """Prepared grouped batch replayed from a CUDA graph."""
+
+    def __init__(self, problems, dtype=np.float32, mode=PLAIN):
+        self.ctx = default_context()
+        dt = L.FG_I8 if np.dtype(dtype) == np.int8 else L.FG_F32
+        self._tab = _table(problems)
+        h = C.c_void_p()
+        check(self.ctx._lib.fg_grouped_plan_create(self.ctx.handle, dt, _mode(mode), self._tab,
+                                                   len(problems), None, C.byref(h)), "plan")
+        self.handle = h
+
+    def run(self, sync=True):
+        check(self.ctx._lib.fg_grouped_plan_run(self.handle, None), "plan run")
+        if sync:
+            self.ctx.sync()
+
+    def close(self):
+        if self.handle:
+            self.ctx._lib.fg_grouped_plan_destroy(self.handle)
+            self.handle = None

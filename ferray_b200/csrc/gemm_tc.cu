@@ -1,0 +1,331 @@
+// gemm_tc.cu -- host launchers of the tcgen05 GEMM family:
+//   * i8 x i8 and u8 x i8 -> i32 (exact, wrapping)            [kind::i8]
+//   * i16 x i16 -> i32 as 4 byte-slice products, recombined    [kind::i8]
+//   * quantized u8 x i8 -> f32 with the zero-point correction
+//     fused into the epilogue                                  [kind::i8]
+//   * 3xBF16 SGEMM / CGEMM (split mode)                        [kind::f16]
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "prep_kernels.cuh"
+#include "runtime.h"
+#include "tc_gemm.cuh"
+
+namespace fgrt {
+
+using namespace fg;
+
+using CfgI8 = TcCfg<KIND_I8, 256, 4, 1, 1, 1, 1, EPI_I32>;
+using CfgQmm = TcCfg<KIND_I8, 256, 4, 1, 1, 1, 1, EPI_QMM>;
+using CfgI16 = TcCfg<KIND_I8, 128, 3, 2, 2, 3, 4, EPI_I16>;
+using CfgBf16x3 = TcCfg<KIND_BF16, 256, 2, 2, 2, 1, 3, EPI_F32>;
+
+static unsigned long long kTimeoutNs = 4000000000ull;  // 4 s per wait
+
+template <class Cfg>
+static fg_status launch_cfg(fg_ctx* ctx, const TcMaps& maps, TcArgs& args, cudaStream_t st) {
+    static std::once_flag once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(once, [] {
+        attr_err = cudaFuncSetAttribute(tc_gemm_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(tc_smem_bytes<Cfg>()));
+    });
+    FG_CUDA(attr_err);
+    args.status = ctx->d_status;
+    args.timeout_ns = kTimeoutNs;
+    const long long tiles = (long long)args.batch * args.tiles_m * args.tiles_n;
+    if (tiles == 0) return FG_OK;
+    const int grid = static_cast<int>(std::min<long long>(tiles, ctx->sm_count));
+    tc_gemm_kernel<Cfg><<<grid, Cfg::THREADS, tc_smem_bytes<Cfg>(), st>>>(maps, args);
+    count_launch();
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+// Operand map for a row-major matrix stack: inner = contiguous extent,
+// rows = outer extent, `count` matrices `mstride_bytes` apart.
+static fg_status operand_map(CUtensorMap* map, CUtensorMapDataType dt, const void* base,
+                             long long inner, long long rows, long long ld_bytes, long long count,
+                             long long mstride_bytes, uint32_t box_inner, uint32_t box_rows,
+                             int* rank3) {
+    uint64_t dims[3] = {static_cast<uint64_t>(inner), static_cast<uint64_t>(rows),
+                        static_cast<uint64_t>(count)};
+    uint64_t strides[2] = {static_cast<uint64_t>(ld_bytes), static_cast<uint64_t>(mstride_bytes)};
+    uint32_t box[3] = {box_inner, box_rows, 1};
+    *rank3 = count > 1 ? 1 : 0;
+    return encode_map(map, dt, count > 1 ? 3 : 2, base, dims, strides, box);
+}
+
+static bool tma_ok(const void* p, long long ld_bytes, long long count, long long mstride_bytes) {
+    if (reinterpret_cast<uintptr_t>(p) & 15) return false;
+    if (ld_bytes % 16) return false;
+    if (count > 1 && (mstride_bytes % 16)) return false;
+    return true;
+}
+
+static long long round_up(long long x, long long a) { return (x + a - 1) / a * a; }
+
+static void fill_batch(const Gemm& g, TcArgs& a) {
+    a.batch = g.batch;
+    a.bdims = g.bdims;
+    for (int d = 0; d < 4; ++d) {
+        a.bshape[d] = g.bshape[d];
+        a.a_bstride[d] = g.a_istride[d];
+        a.b_bstride[d] = g.b_istride[d];
+    }
+    a.strideC = g.c_stride;
+}
+
+static int grid_for(long long total) {
+    return static_cast<int>(std::min<long long>(std::max<long long>((total + 255) / 256, 1), 4096));
+}
+
+// Copies an operand stack of 1-byte (or `esize`) rows into a 16-byte-pitched
+// scratch buffer when its pointer/strides break the TMA rules.
+static fg_status make_tma_operand(const void* src, long long rows, long long cols, long long ld,
+                                  long long count, long long mstride, int esize, Scratch& sc,
+                                  const void** out, long long* out_ld, long long* out_mstride,
+                                  cudaStream_t st) {
+    const long long ld_b = ld * esize, ms_b = mstride * esize;
+    if (tma_ok(src, ld_b, count, ms_b)) {
+        *out = src;
+        *out_ld = ld;
+        *out_mstride = mstride;
+        return FG_OK;
+    }
+    const long long pitch = round_up(cols * esize, 16);
+    FG_TRY(sc.alloc(static_cast<size_t>(pitch * rows * count), st));
+    dim3 grid(grid_for(rows * cols * esize), static_cast<unsigned>(count));
+    pad_rows_kernel<<<grid, 256, 0, st>>>(static_cast<const uint8_t*>(src), rows, cols * esize, ld_b,
+                                          static_cast<uint8_t*>(sc.p), pitch, ms_b, pitch * rows);
+    count_launch();
+    FG_CUDA(cudaGetLastError());
+    *out = sc.p;
+    *out_ld = pitch / esize;
+    *out_mstride = pitch * rows / esize;
+    return FG_OK;
+}
+
+// Largest K one launch may cover with exact int32 accumulation.
+static long long max_k_chunk(fg_dtype d) {
+    switch (d) {
+        case FG_I8: return 131072;   // |a*b| <= 2^14
+        case FG_U8I8: return 65536;  // |a*b| <= 255*128
+        case FG_I16: return 32768;   // byte-slice products <= 255^2 (two per mid term)
+        default: return 1LL << 40;
+    }
+}
+
+fg_status launch_int_tc(fg_ctx* ctx, const Gemm& g0, cudaStream_t st) {
+    const long long kchunk = max_k_chunk(g0.dtype);
+    if (g0.K > kchunk) {
+        // Split K; later chunks accumulate into C (wrapping, so exact mod 2^32).
+        for (long long k0 = 0; k0 < g0.K; k0 += kchunk) {
+            Gemm g = g0;
+            g.K = std::min(kchunk, g0.K - k0);
+            g.A = static_cast<const uint8_t*>(g0.A) + k0 * in_size(g0.dtype);
+            g.B = static_cast<const uint8_t*>(g0.B) + k0 * g0.ldb * in_size(g0.dtype);
+            g.accumulate = (k0 == 0) ? g0.accumulate : 1;
+            FG_TRY(launch_int_tc(ctx, g, st));
+        }
+        return FG_OK;
+    }
+    const Gemm& g = g0;
+    TcMaps maps;
+    TcArgs args{};
+    args.M = static_cast<int>(g.M);
+    args.N = static_cast<int>(g.N);
+    args.K = static_cast<int>(g.K);
+    args.tiles_m = static_cast<int>((g.M + 127) / 128);
+    args.C = g.C;
+    args.ldc = g.ldc;
+    args.accumulate = g.accumulate;
+    fill_batch(g, args);
+
+    if (g.dtype == FG_I8 || g.dtype == FG_U8I8) {
+        Scratch sa, sb;
+        const void *pa, *pb;
+        long long lda, ldb, msa, msb;
+        FG_TRY(make_tma_operand(g.A, g.M, g.K, g.lda, g.a_count, g.a_mstride, 1, sa, &pa, &lda, &msa, st));
+        FG_TRY(make_tma_operand(g.B, g.K, g.N, g.ldb, g.b_count, g.b_mstride, 1, sb, &pb, &ldb, &msb, st));
+        FG_TRY(operand_map(&maps.a[0], CU_TENSOR_MAP_DATA_TYPE_UINT8, pa, g.K, g.M, lda, g.a_count, msa,
+                           128, 128, &args.a_rank3));
+        FG_TRY(operand_map(&maps.b[0], CU_TENSOR_MAP_DATA_TYPE_UINT8, pb, g.N, g.K, ldb, g.b_count, msb,
+                           128, 128, &args.b_rank3));
+        args.tiles_n = static_cast<int>((g.N + CfgI8::BN - 1) / CfgI8::BN);
+        args.k_blocks = static_cast<int>((g.K + CfgI8::BK - 1) / CfgI8::BK);
+        args.ops[0] = TcOp{0, 0, 0, g.dtype == FG_I8 ? 1 : 0, 1};
+        return launch_cfg<CfgI8>(ctx, maps, args, st);
+    }
+    if (g.dtype == FG_I16) {
+        // Byte slices, rows padded to 16 bytes.
+        const long long pa = round_up(g.K, 16), pb = round_up(g.N, 16);
+        const size_t a_bytes = static_cast<size_t>(pa * g.M * g.a_count);
+        const size_t b_bytes = static_cast<size_t>(pb * g.K * g.b_count);
+        Scratch s;
+        FG_TRY(s.alloc(2 * a_bytes + 2 * b_bytes, st));
+        int8_t* ahi = static_cast<int8_t*>(s.p);
+        uint8_t* alo = reinterpret_cast<uint8_t*>(ahi + a_bytes);
+        int8_t* bhi = reinterpret_cast<int8_t*>(alo + a_bytes);
+        uint8_t* blo = reinterpret_cast<uint8_t*>(bhi + b_bytes);
+        if (g.M * g.K > 0) {
+            split_i16_kernel<<<dim3(grid_for(g.M * g.K), static_cast<unsigned>(g.a_count)), 256, 0, st>>>(
+                static_cast<const int16_t*>(g.A), g.M, g.K, g.lda, ahi, alo, pa, g.a_mstride, pa * g.M);
+            count_launch();
+        }
+        if (g.K * g.N > 0) {
+            split_i16_kernel<<<dim3(grid_for(g.K * g.N), static_cast<unsigned>(g.b_count)), 256, 0, st>>>(
+                static_cast<const int16_t*>(g.B), g.K, g.N, g.ldb, bhi, blo, pb, g.b_mstride, pb * g.K);
+            count_launch();
+        }
+        FG_CUDA(cudaGetLastError());
+        int r3;
+        FG_TRY(operand_map(&maps.a[0], CU_TENSOR_MAP_DATA_TYPE_UINT8, ahi, g.K, g.M, pa, g.a_count, pa * g.M, 128, 128, &args.a_rank3));
+        FG_TRY(operand_map(&maps.a[1], CU_TENSOR_MAP_DATA_TYPE_UINT8, alo, g.K, g.M, pa, g.a_count, pa * g.M, 128, 128, &r3));
+        FG_TRY(operand_map(&maps.b[0], CU_TENSOR_MAP_DATA_TYPE_UINT8, bhi, g.N, g.K, pb, g.b_count, pb * g.K, 128, 128, &args.b_rank3));
+        FG_TRY(operand_map(&maps.b[1], CU_TENSOR_MAP_DATA_TYPE_UINT8, blo, g.N, g.K, pb, g.b_count, pb * g.K, 128, 128, &r3));
+        args.tiles_n = static_cast<int>((g.N + CfgI16::BN - 1) / CfgI16::BN);
+        args.k_blocks = static_cast<int>((g.K + CfgI16::BK - 1) / CfgI16::BK);
+        args.ops[0] = TcOp{0, 0, 0, 1, 1};  // hi*hi        -> acc0 (<<16)
+        args.ops[1] = TcOp{0, 1, 1, 1, 0};  // hi(s8)*lo(u8) -> acc1 (<<8)
+        args.ops[2] = TcOp{1, 0, 1, 0, 1};  // lo(u8)*hi(s8) -> acc1
+        args.ops[3] = TcOp{1, 1, 2, 0, 0};  // lo*lo (u8)    -> acc2
+        return launch_cfg<CfgI16>(ctx, maps, args, st);
+    }
+    return set_error(FG_ERR_DTYPE, "integer tensor-core path: unsupported dtype");
+}
+
+fg_status launch_qmm(fg_ctx* ctx, long long M, long long N, long long K, const uint8_t* a,
+                     int a_zp, float scale, const int8_t* b, int b_zp, float* c, int accumulate,
+                     cudaStream_t st) {
+    if (K > max_k_chunk(FG_U8I8))
+        return set_error(FG_ERR_UNSUPPORTED, "quantized_matmul: K above 65536 would overflow the exact i32 accumulator");
+    Scratch sums;
+    FG_TRY(sums.alloc(static_cast<size_t>((M + N) * sizeof(int)), st));
+    int* row_sum = static_cast<int*>(sums.p);
+    int* col_sum = row_sum + M;
+    row_sum_u8_kernel<<<grid_for(M * 32), 256, 0, st>>>(a, M, K, K, row_sum);
+    col_sum_i8_kernel<<<grid_for(N), 256, 0, st>>>(b, K, N, N, col_sum);
+    count_launch(2);
+    FG_CUDA(cudaGetLastError());
+    Scratch sa, sb;
+    const void *pa, *pb;
+    long long lda, ldb, msa, msb;
+    FG_TRY(make_tma_operand(a, M, K, K, 1, 0, 1, sa, &pa, &lda, &msa, st));
+    FG_TRY(make_tma_operand(b, K, N, N, 1, 0, 1, sb, &pb, &ldb, &msb, st));
+    TcMaps maps;
+    TcArgs args{};
+    args.M = static_cast<int>(M);
+    args.N = static_cast<int>(N);
+    args.K = static_cast<int>(K);
+    args.tiles_m = static_cast<int>((M + 127) / 128);
+    args.tiles_n = static_cast<int>((N + CfgQmm::BN - 1) / CfgQmm::BN);
+    args.k_blocks = static_cast<int>((K + CfgQmm::BK - 1) / CfgQmm::BK);
+    args.batch = 1;
+    args.C = c;
+    args.ldc = N;
+    args.accumulate = accumulate;
+    args.row_sum = row_sum;
+    args.col_sum = col_sum;
+    args.a_zp = a_zp;
+    args.b_zp = b_zp;
+    args.scale = scale;
+    args.ops[0] = TcOp{0, 0, 0, 0, 1};
+    FG_TRY(operand_map(&maps.a[0], CU_TENSOR_MAP_DATA_TYPE_UINT8, pa, K, M, lda, 1, 0, 128, 128, &args.a_rank3));
+    FG_TRY(operand_map(&maps.b[0], CU_TENSOR_MAP_DATA_TYPE_UINT8, pb, N, K, ldb, 1, 0, 128, 128, &args.b_rank3));
+    return launch_cfg<CfgQmm>(ctx, maps, args, st);
+}
+
+// 3xBF16: C = alpha * (Alo*Bhi + Ahi*Blo + Ahi*Bhi) + beta * C, f32 accumulate.
+fg_status launch_split_bf16(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
+    const bool cplx = g.dtype == FG_C32;
+    if (cplx && g.batch > 1) {
+        // Complex batches run one embedded product per output matrix.
+        for (int i = 0; i < g.batch; ++i) {
+            Gemm s = g;
+            long long ia = 0, ib = 0;
+            int rem = i;
+            for (int d = g.bdims - 1; d >= 0; --d) {
+                int idx = rem % g.bshape[d];
+                rem /= g.bshape[d];
+                ia += idx * g.a_istride[d];
+                ib += idx * g.b_istride[d];
+            }
+            s.batch = 1;
+            s.bdims = 0;
+            s.a_count = s.b_count = 1;
+            s.A = static_cast<const float2*>(g.A) + ia * g.a_mstride;
+            s.B = static_cast<const float2*>(g.B) + ib * g.b_mstride;
+            s.C = static_cast<float2*>(g.C) + i * g.c_stride;
+            FG_TRY(launch_split_bf16(ctx, s, st));
+        }
+        return FG_OK;
+    }
+    // Real-embedded sizes for complex: (M x 2K) * (2K x 2N).
+    const long long M = g.M, K = cplx ? 2 * g.K : g.K, N = cplx ? 2 * g.N : g.N;
+    const long long pa = round_up(K, 8), pb = round_up(N, 8);  // bf16 elements, 16-byte pitch
+    const size_t a_elems = static_cast<size_t>(pa * M * g.a_count);
+    const size_t b_elems = static_cast<size_t>(pb * K * g.b_count);
+    Scratch s;
+    FG_TRY(s.alloc((2 * a_elems + 2 * b_elems) * sizeof(__nv_bfloat16), st));
+    __nv_bfloat16* ahi = static_cast<__nv_bfloat16*>(s.p);
+    __nv_bfloat16* alo = ahi + a_elems;
+    __nv_bfloat16* bhi = alo + a_elems;
+    __nv_bfloat16* blo = bhi + b_elems;
+    if (cplx) {
+        if (g.M * g.K > 0) {
+            split_bf16_cplx_a_kernel<<<grid_for(g.M * g.K), 256, 0, st>>>(
+                static_cast<const float2*>(g.A), g.M, g.K, g.lda, ahi, alo, pa);
+            count_launch();
+        }
+        if (g.K * g.N > 0) {
+            split_bf16_cplx_b_kernel<<<grid_for(g.K * g.N), 256, 0, st>>>(
+                static_cast<const float2*>(g.B), g.K, g.N, g.ldb, bhi, blo, pb);
+            count_launch();
+        }
+    } else {
+        if (M * K > 0) {
+            split_bf16_kernel<<<dim3(grid_for(M * K), static_cast<unsigned>(g.a_count)), 256, 0, st>>>(
+                static_cast<const float*>(g.A), M, K, g.lda, ahi, alo, pa, g.a_mstride, pa * M);
+            count_launch();
+        }
+        if (K * N > 0) {
+            split_bf16_kernel<<<dim3(grid_for(K * N), static_cast<unsigned>(g.b_count)), 256, 0, st>>>(
+                static_cast<const float*>(g.B), K, N, g.ldb, bhi, blo, pb, g.b_mstride, pb * K);
+            count_launch();
+        }
+    }
+    FG_CUDA(cudaGetLastError());
+    TcMaps maps;
+    TcArgs args{};
+    int r3;
+    FG_TRY(operand_map(&maps.a[0], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, ahi, K, M, pa * 2, g.a_count, pa * M * 2, 64, 128, &args.a_rank3));
+    FG_TRY(operand_map(&maps.a[1], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, alo, K, M, pa * 2, g.a_count, pa * M * 2, 64, 128, &r3));
+    FG_TRY(operand_map(&maps.b[0], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, bhi, N, K, pb * 2, g.b_count, pb * K * 2, 64, 64, &args.b_rank3));
+    FG_TRY(operand_map(&maps.b[1], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, blo, N, K, pb * 2, g.b_count, pb * K * 2, 64, 64, &r3));
+    args.M = static_cast<int>(M);
+    args.N = static_cast<int>(N);
+    args.K = static_cast<int>(K);
+    args.tiles_m = static_cast<int>((M + 127) / 128);
+    args.tiles_n = static_cast<int>((N + CfgBf16x3::BN - 1) / CfgBf16x3::BN);
+    args.k_blocks = static_cast<int>((K + CfgBf16x3::BK - 1) / CfgBf16x3::BK);
+    args.C = g.C;
+    args.ldc = g.ldc;  // complex: in complex elements -> float pitch below
+    args.alpha = static_cast<float>(g.alpha_re);
+    args.beta = static_cast<float>(g.beta_re);
+    fill_batch(g, args);
+    if (cplx) {
+        if (g.alpha_im != 0.0 || g.beta_im != 0.0)
+            return set_error(FG_ERR_UNSUPPORTED, "split CGEMM: complex alpha/beta must be real");
+        args.cplx_half = static_cast<int>(g.N);
+        args.ldc = 2 * g.ldc;
+    }
+    args.ops[0] = TcOp{1, 0, 0, 1, 1};  // lo * hi
+    args.ops[1] = TcOp{0, 1, 0, 1, 1};  // hi * lo
+    args.ops[2] = TcOp{0, 0, 0, 1, 1};  // hi * hi
+    return launch_cfg<CfgBf16x3>(ctx, maps, args, st);
+}
+
+}  // namespace fgrt

@@ -1,0 +1,153 @@
+// prep_kernels.cuh -- operand preparation passes that feed the tensor-core
+// kernels.  All are HBM-bound elementwise passes (one read, one or two
+// writes per element) with grid-stride loops.
+//
+//  * split_bf16: x -> (hi, lo) with hi = bf16(x), lo = bf16(x - hi), both
+//    round-to-nearest-even, for the 3xBF16 SGEMM (x = hi + lo + r,
+//    |r| <= 2^-17 |x|).  Optional complex real-embedding: the complex
+//    product A*B equals the real product [Ar Ai] * [[Br Bi], [-Bi Br]],
+//    whose columns are [Re C | Im C].
+//  * split_i16: x -> (hi, lo) with x = 256*hi + lo, hi signed 8-bit,
+//    lo unsigned 8-bit, for the byte-sliced i16 GEMM.
+//  * pad_rows: copies a row-major byte matrix into a buffer whose row pitch
+//    is a multiple of 16 bytes (TMA stride rule).
+//  * row/column sums for the quantized GEMM's zero-point correction.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace fg {
+
+__device__ __forceinline__ void split_one(float x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+    hi = __float2bfloat16_rn(x);
+    lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+}
+
+// Real operand: X (rows x cols, pitch ldx) -> hi/lo (pitch ldo).
+static __global__ void split_bf16_kernel(const float* __restrict__ X, long long rows, long long cols,
+                                  long long ldx, __nv_bfloat16* __restrict__ hi,
+                                  __nv_bfloat16* __restrict__ lo, long long ldo,
+                                  long long x_bstride, long long o_bstride) {
+    const float* Xb = X + blockIdx.y * x_bstride;
+    __nv_bfloat16* hb = hi + blockIdx.y * o_bstride;
+    __nv_bfloat16* lb = lo + blockIdx.y * o_bstride;
+    const long long total = rows * cols;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        long long r = e / cols, c = e - r * cols;
+        __nv_bfloat16 h, l;
+        split_one(Xb[r * ldx + c], h, l);
+        hb[r * ldo + c] = h;
+        lb[r * ldo + c] = l;
+    }
+}
+
+// Complex A (M x K, interleaved) -> real-embedded A' = [Ar | Ai] (M x 2K).
+static __global__ void split_bf16_cplx_a_kernel(const float2* __restrict__ A, long long M, long long K,
+                                         long long lda, __nv_bfloat16* __restrict__ hi,
+                                         __nv_bfloat16* __restrict__ lo, long long ldo) {
+    const long long total = M * K;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        long long r = e / K, c = e - r * K;
+        float2 v = A[r * lda + c];
+        __nv_bfloat16 h, l;
+        split_one(v.x, h, l);
+        hi[r * ldo + c] = h;
+        lo[r * ldo + c] = l;
+        split_one(v.y, h, l);
+        hi[r * ldo + K + c] = h;
+        lo[r * ldo + K + c] = l;
+    }
+}
+
+// Complex B (K x N) -> B' = [[Br, Bi], [-Bi, Br]] (2K x 2N).
+static __global__ void split_bf16_cplx_b_kernel(const float2* __restrict__ B, long long K, long long N,
+                                         long long ldb, __nv_bfloat16* __restrict__ hi,
+                                         __nv_bfloat16* __restrict__ lo, long long ldo) {
+    const long long total = K * N;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        long long r = e / N, c = e - r * N;
+        float2 v = B[r * ldb + c];
+        __nv_bfloat16 hr, lr, hi_, li;
+        split_one(v.x, hr, lr);
+        split_one(v.y, hi_, li);
+        // top block row r: [Br Bi]
+        hi[r * ldo + c] = hr;
+        lo[r * ldo + c] = lr;
+        hi[r * ldo + N + c] = hi_;
+        lo[r * ldo + N + c] = li;
+        // bottom block row K + r: [-Bi Br]  (negation is exact in bf16)
+        hi[(K + r) * ldo + c] = __hneg(hi_);
+        lo[(K + r) * ldo + c] = __hneg(li);
+        hi[(K + r) * ldo + N + c] = hr;
+        lo[(K + r) * ldo + N + c] = lr;
+    }
+}
+
+static __global__ void split_i16_kernel(const int16_t* __restrict__ X, long long rows, long long cols,
+                                 long long ldx, int8_t* __restrict__ hi, uint8_t* __restrict__ lo,
+                                 long long ldo, long long x_bstride, long long o_bstride) {
+    const int16_t* Xb = X + blockIdx.y * x_bstride;
+    int8_t* hb = hi + blockIdx.y * o_bstride;
+    uint8_t* lb = lo + blockIdx.y * o_bstride;
+    const long long total = rows * cols;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        long long r = e / cols, c = e - r * cols;
+        int v = Xb[r * ldx + c];
+        hb[r * ldo + c] = static_cast<int8_t>(v >> 8);  // arithmetic shift: floor(v / 256)
+        lb[r * ldo + c] = static_cast<uint8_t>(v & 0xFF);
+    }
+}
+
+static __global__ void pad_rows_kernel(const uint8_t* __restrict__ X, long long rows, long long row_bytes,
+                                long long ldx_bytes, uint8_t* __restrict__ Y, long long ldy_bytes,
+                                long long x_bstride, long long y_bstride) {
+    const uint8_t* Xb = X + blockIdx.y * x_bstride;
+    uint8_t* Yb = Y + blockIdx.y * y_bstride;
+    const long long total = rows * row_bytes;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        long long r = e / row_bytes, c = e - r * row_bytes;
+        Yb[r * ldy_bytes + c] = Xb[r * ldx_bytes + c];
+    }
+}
+
+// row_sum[i] = sum_k a[i, k] (u8), one warp per row, wrapping i32.
+static __global__ void row_sum_u8_kernel(const uint8_t* __restrict__ A, long long M, long long K,
+                                  long long lda, int* __restrict__ out) {
+    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x % 32;
+    if (warp >= M) return;
+    uint32_t s = 0;
+    for (long long k = lane; k < K; k += 32) s += A[warp * lda + k];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
+    if (lane == 0) out[warp] = static_cast<int>(s);
+}
+
+// col_sum[j] = sum_k b[k, j] (i8), one thread per column, wrapping i32.
+static __global__ void col_sum_i8_kernel(const int8_t* __restrict__ B, long long K, long long N,
+                                  long long ldb, int* __restrict__ out) {
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= N) return;
+    uint32_t s = 0;
+    for (long long k = 0; k < K; ++k) s += static_cast<uint32_t>(static_cast<int32_t>(B[k * ldb + j]));
+    out[j] = static_cast<int>(s);
+}
+
+// C = beta * C for k == 0 (real / complex), and fill.
+template <typename T>
+static __global__ void scale_kernel(T* __restrict__ C, long long rows, long long cols, long long ldc,
+                             T beta) {
+    const long long total = rows * cols;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        long long r = e / cols, c = e - r * cols;
+        C[r * ldc + c] = beta == T(0) ? T(0) : beta * C[r * ldc + c];
+    }
+}
+
+}  // namespace fg

@@ -1,0 +1,37 @@
+// stubs.cu -- entry points whose kernels are not built yet report
+// FG_ERR_UNSUPPORTED (never a CPU fallback).
+#include "runtime.h"
+
+namespace fgrt {
+fg_status launch_ozaki(fg_ctx*, const Gemm&, cudaStream_t) {
+    return set_error(FG_ERR_UNSUPPORTED, "Ozaki split DGEMM/ZGEMM not built yet");
+}
+}  // namespace fgrt
+
+using namespace fgrt;
+extern "C" {
+fg_status fg_gemm_grouped(fg_ctx*, fg_dtype, fg_mode, const fg_problem*, size_t, fg_stream) {
+    return set_error(FG_ERR_UNSUPPORTED, "grouped GEMM not built yet");
+}
+fg_status fg_grouped_plan_create(fg_ctx*, fg_dtype, fg_mode, const fg_problem*, size_t, fg_stream,
+                                 fg_grouped_plan**) {
+    return set_error(FG_ERR_UNSUPPORTED, "grouped GEMM not built yet");
+}
+fg_status fg_grouped_plan_run(fg_grouped_plan*, fg_stream) {
+    return set_error(FG_ERR_UNSUPPORTED, "grouped GEMM not built yet");
+}
+fg_status fg_grouped_plan_destroy(fg_grouped_plan*) { return FG_OK; }
+fg_status fg_server_start(fg_ctx*, size_t, int, int, fg_server**) {
+    return set_error(FG_ERR_UNSUPPORTED, "server not built yet");
+}
+fg_status fg_server_submit(fg_server*, const fg_request*, uint64_t*) {
+    return set_error(FG_ERR_UNSUPPORTED, "server not built yet");
+}
+fg_status fg_server_wait(fg_server*, uint64_t, int64_t) {
+    return set_error(FG_ERR_UNSUPPORTED, "server not built yet");
+}
+fg_status fg_server_stats_get(fg_server*, fg_server_stats*) {
+    return set_error(FG_ERR_UNSUPPORTED, "server not built yet");
+}
+fg_status fg_server_stop(fg_server*) { return FG_OK; }
+}

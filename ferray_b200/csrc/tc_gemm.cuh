@@ -1,0 +1,427 @@
+// tc_gemm.cuh -- persistent, warp-specialised tcgen05 GEMM for sm_100a.
+//
+// One CTA per SM walks a strided list of output tiles (BM=128 rows x BN
+// columns).  Warp roles:
+//   warp 0      TMA producer: loads the operand tiles of one K block
+//               (128 bytes of K) into a ring of shared-memory stages;
+//   warp 1      TMEM owner + MMA issuer: one elected thread issues
+//               tcgen05.mma for every (A tile, B tile, accumulator) product
+//               of the stage, then tcgen05.commit frees the stage;
+//   warps 2-5   epilogue: tcgen05.ld the accumulators of a finished tile
+//               (one TMEM lane = one output row per thread), combine them
+//               (wrapping i32, i16 byte-slice recombination, alpha/beta,
+//               quantized zero-point correction, complex interleave) and
+//               store to global memory.
+// Accumulators live in TMEM and are double-buffered when they fit in the 512
+// columns, so the epilogue of tile t overlaps the MMAs of tile t+1.
+//
+// A is K-major (row-major M x K in global memory), B is MN-major (row-major
+// K x N): both are read straight from the user's layout, 128-byte swizzled by
+// TMA, with no transpose pass.
+//
+// A "scheme" describes which operand tiles a K block loads and which
+// products accumulate where:
+//   plain i8/u8   1 A x 1 B -> 1 accumulator;
+//   i16           A = hi(s8)*256 + lo(u8), B likewise: 4 products into
+//                 3 accumulators (hh, hl+lh, ll), recombined mod 2^32;
+//   split bf16    A = hi + lo, B = hi + lo (bf16): lo*hi + hi*lo + hi*hi
+//                 into one f32 accumulator (the 3xBF16 SGEMM).
+#pragma once
+#include "fg_device.cuh"
+
+namespace fg {
+
+enum : int { KIND_I8 = 0, KIND_BF16 = 1 };
+enum : int { EPI_I32 = 0, EPI_I16 = 1, EPI_F32 = 2, EPI_QMM = 3 };
+
+constexpr int TC_MAX_OPS = 8;
+constexpr int TC_MAX_OPERANDS = 4;
+
+struct TcOp {
+    int a, b, acc;
+    int a_fmt, b_fmt;  // kind::i8: 0 = u8, 1 = s8; kind::f16: 1 = bf16
+};
+
+template <int KIND_, int BN_, int STAGES_, int NA_, int NB_, int NACC_, int NOPS_, int EPI_>
+struct TcCfg {
+    static constexpr int KIND = KIND_, BM = 128, BN = BN_, STAGES = STAGES_;
+    static constexpr int NA = NA_, NB = NB_, NACC = NACC_, NOPS = NOPS_, EPI = EPI_;
+    static constexpr int ESIZE = KIND == KIND_I8 ? 1 : 2;  // operand bytes
+    static constexpr int BK_BYTES = 128;
+    static constexpr int BK = BK_BYTES / ESIZE;             // K elements per block
+    static constexpr int KSTEP_BYTES = 32;                  // one MMA: 256 bits of K
+    static constexpr int KSTEPS = BK_BYTES / KSTEP_BYTES;   // MMAs per tile product
+    static constexpr int A_TILE = BM * BK_BYTES;            // bytes
+    static constexpr int B_TILE = BN * BK_BYTES;
+    static constexpr int B_CHUNK_ELEMS = 128 / ESIZE;       // N elements per TMA box
+    static constexpr int B_CHUNKS = BN / B_CHUNK_ELEMS;
+    static constexpr int B_CHUNK_BYTES = BK * 128;
+    static constexpr int STAGE_BYTES = NA * A_TILE + NB * B_TILE;
+    static constexpr int ACC_COLS = NACC * BN;
+    static constexpr int ACC_BUFS = (2 * ACC_COLS <= 512) ? 2 : 1;
+    static constexpr int TMEM_COLS = 512;
+    static constexpr int THREADS = 192;
+    static_assert(ACC_COLS <= 512, "accumulators exceed TMEM");
+    static_assert(BN % 16 == 0 && BN <= 256, "UMMA N");
+    static_assert(BN % B_CHUNK_ELEMS == 0, "B tile must be whole 128-byte chunks");
+};
+
+struct TcMaps {
+    CUtensorMap a[TC_MAX_OPERANDS];
+    CUtensorMap b[TC_MAX_OPERANDS];
+};
+
+struct TcArgs {
+    int M, N, K;
+    int tiles_m, tiles_n, k_blocks;
+    int batch;                 // number of output matrices
+    int a_rank3, b_rank3;      // 1 when the operand map is 3-D (batched)
+    // NumPy-style broadcast: output batch index -> operand matrix index.
+    int bdims;                 // number of batch dims (<= 4)
+    int bshape[4];             // output batch shape
+    long long a_bstride[4];    // operand matrix index strides (0 = broadcast)
+    long long b_bstride[4];
+    void* C;
+    long long ldc, strideC;    // elements
+    int accumulate;            // integer epilogues: add into C
+    float alpha, beta;         // EPI_F32 (beta == 0: C is not read)
+    int cplx_half;             // EPI_F32: >0 writes column j<h as Re, j>=h as Im
+    // EPI_QMM
+    const int* row_sum;
+    const int* col_sum;
+    int a_zp, b_zp;
+    float scale;
+    TcOp ops[TC_MAX_OPS];
+    DevStatus* status;
+    unsigned long long timeout_ns;
+};
+
+__device__ __forceinline__ void tile_coords(const TcArgs& p, int t, int& bz, int& tm, int& tn) {
+    const int per_batch = p.tiles_m * p.tiles_n;
+    bz = t / per_batch;
+    int r = t - bz * per_batch;
+    // Grouped raster: 8 row-tiles share each sweep over the column tiles so
+    // the A rows and B columns of concurrently running tiles stay in L2.
+    const int GROUP = 8;
+    int per_group = GROUP * p.tiles_n;
+    int g = r / per_group;
+    int first_m = g * GROUP;
+    int gm = min(p.tiles_m - first_m, GROUP);
+    int q = r - g * per_group;
+    tm = first_m + q % gm;
+    tn = q / gm;
+}
+
+__device__ __forceinline__ void batch_operands(const TcArgs& p, int bz, int& za, int& zb) {
+    long long ia = 0, ib = 0;
+    int rem = bz;
+    for (int d = p.bdims - 1; d >= 0; --d) {
+        int idx = rem % p.bshape[d];
+        rem /= p.bshape[d];
+        ia += idx * p.a_bstride[d];
+        ib += idx * p.b_bstride[d];
+    }
+    za = static_cast<int>(ia);
+    zb = static_cast<int>(ib);
+}
+
+template <class Cfg>
+struct TcSmem {
+    alignas(1024) uint8_t a[Cfg::STAGES][Cfg::NA][Cfg::A_TILE];
+    alignas(1024) uint8_t b[Cfg::STAGES][Cfg::NB][Cfg::B_TILE];
+    uint64_t full[Cfg::STAGES];
+    uint64_t empty[Cfg::STAGES];
+    uint64_t acc_full[2];
+    uint64_t acc_empty[2];
+    uint64_t drain;
+    uint32_t tmem_base;
+    int abort;
+};
+
+template <class Cfg>
+__device__ __forceinline__ void epilogue_store(const TcArgs& p, int bz, int grow, int gcol0,
+                                               const uint32_t (&v)[Cfg::NACC][32]) {
+    if (grow >= p.M) return;
+    const int ncols = min(32, p.N - gcol0);
+    if (ncols <= 0) return;
+    if constexpr (Cfg::EPI == EPI_I32 || Cfg::EPI == EPI_I16) {
+        int32_t* crow = static_cast<int32_t*>(p.C) + bz * p.strideC + (long long)grow * p.ldc + gcol0;
+        uint32_t out[32];
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            if constexpr (Cfg::EPI == EPI_I32) {
+                out[j] = v[0][j];
+            } else {
+                out[j] = (v[0][j] << 16) + (v[1][j] << 8) + v[2][j];
+            }
+        }
+        const bool vec = ncols == 32 && (reinterpret_cast<uintptr_t>(crow) & 15) == 0;
+        if (vec) {
+#pragma unroll
+            for (int j = 0; j < 32; j += 4) {
+                uint4 w = make_uint4(out[j], out[j + 1], out[j + 2], out[j + 3]);
+                if (p.accumulate) {
+                    uint4 o = *reinterpret_cast<const uint4*>(crow + j);
+                    w.x += o.x; w.y += o.y; w.z += o.z; w.w += o.w;
+                }
+                *reinterpret_cast<uint4*>(crow + j) = w;
+            }
+        } else {
+            for (int j = 0; j < ncols; ++j) {
+                uint32_t w = out[j];
+                if (p.accumulate) w += static_cast<uint32_t>(crow[j]);
+                crow[j] = static_cast<int32_t>(w);
+            }
+        }
+    } else if constexpr (Cfg::EPI == EPI_QMM) {
+        float* crow = static_cast<float*>(p.C) + bz * p.strideC + (long long)grow * p.ldc + gcol0;
+        const uint32_t rs = static_cast<uint32_t>(p.row_sum[grow]);
+        const uint32_t azp = static_cast<uint32_t>(p.a_zp), bzp = static_cast<uint32_t>(p.b_zp);
+        const uint32_t kab = static_cast<uint32_t>(p.K) * azp * bzp;
+        for (int j = 0; j < ncols; ++j) {
+            uint32_t cs = static_cast<uint32_t>(p.col_sum[gcol0 + j]);
+            uint32_t corr = v[0][j] - azp * cs - bzp * rs + kab;
+            // Separate roundings, as gemm/mod.rs:566-571 computes them (no FMA).
+            float o = __fmul_rn(p.scale, static_cast<float>(static_cast<int32_t>(corr)));
+            if (p.accumulate) o = __fadd_rn(crow[j], o);
+            crow[j] = o;
+        }
+    } else {  // EPI_F32
+        float* cbase = static_cast<float*>(p.C) + bz * p.strideC;
+        if (p.cplx_half > 0) {
+            // Column j of the real-embedded product is Re (j < h) or Im (j >= h)
+            // of complex column j mod h; C is interleaved (re, im).
+            const int h = p.cplx_half;
+            for (int j = 0; j < ncols; ++j) {
+                int col = gcol0 + j;
+                int cc = col < h ? col : col - h;
+                float* dst = cbase + (long long)grow * p.ldc + 2 * cc + (col < h ? 0 : 1);
+                float o = p.alpha * __uint_as_float(v[0][j]);
+                if (p.beta != 0.f) o = fmaf(p.beta, *dst, o);
+                *dst = o;
+            }
+            return;
+        }
+        float* crow = cbase + (long long)grow * p.ldc + gcol0;
+        float out[32];
+#pragma unroll
+        for (int j = 0; j < 32; ++j) out[j] = p.alpha * __uint_as_float(v[0][j]);
+        const bool vec = ncols == 32 && (reinterpret_cast<uintptr_t>(crow) & 15) == 0;
+        if (vec) {
+#pragma unroll
+            for (int j = 0; j < 32; j += 4) {
+                float4 w = make_float4(out[j], out[j + 1], out[j + 2], out[j + 3]);
+                if (p.beta != 0.f) {
+                    float4 o = *reinterpret_cast<const float4*>(crow + j);
+                    w.x = fmaf(p.beta, o.x, w.x); w.y = fmaf(p.beta, o.y, w.y);
+                    w.z = fmaf(p.beta, o.z, w.z); w.w = fmaf(p.beta, o.w, w.w);
+                }
+                *reinterpret_cast<float4*>(crow + j) = w;
+            }
+        } else {
+            for (int j = 0; j < ncols; ++j) {
+                float o = out[j];
+                if (p.beta != 0.f) o = fmaf(p.beta, crow[j], o);
+                crow[j] = o;
+            }
+        }
+    }
+}
+
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::THREADS, 1)
+    tc_gemm_kernel(const __grid_constant__ TcMaps maps, const __grid_constant__ TcArgs p) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    // The dynamic shared window is only guaranteed 16-byte aligned: round up
+    // to the 1024-byte alignment the 128-byte swizzle atoms need (the launch
+    // reserves the extra kilobyte).
+    uint8_t* base = reinterpret_cast<uint8_t*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+    TcSmem<Cfg>& s = *reinterpret_cast<TcSmem<Cfg>*>(base);
+
+    const int warp = threadIdx.x / 32;
+    const int lane = threadIdx.x % 32;
+    const int total_tiles = p.batch * p.tiles_m * p.tiles_n;
+    volatile int* abort = &s.abort;
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < Cfg::STAGES; ++i) {
+            mbar_init(&s.full[i], 1);
+            mbar_init(&s.empty[i], 1);
+        }
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&s.acc_full[i], 1);
+            mbar_init(&s.acc_empty[i], 4);  // one arrive per epilogue warp
+        }
+        mbar_init(&s.drain, 1);
+        s.abort = 0;
+        fence_mbar_init();
+    }
+    if (warp == 0 && lane == 0) {
+        for (int i = 0; i < Cfg::NA; ++i) tma_prefetch_desc(&maps.a[i]);
+        for (int i = 0; i < Cfg::NB; ++i) tma_prefetch_desc(&maps.b[i]);
+    }
+    if (warp == 1) {
+        tmem_alloc(&s.tmem_base, Cfg::TMEM_COLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s.tmem_base;
+
+    if (warp == 0) {
+        // ------------------------------------------------ TMA producer
+        if (elect_one()) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int issued_parity[Cfg::STAGES];
+            for (int i = 0; i < Cfg::STAGES; ++i) issued_parity[i] = -1;
+            bool ok = true;
+            for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x) {
+                int bz, tm, tn, za, zb;
+                tile_coords(p, t, bz, tm, tn);
+                batch_operands(p, bz, za, zb);
+                for (int kb = 0; kb < p.k_blocks; ++kb) {
+                    if (!mbar_wait(&s.empty[stage], phase ^ 1u, p.timeout_ns, p.status, 0x01,
+                                   abort)) {
+                        ok = false;
+                        break;
+                    }
+                    mbar_arrive_expect_tx(&s.full[stage], Cfg::STAGE_BYTES);
+                    const int kx = kb * Cfg::BK;
+                    for (int i = 0; i < Cfg::NA; ++i) {
+                        if (p.a_rank3)
+                            tma_load_3d(s.a[stage][i], &maps.a[i], kx, tm * Cfg::BM, za, &s.full[stage]);
+                        else
+                            tma_load_2d(s.a[stage][i], &maps.a[i], kx, tm * Cfg::BM, &s.full[stage]);
+                    }
+                    for (int i = 0; i < Cfg::NB; ++i) {
+#pragma unroll
+                        for (int c = 0; c < Cfg::B_CHUNKS; ++c) {
+                            uint8_t* dst = s.b[stage][i] + c * Cfg::B_CHUNK_BYTES;
+                            const int nx = tn * Cfg::BN + c * Cfg::B_CHUNK_ELEMS;
+                            if (p.b_rank3)
+                                tma_load_3d(dst, &maps.b[i], nx, kx, zb, &s.full[stage]);
+                            else
+                                tma_load_2d(dst, &maps.b[i], nx, kx, &s.full[stage]);
+                        }
+                    }
+                    issued_parity[stage] = static_cast<int>(phase);
+                    if (++stage == Cfg::STAGES) {
+                        stage = 0;
+                        phase ^= 1u;
+                    }
+                }
+            }
+            if (!ok) {
+                // Let every load this thread issued land before the CTA exits.
+                for (int i = 0; i < Cfg::STAGES; ++i) {
+                    if (issued_parity[i] < 0) continue;
+                    volatile int never = 0;
+                    mbar_wait(&s.full[i], static_cast<uint32_t>(issued_parity[i]), p.timeout_ns,
+                              nullptr, 0, &never);
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------ MMA issuer
+        if (elect_one()) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int it = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x, ++it) {
+                const int buf = it % Cfg::ACC_BUFS;
+                const uint32_t acc_par = static_cast<uint32_t>((it / Cfg::ACC_BUFS) & 1);
+                if (!mbar_wait(&s.acc_empty[buf], acc_par ^ 1u, p.timeout_ns, p.status, 0x11, abort)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t acc_base = tmem + buf * Cfg::ACC_COLS;
+                for (int kb = 0; kb < p.k_blocks; ++kb) {
+                    if (!mbar_wait(&s.full[stage], phase, p.timeout_ns, p.status, 0x12, abort)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+#pragma unroll
+                    for (int o = 0; o < Cfg::NOPS; ++o) {
+                        const TcOp op = p.ops[o];
+                        // first product into this accumulator in the tile?
+                        bool first_for_acc = true;
+#pragma unroll
+                        for (int q = 0; q < o; ++q)
+                            if (p.ops[q].acc == op.acc) first_for_acc = false;
+                        const uint32_t idesc = umma_idesc(Cfg::KIND == KIND_I8 ? 2u : 1u,
+                                                          op.a_fmt, op.b_fmt, 0u, 1u, Cfg::BM, Cfg::BN);
+                        const uint32_t a_addr = smem_u32(s.a[stage][op.a]);
+                        const uint32_t b_addr = smem_u32(s.b[stage][op.b]);
+#pragma unroll
+                        for (int kk = 0; kk < Cfg::KSTEPS; ++kk) {
+                            const uint64_t ad = umma_desc_sw128(a_addr + kk * Cfg::KSTEP_BYTES, 16, 1024);
+                            const uint64_t bd = umma_desc_sw128(
+                                b_addr + kk * (Cfg::KSTEP_BYTES / Cfg::ESIZE) * 128, Cfg::B_CHUNK_BYTES, 1024);
+                            const uint32_t acc = (kb > 0 || kk > 0 || !first_for_acc) ? 1u : 0u;
+                            if constexpr (Cfg::KIND == KIND_I8)
+                                tc_mma_i8(acc_base + op.acc * Cfg::BN, ad, bd, idesc, acc);
+                            else
+                                tc_mma_f16(acc_base + op.acc * Cfg::BN, ad, bd, idesc, acc);
+                        }
+                    }
+                    tc_commit(&s.empty[stage]);
+                    if (++stage == Cfg::STAGES) {
+                        stage = 0;
+                        phase ^= 1u;
+                    }
+                }
+                if (!ok) break;
+                tc_commit(&s.acc_full[buf]);
+            }
+            // Every MMA issued above has completed once `drain` flips.
+            tc_commit(&s.drain);
+            volatile int never = 0;
+            mbar_wait(&s.drain, 0, p.timeout_ns, ok ? p.status : nullptr, 0x13, &never);
+        }
+    } else {
+        // ------------------------------------------------ epilogue
+        const int ew = warp & 3;  // TMEM lane quarter this warp may access
+        int it = 0;
+        for (int t = blockIdx.x; t < total_tiles; t += gridDim.x, ++it) {
+            const int buf = it % Cfg::ACC_BUFS;
+            const uint32_t acc_par = static_cast<uint32_t>((it / Cfg::ACC_BUFS) & 1);
+            if (!mbar_wait(&s.acc_full[buf], acc_par, p.timeout_ns, p.status, 0x21, abort)) break;
+            tc_fence_after();
+            int bz, tm, tn;
+            tile_coords(p, t, bz, tm, tn);
+            const int grow = tm * Cfg::BM + ew * 32 + lane;
+            const uint32_t row_addr = tmem + (static_cast<uint32_t>(ew * 32) << 16) + buf * Cfg::ACC_COLS;
+#pragma unroll 1
+            for (int c = 0; c < Cfg::BN / 32; ++c) {
+                uint32_t v[Cfg::NACC][32];
+#pragma unroll
+                for (int a = 0; a < Cfg::NACC; ++a) tmem_ld_32x32b_x32(row_addr + a * Cfg::BN + c * 32, v[a]);
+                tmem_wait_ld();
+                epilogue_store<Cfg>(p, bz, grow, tn * Cfg::BN + c * 32, v);
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&s.acc_empty[buf]);
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem, Cfg::TMEM_COLS);
+    }
+}
+
+template <class Cfg>
+constexpr size_t tc_smem_bytes() {
+    return sizeof(TcSmem<Cfg>) + 1024;
+}
+
+}  // namespace fg

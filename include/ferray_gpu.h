@@ -1,0 +1,253 @@
+/*
+ * ferray_gpu.h -- C ABI of the ferray B200 GEMM backend (libferray_b200.so).
+ *
+ * Replaces the GEMM behind ferray_linalg::matmul / ferray::matmul.  Every
+ * entry point below names the ferray function (file:line inside the ferray
+ * workspace) whose contract it keeps.  Conventions:
+ *
+ *  - Matrices are row-major.  Leading dimensions are in ELEMENTS (complex
+ *    elements for complex types), exactly like the reference's internal
+ *    drivers (gemm/outer.rs: lda, ldb, ldc); the fg_gemm_<dtype> forms fix
+ *    lda = k, ldb = n, ldc = n like the reference's public entry points.
+ *  - Complex operands are interleaved (re, im) pairs, the layout of
+ *    num_complex::Complex<T> (repr(C)).  As in ferray, "c64" means
+ *    Complex<f64> and "c32" means Complex<f32>.
+ *  - Pointers passed to fg_gemm_* / fg_matmul_* are DEVICE pointers (from
+ *    fg_buffer_alloc or any cudaMalloc'd memory of the context's device).
+ *    The *_host forms take host pointers, stage through the device and
+ *    return when the result is back in host memory: they are the drop-in
+ *    for ferray's slice-based entry points.
+ *  - Every function returns fg_status.  FG_OK is 0.  The reference returns
+ *    `false` when no CPU kernel applies and FerrayError::ShapeMismatch /
+ *    BroadcastFailure for bad shapes (ferray-core/src/error.rs:16-99); here
+ *    those become FG_ERR_UNSUPPORTED, FG_ERR_SHAPE and FG_ERR_BROADCAST.
+ *  - Device-pointer calls are asynchronous on `stream` (NULL = the
+ *    context's stream).  Kernel-side failures (a bounded wait that ran out)
+ *    are reported by the next fg_sync on that context.
+ *  - Thread safety: a context may be used from many host threads; calls on
+ *    different streams may overlap on the device.  Scratch memory comes
+ *    from the stream-ordered allocator on the call's stream.
+ *  - No CPU fallback: without a usable sm_100 device fg_init fails.
+ */
+#ifndef FERRAY_GPU_H
+#define FERRAY_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum fg_status {
+    FG_OK = 0,
+    FG_ERR_SHAPE = 1,       /* inner dimensions / lengths disagree            */
+    FG_ERR_DTYPE = 2,       /* dtype not valid for this entry point           */
+    FG_ERR_OOM = 3,         /* device allocation failed                        */
+    FG_ERR_BUDGET = 4,      /* request exceeds the server's HBM budget        */
+    FG_ERR_TIMEOUT = 5,     /* a bounded device or host wait ran out           */
+    FG_ERR_DEVICE = 6,      /* CUDA error                                      */
+    FG_ERR_INVALID = 7,     /* bad argument (null pointer, bad mode, ...)      */
+    FG_ERR_UNSUPPORTED = 8, /* no kernel for this case (reference: `false`)    */
+    FG_ERR_BROADCAST = 9    /* batch shapes do not broadcast                   */
+} fg_status;
+
+typedef enum fg_dtype {
+    FG_F64 = 0,  /* f64                     */
+    FG_F32 = 1,  /* f32                     */
+    FG_C64 = 2,  /* Complex<f64> (16 bytes) */
+    FG_C32 = 3,  /* Complex<f32> (8 bytes)  */
+    FG_I8 = 4,   /* i8 x i8 -> i32          */
+    FG_U8I8 = 5, /* u8 x i8 -> i32          */
+    FG_I16 = 6   /* i16 x i16 -> i32        */
+} fg_dtype;
+
+typedef enum fg_mode {
+    /* f64/c64: FP64 pipe; f32/c32: FFMA; integers: integer tensor cores.   */
+    FG_MODE_PLAIN = 0,
+    /* f32/c32: 3 x BF16 products on tcgen05 with FP32 accumulation;        */
+    /* f64/c64: Ozaki INT8 slicing with exact INT32 accumulation.           */
+    /* Integer dtypes ignore the mode (they are exact either way).          */
+    FG_MODE_SPLIT = 1
+} fg_mode;
+
+typedef struct fg_ctx fg_ctx;
+typedef void *fg_stream; /* a cudaStream_t */
+
+/* ------------------------------------------------------------ context */
+/* Opens `device` (must be sm_100).  ferray's GEMM has no handle; its pool
+ * is process-global (gemm/outer.rs:142-155). */
+fg_status fg_init(int device, fg_ctx **out);
+fg_status fg_shutdown(fg_ctx *ctx);
+/* Waits for `stream` (NULL: context stream) and reports kernel-side errors
+ * recorded since the last fg_sync. */
+fg_status fg_sync(fg_ctx *ctx, fg_stream stream);
+const char *fg_status_string(fg_status s);
+/* Message of the last error raised on the calling thread ("" if none). */
+const char *fg_last_error(void);
+/* Number of kernels this library has launched in the process. */
+uint64_t fg_launch_count(void);
+/* Device properties used for roofline bookkeeping. */
+fg_status fg_device_info(fg_ctx *ctx, int *sm_count, int *cc_major, int *cc_minor,
+                         size_t *hbm_bytes);
+
+/* ------------------------------------------------------------ buffers */
+/* Device-resident buffers: the device counterpart of ferray-core's
+ * Array storage (ferray-core/src/array/owned.rs:21, buffer.rs:25-49). */
+fg_status fg_buffer_alloc(fg_ctx *ctx, size_t bytes, void **dptr);
+fg_status fg_buffer_free(fg_ctx *ctx, void *dptr);
+fg_status fg_upload(fg_ctx *ctx, void *dst_dev, const void *src_host, size_t bytes,
+                    fg_stream stream);
+fg_status fg_download(fg_ctx *ctx, void *dst_host, const void *src_dev, size_t bytes,
+                      fg_stream stream);
+/* Page-lock host memory so uploads/downloads run at full PCIe speed. */
+fg_status fg_host_register(fg_ctx *ctx, void *host, size_t bytes);
+fg_status fg_host_unregister(fg_ctx *ctx, void *host);
+
+/* ------------------------------------------------------------ raw GEMMs */
+/* C = alpha*A@B + beta*C, f64.  Replaces gemm_f64 (gemm/mod.rs:197-328).
+ * mode SPLIT = Ozaki INT8 with `ozaki_slices` slices (0 = default 8). */
+fg_status fg_gemm_f64(fg_ctx *ctx, fg_mode mode, int ozaki_slices, size_t m, size_t n,
+                      size_t k, double alpha, const double *a, const double *b, double beta,
+                      double *c, fg_stream stream);
+/* C = alpha*A@B + beta*C, f32.  Replaces gemm_f32 (gemm/mod.rs:940-1062).
+ * mode SPLIT = 3 x BF16 on tcgen05. */
+fg_status fg_gemm_f32(fg_ctx *ctx, fg_mode mode, size_t m, size_t n, size_t k, float alpha,
+                      const float *a, const float *b, float beta, float *c, fg_stream stream);
+/* Complex<f64>.  Replaces gemm_c64 (gemm/mod.rs:757-826). */
+fg_status fg_gemm_c64(fg_ctx *ctx, fg_mode mode, int ozaki_slices, size_t m, size_t n,
+                      size_t k, double alpha_re, double alpha_im, const double *a,
+                      const double *b, double beta_re, double beta_im, double *c,
+                      fg_stream stream);
+/* Complex<f32>.  Replaces gemm_c32 (gemm/mod.rs:669-736). */
+fg_status fg_gemm_c32(fg_ctx *ctx, fg_mode mode, size_t m, size_t n, size_t k, float alpha_re,
+                      float alpha_im, const float *a, const float *b, float beta_re,
+                      float beta_im, float *c, fg_stream stream);
+/* i8 x i8 -> i32, wrapping, optional accumulate into C.
+ * Replaces gemm_i8_signed (gemm/mod.rs:414-448). */
+fg_status fg_gemm_i8_signed(fg_ctx *ctx, size_t m, size_t n, size_t k, const int8_t *a,
+                            const int8_t *b, int32_t *c, int accumulate, fg_stream stream);
+/* u8 x i8 -> i32, exact (the VNNI semantics).  Replaces gemm_i8
+ * (gemm/mod.rs:601-651). */
+fg_status fg_gemm_i8(fg_ctx *ctx, size_t m, size_t n, size_t k, const uint8_t *a,
+                     const int8_t *b, int32_t *c, int accumulate, fg_stream stream);
+/* i16 x i16 -> i32, wrapping.  Replaces gemm_i16 (gemm/mod.rs:348-392). */
+fg_status fg_gemm_i16(fg_ctx *ctx, size_t m, size_t n, size_t k, const int16_t *a,
+                      const int16_t *b, int32_t *c, int accumulate, fg_stream stream);
+/* scale_a*scale_b*sum((a-a_zp)*(b-b_zp)) -> f32, zero points and scale fused
+ * into the i8 kernel's epilogue.  Replaces quantized_matmul
+ * (gemm/mod.rs:484-575). */
+fg_status fg_quantized_matmul(fg_ctx *ctx, size_t m, size_t n, size_t k, const uint8_t *a,
+                              uint8_t a_zp, float scale_a, const int8_t *b, int8_t b_zp,
+                              float scale_b, float *c, int accumulate, fg_stream stream);
+
+/* Generic strided form of all of the above (the reference's internal
+ * drivers take lda/ldb/ldc: gemm/outer.rs:198-210).  alpha/beta point to a
+ * scalar of the dtype's real type (two for complex: re, im); integer dtypes
+ * ignore them and use `accumulate`. */
+fg_status fg_gemm(fg_ctx *ctx, fg_dtype dtype, fg_mode mode, int ozaki_slices, size_t m,
+                  size_t n, size_t k, const void *alpha, const void *a, size_t lda,
+                  const void *b, size_t ldb, const void *beta, void *c, size_t ldc,
+                  int accumulate, fg_stream stream);
+
+/* Host-pointer drop-ins: same contracts as the device forms above, with
+ * host slices in and out (the signatures of gemm/mod.rs).  Synchronous. */
+fg_status fg_gemm_f64_host(fg_ctx *ctx, fg_mode mode, int ozaki_slices, size_t m, size_t n,
+                           size_t k, double alpha, const double *a, const double *b,
+                           double beta, double *c);
+fg_status fg_gemm_f32_host(fg_ctx *ctx, fg_mode mode, size_t m, size_t n, size_t k,
+                           float alpha, const float *a, const float *b, float beta, float *c);
+fg_status fg_gemm_host(fg_ctx *ctx, fg_dtype dtype, fg_mode mode, int ozaki_slices, size_t m,
+                       size_t n, size_t k, const void *alpha, const void *a, const void *b,
+                       const void *beta, void *c, int accumulate);
+
+/* ------------------------------------------------------------ batches */
+/* Stacked GEMM with one M,N,K for all `batch` problems: problem i reads
+ * A + i*stride_a, B + i*stride_b and writes C + i*stride_c (element
+ * strides; 0 broadcasts one operand).  Replaces the per-problem loop of
+ * matmul_batched (products/mod.rs:579-659). */
+fg_status fg_gemm_batched_strided(fg_ctx *ctx, fg_dtype dtype, fg_mode mode, int ozaki_slices,
+                                  size_t batch, size_t m, size_t n, size_t k, const void *alpha,
+                                  const void *a, size_t lda, int64_t stride_a, const void *b,
+                                  size_t ldb, int64_t stride_b, const void *beta, void *c,
+                                  size_t ldc, int64_t stride_c, int accumulate,
+                                  fg_stream stream);
+
+/* NumPy `matmul` on device arrays of any rank (1-D operands promoted and
+ * squeezed, batch dims broadcast with NumPy rules).  Replaces matmul
+ * (products/mod.rs:362-437), matmul_batched + broadcast_shapes
+ * (:579-686) and matmul_complex (complex.rs:136-264).  The output shape is
+ * written to out_shape/out_ndim (capacity 8); pass c = NULL to query it. */
+fg_status fg_matmul(fg_ctx *ctx, fg_dtype dtype, fg_mode mode, const void *a, int ndim_a,
+                    const int64_t *shape_a, const void *b, int ndim_b, const int64_t *shape_b,
+                    void *c, int64_t *out_shape, int *out_ndim, fg_stream stream);
+
+/* Ragged batch: `count` independent problems with their own M, N, K,
+ * pointers and leading dimensions, run by ONE persistent grouped kernel
+ * driven by a device-side problem table and tile counter.  No reference
+ * counterpart (ferray calls matmul_raw once per problem). */
+typedef struct fg_problem {
+    int64_t m, n, k;
+    const void *a;
+    const void *b;
+    void *c;
+    int64_t lda, ldb, ldc;
+} fg_problem;
+
+/* `table` is a HOST array; it is copied to the device on `stream`.
+ * dtype: FG_F32 (plain FFMA or SPLIT 3xBF16) or FG_I8 (exact). */
+fg_status fg_gemm_grouped(fg_ctx *ctx, fg_dtype dtype, fg_mode mode, const fg_problem *table,
+                          size_t count, fg_stream stream);
+
+/* Opaque prepared plan for a grouped batch whose shapes repeat: the table is
+ * uploaded once and the launch sequence is captured in a CUDA graph;
+ * fg_grouped_plan_run replays it. */
+typedef struct fg_grouped_plan fg_grouped_plan;
+fg_status fg_grouped_plan_create(fg_ctx *ctx, fg_dtype dtype, fg_mode mode,
+                                 const fg_problem *table, size_t count, fg_stream stream,
+                                 fg_grouped_plan **out);
+fg_status fg_grouped_plan_run(fg_grouped_plan *plan, fg_stream stream);
+fg_status fg_grouped_plan_destroy(fg_grouped_plan *plan);
+
+/* ------------------------------------------------------------ serving */
+/* Continuous-batching request loop.  Host threads submit matmul requests
+ * (mixed shapes and dtypes) whose operands are already on the device; the
+ * server admits them against an HBM budget, folds queued requests into
+ * grouped launches while earlier ones still run on other streams, and
+ * completes tickets as their results land.  No reference counterpart. */
+typedef struct fg_server fg_server;
+
+typedef struct fg_request {
+    fg_dtype dtype;
+    fg_mode mode;
+    int64_t m, n, k;
+    const void *a; /* device, row-major m x k  */
+    const void *b; /* device, row-major k x n  */
+    void *c;       /* device, row-major m x n  */
+    size_t scratch_bytes; /* 0: the server estimates it from the shape */
+} fg_request;
+
+typedef struct fg_server_stats {
+    uint64_t completed;
+    uint64_t launches;
+    uint64_t grouped_launches;
+    double p50_ms, p99_ms, mean_ms;
+    double useful_flops;   /* sum of 2mnk (8mnk complex) of completed work */
+    double busy_seconds;   /* wall time from first admit to last completion */
+    size_t hbm_in_use, hbm_peak;
+} fg_server_stats;
+
+fg_status fg_server_start(fg_ctx *ctx, size_t hbm_budget_bytes, int streams,
+                          int max_group, fg_server **out);
+fg_status fg_server_submit(fg_server *srv, const fg_request *req, uint64_t *ticket);
+/* Waits up to timeout_ms (<0: forever) for the ticket; FG_ERR_TIMEOUT if
+ * it has not completed. */
+fg_status fg_server_wait(fg_server *srv, uint64_t ticket, int64_t timeout_ms);
+fg_status fg_server_stats_get(fg_server *srv, fg_server_stats *out);
+fg_status fg_server_stop(fg_server *srv);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FERRAY_GPU_H */

@@ -1,0 +1,65 @@
+"""CPU tests of the C-ABI library: it loads without a GPU and exports every
+function include/ferray_gpu.h declares; calls that need no device report
+errors the way the header says (no compute is issued)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "ferray_gpu.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(fg_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_the_reference_surface():
+    names = declared_functions()
+    for want in ("fg_gemm_f64", "fg_gemm_f32", "fg_gemm_c64", "fg_gemm_c32", "fg_gemm_i8",
+                 "fg_gemm_i8_signed", "fg_gemm_i16", "fg_quantized_matmul", "fg_matmul",
+                 "fg_gemm_batched_strided", "fg_gemm_grouped", "fg_server_start"):
+        assert want in names
+
+
+def test_library_exports_every_declared_symbol():
+    from ferray_b200 import _lib
+    lib = C.CDLL(_lib.LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+    # the Python binding declares the same set
+    assert set(declared_functions()) <= set(_lib.SIGNATURES)
+
+
+def test_status_strings_and_errors_without_device():
+    from ferray_b200 import _lib
+    lib = _lib.load()
+    assert lib.fg_status_string(_lib.FG_OK) == b"ok"
+    assert lib.fg_status_string(_lib.FG_ERR_SHAPE) == b"shape mismatch"
+    # null context / null out pointer are argument errors, not crashes
+    assert lib.fg_gemm_f64(None, 0, 0, 1, 1, 1, 1.0, None, None, 0.0, None, None) == _lib.FG_ERR_INVALID
+    assert lib.fg_init(0, None) == _lib.FG_ERR_INVALID
+
+
+def test_init_fails_loudly_without_gpu():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from ferray_b200 import _lib
+    lib = _lib.load()
+    h = C.c_void_p()
+    assert lib.fg_init(0, C.byref(h)) != _lib.FG_OK
+    assert h.value is None
+
+
+def test_package_has_no_cpu_fallback(tmp_path, monkeypatch):
+    import importlib
+    from ferray_b200 import _lib
+    monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "missing.so"))
+    monkeypatch.setattr(_lib, "_lib", None)
+    with pytest.raises(OSError):
+        _lib.load()
+    importlib.reload(_lib)

@@ -1,0 +1,182 @@
+"""CPU tests of the oracle itself, pinned to the reference's golden vectors.
+
+* ferray's restated CPU GEMM reproduces the NumPy 2.4.5 fixture
+  (fixtures/linalg/matmul.json, tolerance_ulps per case) and the exact NumPy
+  hex-float answers of gemm/mod.rs:1213-1275;
+* the integer restatement equals the naive wrapping-i32 loops the reference
+  asserts against (gemm/integer_tests.rs), case by case;
+* the double-double oracle agrees with exact rational arithmetic on small
+  cases and is far more accurate than any FP64 result it judges.
+"""
+import json
+import os
+from fractions import Fraction
+
+import numpy as np
+import pytest
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def ulps(a, b):
+    a = np.asarray(a, np.float64).view(np.int64)
+    b = np.asarray(b, np.float64).view(np.int64)
+    return np.abs(a - b)
+
+
+def test_numpy_fixture_matmul(oracle):
+    d = json.load(open(os.path.join(GOLD, "matmul_numpy.json")))
+    assert d["numpy_version"] == "2.4.5"
+    for cs in d["cases"]:
+        a = np.array(cs["a"], np.float64).reshape(cs["a_shape"])
+        b = np.array(cs["b"], np.float64).reshape(cs["b_shape"])
+        exp = np.array(cs["expected"], np.float64)
+        got = oracle.matmul_raw(a, b).reshape(-1)
+        # ferray-test-oracle floors every ULP tolerance at 10 (lib.rs:59)
+        assert np.all(ulps(got, exp) <= max(cs["tolerance_ulps"], 10)), cs["name"]
+        dd = oracle.dd_full(a, b).reshape(-1)
+        assert np.all(ulps(dd, exp) <= cs["tolerance_ulps"]), cs["name"]
+
+
+def test_hexfloat_goldens(oracle):
+    cases = json.load(open(os.path.join(GOLD, "gemm_hexfloat.json")))
+    for cs in cases:
+        a = np.array([float.fromhex(x) for x in cs["a"]]).reshape(cs["a_shape"])
+        b = np.array([float.fromhex(x) for x in cs["b"]]).reshape(cs["b_shape"])
+        exp = np.array([float.fromhex(x) for x in cs["expected"]])
+        got = oracle.gemm_f64(a, b).reshape(-1)
+        assert np.all(ulps(got, exp) <= cs["max_ulps"]), (cs["name"], got, exp)
+        # NumPy's answer itself carries rounding error (up to k*u*|A||B|
+        # elementwise), so the correctly rounded DD value may differ from it
+        # by more ulps where the sum cancels; bound the difference instead.
+        dd = oracle.dd_full(a, b).reshape(-1)
+        bound = (np.abs(a) @ np.abs(b)).reshape(-1) * a.shape[1] * 2.0 ** -53
+        assert np.all(np.abs(dd - exp) <= bound), cs["name"]
+
+
+def test_integer_golden_cases(oracle):
+    cases = json.load(open(os.path.join(GOLD, "integer_cases.json")))
+    seen = set()
+    for cs in cases:
+        m, n, k = cs["m"], cs["n"], cs["k"]
+        seen.add(cs["kind"])
+        if cs["kind"] in ("i16", "i8s"):
+            dt = np.int16 if cs["kind"] == "i16" else np.int8
+            a = np.array(cs["a"], dt).reshape(m, k)
+            b = np.array(cs["b"], dt).reshape(k, n)
+            c0 = None if cs["c0"] is None else np.array(cs["c0"], np.int32).reshape(m, n)
+            fn = oracle.gemm_i16 if cs["kind"] == "i16" else oracle.gemm_i8_signed
+            got = fn(a, b, c=c0, accumulate=c0 is not None)
+            np.testing.assert_array_equal(got.reshape(-1), np.array(cs["expected"], np.int32),
+                                          cs["name"])
+        else:
+            a = np.array(cs["a"], np.uint8).reshape(m, k)
+            b = np.array(cs["b"], np.int8).reshape(k, n)
+            c0 = cs.get("c0_f32")
+            c0 = None if c0 is None else np.array(c0, np.float32).reshape(m, n)
+            # the naive formula of integer_tests.rs:30-63
+            acc = ((a.astype(np.int64) - cs["a_zp"]) @ (b.astype(np.int64) - cs["b_zp"]))
+            acc = ((acc + 2 ** 31) % 2 ** 32 - 2 ** 31).astype(np.int32)
+            want = np.float32(np.float32(cs["scale_a"]) * np.float32(cs["scale_b"])) * acc.astype(np.float32)
+            if c0 is not None:
+                want = c0 + want
+            for variant in ("vnni", "avx2"):
+                got = oracle.quantized_matmul(a, cs["a_zp"], cs["scale_a"], b, cs["b_zp"],
+                                              cs["scale_b"], c=None if c0 is None else c0.copy(),
+                                              accumulate=c0 is not None, variant=variant)
+                rel = np.abs(got - want) / np.maximum(np.abs(want), 1.0)
+                assert np.all(rel < cs["rel_tol"]), (cs["name"], variant)
+    assert seen == {"i16", "i8s", "qmm"}
+
+
+def test_u8i8_avx2_saturates_only_full_tiles(oracle):
+    # a = 255 and b = 127 on a K pair: 2*255*127 = 64770 > 32767 saturates in
+    # full 4x8 tiles (kernel_avx2_i8.rs:97-117); the edge tile stays exact.
+    m, n, k = 5, 9, 4
+    a = np.full((m, k), 255, np.uint8)
+    b = np.full((k, n), 127, np.int8)
+    exact = oracle.gemm_i8(a, b, variant="vnni")
+    sat = oracle.gemm_i8(a, b, variant="avx2")
+    assert np.all(exact == 4 * 255 * 127)
+    assert np.all(sat[:4, :8] == 2 * 32767)
+    assert np.all(sat[4, :] == exact[4, :]) and np.all(sat[:, 8] == exact[:, 8])
+
+
+def test_dd_exact_small(oracle):
+    rng = np.random.default_rng(0)
+    a = rng.uniform(-1, 1, (6, 9))
+    b = rng.uniform(-1, 1, (9, 5))
+    dd = oracle.dd_full(a, b)
+    for i in range(6):
+        for j in range(5):
+            exact = sum(Fraction(a[i, p]) * Fraction(b[p, j]) for p in range(9))
+            assert dd[i, j] == float(exact)
+
+
+def test_dd_complex_and_f32(oracle):
+    rng = np.random.default_rng(1)
+    a = (rng.standard_normal((7, 11)) + 1j * rng.standard_normal((7, 11)))
+    b = (rng.standard_normal((11, 4)) + 1j * rng.standard_normal((11, 4)))
+    dd = oracle.dd_full(a, b)
+    assert np.max(np.abs(dd - a @ b)) < 1e-13
+    af = a.astype(np.complex64)
+    bf = b.astype(np.complex64)
+    ddf = oracle.dd_full(af, bf)
+    want = af.astype(np.complex128) @ bf.astype(np.complex128)
+    assert np.max(np.abs(ddf - want)) < 1e-13
+
+
+@pytest.mark.parametrize("m,n,k", [(17, 13, 9), (8, 6, 300), (129, 65, 513)])
+def test_restatement_close_to_dd(oracle, m, n, k):
+    rng = np.random.default_rng(m)
+    a = rng.uniform(-1, 1, (m, k))
+    b = rng.uniform(-1, 1, (k, n))
+    c = oracle.gemm_f64(a, b)
+    assert oracle.error_vs_dd(a, b, c) <= k * 2.0 ** -53
+    af, bf = a.astype(np.float32), b.astype(np.float32)
+    assert oracle.error_vs_dd(af, bf, oracle.gemm_f32(af, bf)) <= k * 2.0 ** -24
+
+
+def test_restatement_panel_summation_order(oracle):
+    # K = 300 spans two KC=256 panels: C = chain(0..256) + chain(256..300),
+    # each chain a fused-multiply-add recurrence from zero (outer.rs:415-421).
+    rng = np.random.default_rng(7)
+    m, n, k = 8, 16, 300
+    a = rng.uniform(-1, 1, (m, k))
+    b = rng.uniform(-1, 1, (k, n))
+    got = oracle.gemm_f64(a, b)
+    import ctypes
+    libm = ctypes.CDLL("libm.so.6")
+    libm.fma.restype = ctypes.c_double
+    libm.fma.argtypes = [ctypes.c_double] * 3
+    for i in (0, 5):
+        for j in (0, 11):
+            p1 = 0.0
+            for p in range(256):
+                p1 = libm.fma(a[i, p], b[p, j], p1)
+            p2 = 0.0
+            for p in range(256, 300):
+                p2 = libm.fma(a[i, p], b[p, j], p2)
+            assert got[i, j] == p1 + p2
+
+
+def test_alpha_beta_rules(oracle):
+    rng = np.random.default_rng(3)
+    m, n, k = 9, 17, 20
+    a, b = rng.uniform(-1, 1, (m, k)), rng.uniform(-1, 1, (k, n))
+    c0 = rng.uniform(-1, 1, (m, n))
+    got = oracle.gemm_f64(a, b, alpha=0.5, beta=2.0, c=c0)
+    assert np.max(np.abs(got - (0.5 * (a @ b) + 2.0 * c0))) < 1e-13
+    # k == 0: C = beta * C (outer.rs:213-229)
+    z = oracle.gemm_f64(np.zeros((m, 0)), np.zeros((0, n)), beta=3.0, c=c0)
+    assert np.array_equal(z, 3.0 * c0)
+
+
+def test_normwise_sampling_consistent(oracle):
+    rng = np.random.default_rng(5)
+    m, n, k = 300, 280, 64
+    a, b = rng.uniform(-1, 1, (m, k)), rng.uniform(-1, 1, (k, n))
+    c = (a.astype(np.float32) @ b.astype(np.float32)).astype(np.float64)
+    full = oracle.normwise_error(c, oracle.dd_full(a, b), m, n, oracle.fro(a), oracle.fro(b))
+    sampled = oracle.error_vs_dd(a, b, c)
+    assert 0.5 < sampled / full < 2.0
