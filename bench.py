@@ -1,0 +1,367 @@
+#!/usr/bin/env python
+"""Benchmark of the ferray B200 GEMM backend.
+
+Workload (one "step"): one SGEMM C = A @ B at M = N = K = 8192, f32 operands
+drawn N(0,1) from seed 42, in the split form (3 x BF16 products on tcgen05
+with FP32 accumulation).  The same step in the plain form (FFMA) is timed
+beside it.  Inputs are 256 MiB each, larger than the 126 MB L2, so no flush
+is needed between steps.
+
+`value` = TFLOP/s of the split step with operands resident in HBM (2*N^3
+credited flops, the flops of the emulated SGEMM), timed with CUDA events on
+the launching stream, max over ranks.  `e2e` = the same metric through the
+host-pointer C-ABI entry point fg_gemm_f32_host (host->device copies of A and
+B and the device->host copy of C inside the timed region, pinned host
+memory).
+
+`--impl reference` times ferray's own CPU SGEMM (the restatement in
+oracle/ferray_cpu.c; the reference is Rust and cannot be built here) on all
+host threads, on a bounded row sample of the same workload.
+
+Multi-GPU (torchrun, --gpus N): every rank runs the same workload on its own
+GPU (independent replicas: GEMM problems shard across GPUs with no exchange),
+so scaling is weak; value = all ranks' flops / max-over-ranks time.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_DEFAULT = 8192
+SEED = 42
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("bf16_tflops", 1590.0), d.get("hbm_gbs", 6650.0), "measured"
+    return 1590.0, 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def reference_arm(args):
+    """ferray's CPU SGEMM (restated) on the host cores, bounded row sample."""
+    rank, _, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle
+    n = args.n
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    rng = np.random.default_rng(SEED)
+    b = rng.standard_normal((n, n), dtype=np.float32)
+    rows = 64
+    a = rng.standard_normal((rows, n), dtype=np.float32)
+    t0 = time.perf_counter()
+    oracle.gemm_f32(a, b)
+    dt = time.perf_counter() - t0
+    # one step ~ 2 s of CPU work
+    rows = int(max(64, min(n, rows * 2.0 / max(dt, 1e-3))) // 16 * 16)
+    a = rng.standard_normal((rows, n), dtype=np.float32)
+    for _ in range(args.warmup):
+        oracle.gemm_f32(a, b)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.gemm_f32(a, b)
+        times.append(time.perf_counter() - t0)
+    t = float(np.median(times))
+    val = 2.0 * rows * n * n / t / 1e12
+    out = {
+        "metric": "SGEMM TFLOP/s, split 3xBF16 vs plain FFMA, M=N=K=%d (normwise error vs FP64 DD oracle)" % n,
+        "value": round(val, 4), "unit": "TFLOP/s", "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t * 1e3 * n / rows, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic N(0,1), seed 42",
+        "config": {"workload": "sgemm_f32_%d_split_vs_plain" % n, "m": n, "n": n, "k": n,
+                   "sample_rows": rows},
+        "cpu_baseline": {"value": round(val, 4), "unit": "TFLOP/s", "cores": threads,
+                         "kind": "port",
+                         "sample": "%d of %d rows of C (full N, full K) per step" % (rows, n)},
+        "e2e": {"value": round(val, 4), "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def cpu_baseline(n):
+    """Oracle port of ferray's SGEMM on the host: a ~10 s bounded sample."""
+    import oracle
+    threads = min(os.cpu_count() or 1, 8)  # ferray's GEMM pool size (outer.rs:142-155)
+    oracle.set_threads(threads)
+    rng = np.random.default_rng(SEED + 1)
+    b = rng.standard_normal((n, n), dtype=np.float32)
+    rows = 32
+    a = rng.standard_normal((rows, n), dtype=np.float32)
+    t0 = time.perf_counter()
+    oracle.gemm_f32(a, b)
+    dt = time.perf_counter() - t0
+    rows = int(max(32, min(n, rows * 10.0 / max(dt, 1e-3))) // 16 * 16)
+    a = rng.standard_normal((rows, n), dtype=np.float32)
+    t0 = time.perf_counter()
+    oracle.gemm_f32(a, b)
+    dt = time.perf_counter() - t0
+    return {"value": round(2.0 * rows * n * n / dt / 1e12, 4), "unit": "TFLOP/s",
+            "cores": threads, "kind": "port",
+            "sample": "%d of %d rows of C at N=K=%d, %.1f s" % (rows, n, n, dt)}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+    rank, world, local = dist_env()
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    import ferray_b200 as fg
+    from ferray_b200 import _lib as L
+    ctx = fg.Context(local)
+    lib = ctx._lib
+    n = args.n
+    rng = np.random.default_rng(SEED + rank)
+    a_h = rng.standard_normal((n, n), dtype=np.float32)
+    b_h = rng.standard_normal((n, n), dtype=np.float32)
+    da = fg.DeviceArray.from_numpy(a_h, ctx)
+    db = fg.DeviceArray.from_numpy(b_h, ctx)
+    dc = fg.DeviceArray((n, n), np.float32, ctx)
+    stream = torch.cuda.Stream()
+    sh = C.c_void_p(stream.cuda_stream)
+
+    def step(mode):
+        st = lib.fg_gemm_f32(ctx.handle, mode, n, n, n, 1.0, da.ptr, db.ptr, 0.0, dc.ptr, sh)
+        if st != 0:
+            raise RuntimeError(lib.fg_last_error().decode())
+
+    def timed(mode, steps, warmup):
+        for _ in range(warmup):
+            step(mode)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        lc0 = fg.launch_count()
+        lib.fg_profile_enable(1)
+        e0.record(stream)
+        for _ in range(steps):
+            step(mode)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        lib.fg_profile_enable(0)
+        ents = (L.fg_profile_entry * 16)()
+        cnt = C.c_int()
+        lib.fg_profile_collect(ents, 16, C.byref(cnt))
+        prof = {ents[i].name.decode(): (ents[i].launches, ents[i].total_ms)
+                for i in range(cnt.value)}
+        launches = fg.launch_count() - lc0
+        ms = e0.elapsed_time(e1) / steps
+        if dist:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+            dist.barrier()
+        return ms, launches, prof
+
+    ctx.sync()
+    sampler = ClockSampler(local)
+    sampler.start()
+    ms_split, launches, prof_split = timed(L.FG_MODE_SPLIT, args.steps, args.warmup)
+    clocks = sampler.stop()
+    ms_plain, _, _ = timed(L.FG_MODE_PLAIN, max(2, args.steps // 3), 2)
+    ctx.sync()
+
+    # accuracy of both forms vs the double-double oracle (sampled rows x cols)
+    import oracle
+    rows, cols = oracle.sample_indices(n, n, 96, 96, seed=7)
+    ref = oracle.dd_sampled(a_h, b_h, rows, cols)
+    na, nb = oracle.fro(a_h), oracle.fro(b_h)
+    step(L.FG_MODE_SPLIT)
+    torch.cuda.synchronize()
+    c_split = dc.to_numpy()[np.ix_(rows, cols)]
+    step(L.FG_MODE_PLAIN)
+    torch.cuda.synchronize()
+    c_plain = dc.to_numpy()[np.ix_(rows, cols)]
+    err_split = oracle.normwise_error(c_split, ref, n, n, na, nb)
+    err_plain = oracle.normwise_error(c_plain, ref, n, n, na, nb)
+
+    flops = 2.0 * n ** 3
+    tf_split = flops / (ms_split * 1e-3) / 1e12
+    tf_plain = flops / (ms_plain * 1e-3) / 1e12
+
+    # e2e through the host-pointer C ABI (pinned host buffers)
+    e2e = None
+    if not args.no_e2e:
+        c_h = np.empty((n, n), np.float32)
+        for arr in (a_h, b_h, c_h):
+            lib.fg_host_register(ctx.handle, arr.ctypes.data, arr.nbytes)
+        for _ in range(2):
+            lib.fg_gemm_f32_host(ctx.handle, L.FG_MODE_SPLIT, n, n, n, 1.0, a_h.ctypes.data,
+                                 b_h.ctypes.data, 0.0, c_h.ctypes.data)
+        if dist:
+            dist.barrier()
+        k = max(3, args.steps // 2)
+        t0 = time.perf_counter()
+        for _ in range(k):
+            st = lib.fg_gemm_f32_host(ctx.handle, L.FG_MODE_SPLIT, n, n, n, 1.0, a_h.ctypes.data,
+                                      b_h.ctypes.data, 0.0, c_h.ctypes.data)
+            assert st == 0, lib.fg_last_error()
+        dt = (time.perf_counter() - t0) / k
+        if dist:
+            t = torch.tensor([dt], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t.item())
+        for arr in (a_h, b_h, c_h):
+            lib.fg_host_unregister(ctx.handle, arr.ctypes.data)
+        e2e = {"value": round(world * flops / dt / 1e12, 3), "unit": "TFLOP/s",
+               "h2d_bytes_per_step": int(a_h.nbytes + b_h.nbytes),
+               "d2h_bytes_per_step": int(c_h.nbytes), "ms_per_step": round(dt * 1e3, 3)}
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    bf16_peak, _, peak_src = peaks()
+    kname = "tc_gemm_3xbf16"
+    kl, kms = prof_split.get(kname, (0, 0.0))
+    k_avg_ms = kms / kl if kl else None
+    achieved = flops / (k_avg_ms * 1e-3) / 1e12 if k_avg_ms else None
+    roofline = {
+        "bound": "tensor", "kernel": kname,
+        "achieved": round(achieved, 2) if achieved else None,
+        "peak": bf16_peak, "unit": "TFLOP/s",
+        "frac": round(achieved / bf16_peak, 4) if achieved else None,
+        "peak_source": peak_src + " bf16 burst (MEASURED_PEAKS.json)",
+        "tensor_pipe_frac": round(3 * achieved / bf16_peak, 4) if achieved else None,
+        "note": "achieved credits the 2*N^3 flops of the emulated SGEMM; the kernel issues "
+                "3 BF16 products per output, so its tensor-pipe rate is 3x achieved",
+        "kernel_ms": round(k_avg_ms, 4) if k_avg_ms else None,
+        "traffic": None,
+    }
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            tr = json.load(open(tpath)).get(kname, {})
+            if tr.get("n") == n:
+                roofline["traffic"] = tr.get("dram_bytes_per_launch")
+        except Exception:
+            pass
+    out = {
+        "metric": "SGEMM TFLOP/s, split 3xBF16 vs plain FFMA, M=N=K=%d (normwise error vs FP64 DD oracle)" % n,
+        "value": round(world * flops / (ms_split * 1e-3) / 1e12, 3),
+        "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms_split, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (3xbf16 split, f32 accumulate)",
+        "data": "synthetic N(0,1), seed 42",
+        "config": {"workload": "sgemm_f32_%d_split_vs_plain" % n, "m": n, "n": n, "k": n,
+                   "l2": "inputs (256 MiB each) larger than L2, no flush",
+                   "parallelism": "replicas x%d" % world},
+        "split": {"tflops": round(tf_split, 3), "ms": round(ms_split, 4),
+                  "normwise_err": err_split},
+        "plain": {"tflops": round(tf_plain, 3), "ms": round(ms_plain, 4),
+                  "normwise_err": err_plain, "kernel": "simt_sgemm"},
+        "split_over_plain": round(tf_split / tf_plain, 3),
+        "err_split_over_plain": round(err_split / err_plain, 3) if err_plain else None,
+        "roofline": roofline,
+        "kernels": {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in prof_split.items()},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "e2e": e2e,
+    }
+    if not args.no_cpu and world == 1:
+        out["cpu_baseline"] = cpu_baseline(n)
+    print(json.dumps(out), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

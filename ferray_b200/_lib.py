@@ -47,6 +47,10 @@ class fg_server_stats(C.Structure):
                 ("hbm_peak", C.c_size_t)]
 
 
+class fg_profile_entry(C.Structure):
+    _fields_ = [("name", C.c_char * 48), ("launches", C.c_uint64), ("total_ms", C.c_double)]
+
+
 # Every exported symbol with (restype, argtypes); also the list the
 # "library exports every declared symbol" test checks against the header.
 _p, _sz, _i, _i64, _u64, _d, _f = (C.c_void_p, C.c_size_t, C.c_int, C.c_int64, C.c_uint64,
@@ -58,6 +62,8 @@ SIGNATURES = {
     "fg_status_string": (C.c_char_p, [_i]),
     "fg_last_error": (C.c_char_p, []),
     "fg_launch_count": (_u64, []),
+    "fg_profile_enable": (_i, [_i]),
+    "fg_profile_collect": (_i, [C.POINTER(fg_profile_entry), _i, C.POINTER(_i)]),
     "fg_device_info": (_i, [_p, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(_sz)]),
     "fg_buffer_alloc": (_i, [_p, _sz, C.POINTER(_p)]),
     "fg_buffer_free": (_i, [_p, _p]),

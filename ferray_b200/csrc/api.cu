@@ -16,6 +16,19 @@ namespace fgrt {
 using fg::scale_kernel;
 
 std::atomic<uint64_t> g_launches{0};
+std::atomic<int> g_prof_on{0};
+
+struct ProfRec {
+    std::string fam;
+    cudaEvent_t e0, e1;
+};
+static std::mutex g_prof_mu;
+static std::vector<ProfRec> g_prof;
+
+void prof_record(const char* family, cudaEvent_t start, cudaEvent_t stop) {
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    g_prof.push_back(ProfRec{family, start, stop});
+}
 static thread_local std::string t_last_error;
 
 fg_status set_error(fg_status s, const std::string& msg) {
@@ -176,6 +189,45 @@ const char* fg_status_string(fg_status s) {
 const char* fg_last_error(void) { return t_last_error.c_str(); }
 
 uint64_t fg_launch_count(void) { return g_launches.load(); }
+
+fg_status fg_profile_enable(int on) {
+    g_prof_on.store(on ? 1 : 0);
+    return FG_OK;
+}
+
+fg_status fg_profile_collect(fg_profile_entry* out, int capacity, int* count) {
+    std::vector<ProfRec> recs;
+    {
+        std::lock_guard<std::mutex> lk(g_prof_mu);
+        recs.swap(g_prof);
+    }
+    std::vector<fg_profile_entry> agg;
+    fg_status st = FG_OK;
+    for (auto& r : recs) {
+        float ms = 0.f;
+        if (cudaEventSynchronize(r.e1) != cudaSuccess || cudaEventElapsedTime(&ms, r.e0, r.e1) != cudaSuccess)
+            st = set_error(FG_ERR_DEVICE, "profile event failed");
+        cudaEventDestroy(r.e0);
+        cudaEventDestroy(r.e1);
+        fg_profile_entry* e = nullptr;
+        for (auto& x : agg)
+            if (r.fam == x.name) e = &x;
+        if (!e) {
+            agg.push_back(fg_profile_entry{});
+            e = &agg.back();
+            std::strncpy(e->name, r.fam.c_str(), sizeof(e->name) - 1);
+        }
+        e->launches += 1;
+        e->total_ms += ms;
+    }
+    int n = 0;
+    for (auto& x : agg) {
+        if (out && n < capacity) out[n] = x;
+        ++n;
+    }
+    if (count) *count = n;
+    return st;
+}
 
 fg_status fg_init(int device, fg_ctx** out) {
     if (!out) return set_error(FG_ERR_INVALID, "out is null");

@@ -24,6 +24,8 @@ fg_status launch_simt(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
     (void)ctx;
     const BatchMap bm = batch_map(g);
     if (g.batch > 65535) return set_error(FG_ERR_UNSUPPORTED, "batch above 65535");
+    static const char* names[] = {"simt_dgemm", "simt_sgemm", "simt_zgemm", "simt_cgemm"};
+    ProfScope prof(g.dtype <= FG_C32 ? names[g.dtype] : "simt", st);
     switch (g.dtype) {
         case FG_F64: {
             dim3 grid((g.N + 127) / 128, (g.M + 127) / 128, g.batch);

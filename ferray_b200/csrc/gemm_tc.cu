@@ -7,6 +7,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <vector>
 
 #include "prep_kernels.cuh"
@@ -20,9 +21,26 @@ using namespace fg;
 using CfgI8 = TcCfg<KIND_I8, 256, 4, 1, 1, 1, 1, EPI_I32>;
 using CfgQmm = TcCfg<KIND_I8, 256, 4, 1, 1, 1, 1, EPI_QMM>;
 using CfgI16 = TcCfg<KIND_I8, 128, 3, 2, 2, 3, 4, EPI_I16>;
-using CfgBf16x3 = TcCfg<KIND_BF16, 256, 2, 2, 2, 1, 3, EPI_F32>;
+using CfgBf16x3 = TcCfg<KIND_BF16, 128, 3, 2, 2, 1, 3, EPI_F32, 1>;
+
+// K blocks (64 bf16 each) per TMEM accumulation chunk of the split SGEMM.
+static int split_kchunk() {
+    static int v = [] {
+        const char* e = getenv("FG_SPLIT_KCHUNK");
+        return e ? atoi(e) : 4;
+    }();
+    return v;
+}
 
 static unsigned long long kTimeoutNs = 4000000000ull;  // 4 s per wait
+
+template <class Cfg>
+static const char* cfg_name() {
+    if (Cfg::KIND == KIND_BF16) return "tc_gemm_3xbf16";
+    if (Cfg::EPI == EPI_I16) return "tc_gemm_i16";
+    if (Cfg::EPI == EPI_QMM) return "tc_gemm_qmm";
+    return "tc_gemm_i8";
+}
 
 template <class Cfg>
 static fg_status launch_cfg(fg_ctx* ctx, const TcMaps& maps, TcArgs& args, cudaStream_t st) {
@@ -38,7 +56,9 @@ static fg_status launch_cfg(fg_ctx* ctx, const TcMaps& maps, TcArgs& args, cudaS
     const long long tiles = (long long)args.batch * args.tiles_m * args.tiles_n;
     if (tiles == 0) return FG_OK;
     const int grid = static_cast<int>(std::min<long long>(tiles, ctx->sm_count));
+    ProfScope prof(cfg_name<Cfg>(), st);
     tc_gemm_kernel<Cfg><<<grid, Cfg::THREADS, tc_smem_bytes<Cfg>(), st>>>(maps, args);
+    prof.stop();
     count_launch();
     FG_CUDA(cudaGetLastError());
     return FG_OK;
@@ -322,6 +342,7 @@ fg_status launch_split_bf16(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
         args.cplx_half = static_cast<int>(g.N);
         args.ldc = 2 * g.ldc;
     }
+    args.kchunk = split_kchunk();
     args.ops[0] = TcOp{1, 0, 0, 1, 1};  // lo * hi
     args.ops[1] = TcOp{0, 1, 0, 1, 1};  // hi * lo
     args.ops[2] = TcOp{0, 0, 0, 1, 1};  // hi * hi

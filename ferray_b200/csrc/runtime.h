@@ -48,6 +48,31 @@ inline cudaStream_t stream_of(fg_ctx* ctx, fg_stream s) {
 
 inline void count_launch(uint64_t n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+// Optional per-family kernel timing (fg_profile_enable).  Usage:
+//   ProfScope ps("family", stream); launch<<<...>>>; ps.stop();
+extern std::atomic<int> g_prof_on;
+void prof_record(const char* family, cudaEvent_t start, cudaEvent_t stop);
+struct ProfScope {
+    const char* fam;
+    cudaStream_t st;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    ProfScope(const char* family, cudaStream_t stream) : fam(family), st(stream) {
+        if (g_prof_on.load(std::memory_order_relaxed)) {
+            cudaEventCreate(&e0);
+            cudaEventCreate(&e1);
+            cudaEventRecord(e0, st);
+        }
+    }
+    void stop() {
+        if (e0) {
+            cudaEventRecord(e1, st);
+            prof_record(fam, e0, e1);
+            e0 = e1 = nullptr;
+        }
+    }
+    ~ProfScope() { stop(); }
+};
+
 // Stream-ordered scratch: freed on the same stream after the kernels that
 // use it, so concurrent calls on other streams never share it.
 struct Scratch {

@@ -42,9 +42,13 @@ struct TcOp {
     int a_fmt, b_fmt;  // kind::i8: 0 = u8, 1 = s8; kind::f16: 1 = bf16
 };
 
-template <int KIND_, int BN_, int STAGES_, int NA_, int NB_, int NACC_, int NOPS_, int EPI_>
+template <int KIND_, int BN_, int STAGES_, int NA_, int NB_, int NACC_, int NOPS_, int EPI_,
+          int CHUNKED_ = 0>
 struct TcCfg {
     static constexpr int KIND = KIND_, BM = 128, BN = BN_, STAGES = STAGES_;
+    // CHUNKED: K is accumulated in TMEM in chunks of p.kchunk blocks that the
+    // epilogue sums in FP32 registers (EPI_F32 only).
+    static constexpr int CHUNKED = CHUNKED_;
     static constexpr int NA = NA_, NB = NB_, NACC = NACC_, NOPS = NOPS_, EPI = EPI_;
     static constexpr int ESIZE = KIND == KIND_I8 ? 1 : 2;  // operand bytes
     static constexpr int BK_BYTES = 128;
@@ -58,7 +62,7 @@ struct TcCfg {
     static constexpr int B_CHUNK_BYTES = BK * 128;
     static constexpr int STAGE_BYTES = NA * A_TILE + NB * B_TILE;
     static constexpr int ACC_COLS = NACC * BN;
-    static constexpr int ACC_BUFS = (2 * ACC_COLS <= 512) ? 2 : 1;
+    static constexpr int ACC_BUFS = (4 * ACC_COLS <= 512) ? 4 : (2 * ACC_COLS <= 512) ? 2 : 1;
     static constexpr int TMEM_COLS = 512;
     static constexpr int THREADS = 192;
     static_assert(ACC_COLS <= 512, "accumulators exceed TMEM");
@@ -91,6 +95,7 @@ struct TcArgs {
     const int* col_sum;
     int a_zp, b_zp;
     float scale;
+    int kchunk;                // CHUNKED configs: K blocks per TMEM chunk
     TcOp ops[TC_MAX_OPS];
     DevStatus* status;
     unsigned long long timeout_ns;
@@ -131,8 +136,8 @@ struct TcSmem {
     alignas(1024) uint8_t b[Cfg::STAGES][Cfg::NB][Cfg::B_TILE];
     uint64_t full[Cfg::STAGES];
     uint64_t empty[Cfg::STAGES];
-    uint64_t acc_full[2];
-    uint64_t acc_empty[2];
+    uint64_t acc_full[4];
+    uint64_t acc_empty[4];
     uint64_t drain;
     uint32_t tmem_base;
     int abort;
@@ -249,7 +254,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
             mbar_init(&s.full[i], 1);
             mbar_init(&s.empty[i], 1);
         }
-        for (int i = 0; i < 2; ++i) {
+        for (int i = 0; i < 4; ++i) {
             mbar_init(&s.acc_full[i], 1);
             mbar_init(&s.acc_empty[i], 4);  // one arrive per epilogue warp
         }
@@ -329,55 +334,59 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
         if (elect_one()) {
             int stage = 0;
             uint32_t phase = 0;
-            int it = 0;
+            int it = 0;  // accumulator units (tile x K chunk) issued so far
             bool ok = true;
-            for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x, ++it) {
-                const int buf = it % Cfg::ACC_BUFS;
-                const uint32_t acc_par = static_cast<uint32_t>((it / Cfg::ACC_BUFS) & 1);
-                if (!mbar_wait(&s.acc_empty[buf], acc_par ^ 1u, p.timeout_ns, p.status, 0x11, abort)) {
-                    ok = false;
-                    break;
-                }
-                tc_fence_after();
-                const uint32_t acc_base = tmem + buf * Cfg::ACC_COLS;
-                for (int kb = 0; kb < p.k_blocks; ++kb) {
-                    if (!mbar_wait(&s.full[stage], phase, p.timeout_ns, p.status, 0x12, abort)) {
+            const int kchunk = (Cfg::CHUNKED && p.kchunk > 0) ? p.kchunk : p.k_blocks;
+            for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x) {
+                for (int kc0 = 0; kc0 < p.k_blocks && ok; kc0 += kchunk, ++it) {
+                    const int kc1 = min(p.k_blocks, kc0 + kchunk);
+                    const int buf = it % Cfg::ACC_BUFS;
+                    const uint32_t acc_par = static_cast<uint32_t>((it / Cfg::ACC_BUFS) & 1);
+                    if (!mbar_wait(&s.acc_empty[buf], acc_par ^ 1u, p.timeout_ns, p.status, 0x11, abort)) {
                         ok = false;
                         break;
                     }
                     tc_fence_after();
+                    const uint32_t acc_base = tmem + buf * Cfg::ACC_COLS;
+                    for (int kb = kc0; kb < kc1; ++kb) {
+                        if (!mbar_wait(&s.full[stage], phase, p.timeout_ns, p.status, 0x12, abort)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
 #pragma unroll
-                    for (int o = 0; o < Cfg::NOPS; ++o) {
-                        const TcOp op = p.ops[o];
-                        // first product into this accumulator in the tile?
-                        bool first_for_acc = true;
+                        for (int o = 0; o < Cfg::NOPS; ++o) {
+                            const TcOp op = p.ops[o];
+                            // first product into this accumulator in the unit?
+                            bool first_for_acc = true;
 #pragma unroll
-                        for (int q = 0; q < o; ++q)
-                            if (p.ops[q].acc == op.acc) first_for_acc = false;
-                        const uint32_t idesc = umma_idesc(Cfg::KIND == KIND_I8 ? 2u : 1u,
-                                                          op.a_fmt, op.b_fmt, 0u, 1u, Cfg::BM, Cfg::BN);
-                        const uint32_t a_addr = smem_u32(s.a[stage][op.a]);
-                        const uint32_t b_addr = smem_u32(s.b[stage][op.b]);
+                            for (int q = 0; q < o; ++q)
+                                if (p.ops[q].acc == op.acc) first_for_acc = false;
+                            const uint32_t idesc = umma_idesc(Cfg::KIND == KIND_I8 ? 2u : 1u,
+                                                              op.a_fmt, op.b_fmt, 0u, 1u, Cfg::BM, Cfg::BN);
+                            const uint32_t a_addr = smem_u32(s.a[stage][op.a]);
+                            const uint32_t b_addr = smem_u32(s.b[stage][op.b]);
 #pragma unroll
-                        for (int kk = 0; kk < Cfg::KSTEPS; ++kk) {
-                            const uint64_t ad = umma_desc_sw128(a_addr + kk * Cfg::KSTEP_BYTES, 16, 1024);
-                            const uint64_t bd = umma_desc_sw128(
-                                b_addr + kk * (Cfg::KSTEP_BYTES / Cfg::ESIZE) * 128, Cfg::B_CHUNK_BYTES, 1024);
-                            const uint32_t acc = (kb > 0 || kk > 0 || !first_for_acc) ? 1u : 0u;
-                            if constexpr (Cfg::KIND == KIND_I8)
-                                tc_mma_i8(acc_base + op.acc * Cfg::BN, ad, bd, idesc, acc);
-                            else
-                                tc_mma_f16(acc_base + op.acc * Cfg::BN, ad, bd, idesc, acc);
+                            for (int kk = 0; kk < Cfg::KSTEPS; ++kk) {
+                                const uint64_t ad = umma_desc_sw128(a_addr + kk * Cfg::KSTEP_BYTES, 16, 1024);
+                                const uint64_t bd = umma_desc_sw128(
+                                    b_addr + kk * (Cfg::KSTEP_BYTES / Cfg::ESIZE) * 128, Cfg::B_CHUNK_BYTES, 1024);
+                                const uint32_t acc = (kb > kc0 || kk > 0 || !first_for_acc) ? 1u : 0u;
+                                if constexpr (Cfg::KIND == KIND_I8)
+                                    tc_mma_i8(acc_base + op.acc * Cfg::BN, ad, bd, idesc, acc);
+                                else
+                                    tc_mma_f16(acc_base + op.acc * Cfg::BN, ad, bd, idesc, acc);
+                            }
+                        }
+                        tc_commit(&s.empty[stage]);
+                        if (++stage == Cfg::STAGES) {
+                            stage = 0;
+                            phase ^= 1u;
                         }
                     }
-                    tc_commit(&s.empty[stage]);
-                    if (++stage == Cfg::STAGES) {
-                        stage = 0;
-                        phase ^= 1u;
-                    }
+                    if (!ok) break;
+                    tc_commit(&s.acc_full[buf]);
                 }
-                if (!ok) break;
-                tc_commit(&s.acc_full[buf]);
             }
             // Every MMA issued above has completed once `drain` flips.
             tc_commit(&s.drain);
@@ -388,26 +397,74 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
         // ------------------------------------------------ epilogue
         const int ew = warp & 3;  // TMEM lane quarter this warp may access
         int it = 0;
-        for (int t = blockIdx.x; t < total_tiles; t += gridDim.x, ++it) {
-            const int buf = it % Cfg::ACC_BUFS;
-            const uint32_t acc_par = static_cast<uint32_t>((it / Cfg::ACC_BUFS) & 1);
-            if (!mbar_wait(&s.acc_full[buf], acc_par, p.timeout_ns, p.status, 0x21, abort)) break;
-            tc_fence_after();
-            int bz, tm, tn;
-            tile_coords(p, t, bz, tm, tn);
-            const int grow = tm * Cfg::BM + ew * 32 + lane;
-            const uint32_t row_addr = tmem + (static_cast<uint32_t>(ew * 32) << 16) + buf * Cfg::ACC_COLS;
-#pragma unroll 1
-            for (int c = 0; c < Cfg::BN / 32; ++c) {
-                uint32_t v[Cfg::NACC][32];
+        if constexpr (Cfg::CHUNKED) {
+            // Tensor-core FP32 accumulation truncates at every MMA, so long K
+            // runs drift.  Each K chunk is accumulated in TMEM from zero and
+            // the chunk sums are added here in FP32 registers with
+            // round-to-nearest.
+            const int kchunk = p.kchunk > 0 ? p.kchunk : p.k_blocks;
+            bool ok = true;
+            for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x) {
+                float run[Cfg::BN];
 #pragma unroll
-                for (int a = 0; a < Cfg::NACC; ++a) tmem_ld_32x32b_x32(row_addr + a * Cfg::BN + c * 32, v[a]);
-                tmem_wait_ld();
-                epilogue_store<Cfg>(p, bz, grow, tn * Cfg::BN + c * 32, v);
+                for (int j = 0; j < Cfg::BN; ++j) run[j] = 0.f;
+                for (int kc0 = 0; kc0 < p.k_blocks; kc0 += kchunk, ++it) {
+                    const int buf = it % Cfg::ACC_BUFS;
+                    const uint32_t acc_par = static_cast<uint32_t>((it / Cfg::ACC_BUFS) & 1);
+                    if (!mbar_wait(&s.acc_full[buf], acc_par, p.timeout_ns, p.status, 0x21, abort)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t row_addr =
+                        tmem + (static_cast<uint32_t>(ew * 32) << 16) + buf * Cfg::ACC_COLS;
+#pragma unroll
+                    for (int c = 0; c < Cfg::BN / 32; ++c) {
+                        uint32_t v[32];
+                        tmem_ld_32x32b_x32(row_addr + c * 32, v);
+                        tmem_wait_ld();
+#pragma unroll
+                        for (int j = 0; j < 32; ++j)
+                            run[c * 32 + j] = __fadd_rn(run[c * 32 + j], __uint_as_float(v[j]));
+                    }
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&s.acc_empty[buf]);
+                }
+                if (!ok) break;
+                int bz, tm, tn;
+                tile_coords(p, t, bz, tm, tn);
+                const int grow = tm * Cfg::BM + ew * 32 + lane;
+#pragma unroll
+                for (int c = 0; c < Cfg::BN / 32; ++c) {
+                    uint32_t v[Cfg::NACC][32];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) v[0][j] = __float_as_uint(run[c * 32 + j]);
+                    epilogue_store<Cfg>(p, bz, grow, tn * Cfg::BN + c * 32, v);
+                }
             }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&s.acc_empty[buf]);
+        } else {
+            for (int t = blockIdx.x; t < total_tiles; t += gridDim.x, ++it) {
+                const int buf = it % Cfg::ACC_BUFS;
+                const uint32_t acc_par = static_cast<uint32_t>((it / Cfg::ACC_BUFS) & 1);
+                if (!mbar_wait(&s.acc_full[buf], acc_par, p.timeout_ns, p.status, 0x21, abort)) break;
+                tc_fence_after();
+                int bz, tm, tn;
+                tile_coords(p, t, bz, tm, tn);
+                const int grow = tm * Cfg::BM + ew * 32 + lane;
+                const uint32_t row_addr = tmem + (static_cast<uint32_t>(ew * 32) << 16) + buf * Cfg::ACC_COLS;
+#pragma unroll 1
+                for (int c = 0; c < Cfg::BN / 32; ++c) {
+                    uint32_t v[Cfg::NACC][32];
+#pragma unroll
+                    for (int a = 0; a < Cfg::NACC; ++a) tmem_ld_32x32b_x32(row_addr + a * Cfg::BN + c * 32, v[a]);
+                    tmem_wait_ld();
+                    epilogue_store<Cfg>(p, bz, grow, tn * Cfg::BN + c * 32, v);
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&s.acc_empty[buf]);
+            }
         }
     }
 

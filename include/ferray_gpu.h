@@ -87,6 +87,18 @@ const char *fg_status_string(fg_status s);
 const char *fg_last_error(void);
 /* Number of kernels this library has launched in the process. */
 uint64_t fg_launch_count(void);
+/* Kernel timing for roofline bookkeeping (no reference counterpart; ferray
+ * has no tracing).  While enabled, every main GEMM kernel launch is
+ * bracketed by CUDA events on its own stream; fg_profile_collect waits for
+ * them and returns per-kernel-family launch counts and summed device time,
+ * then clears the records. */
+typedef struct fg_profile_entry {
+    char name[48];
+    uint64_t launches;
+    double total_ms;
+} fg_profile_entry;
+fg_status fg_profile_enable(int on);
+fg_status fg_profile_collect(fg_profile_entry *out, int capacity, int *count);
 /* Device properties used for roofline bookkeeping. */
 fg_status fg_device_info(fg_ctx *ctx, int *sm_count, int *cc_major, int *cc_minor,
                          size_t *hbm_bytes);
