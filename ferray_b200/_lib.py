@@ -80,6 +80,8 @@ SIGNATURES = {
     "fg_gemm_i16": (_i, [_p, _sz, _sz, _sz, _p, _p, _p, _i, _p]),
     "fg_quantized_matmul": (_i, [_p, _sz, _sz, _sz, _p, C.c_uint8, _f, _p, C.c_int8, _f, _p,
                                  _i, _p]),
+    "fg_quantized_matmul_noalloc": (_i, [_p, _sz, _sz, _sz, _p, C.c_uint8, _f, _p, C.c_int8, _f,
+                                         _p, _i, _p]),
     "fg_gemm": (_i, [_p, _i, _i, _i, _sz, _sz, _sz, _p, _p, _sz, _p, _sz, _p, _p, _sz, _i, _p]),
     "fg_gemm_f64_host": (_i, [_p, _i, _i, _sz, _sz, _sz, _d, _p, _p, _d, _p]),
     "fg_gemm_f32_host": (_i, [_p, _i, _sz, _sz, _sz, _f, _p, _p, _f, _p]),

@@ -153,6 +153,20 @@ fg_status fg_quantized_matmul(fg_ctx *ctx, size_t m, size_t n, size_t k, const u
                               uint8_t a_zp, float scale_a, const int8_t *b, int8_t b_zp,
                               float scale_b, float *c, int accumulate, fg_stream stream);
 
+/* quantized_matmul that allocates nothing -- no counterpart in the
+ * reference.  Same contract and results as fg_quantized_matmul, for callers
+ * that may not allocate device memory at call time (memory owned by another
+ * allocator, a fixed HBM budget, latency-critical loops).  Its zero-point
+ * row/column sums live in one fixed 512 KiB device array per GPU, held until
+ * the process exits; the first call on a device looks up that array's
+ * address and should come before any stream capture.  Calls share the array,
+ * so calls that overlap on the GPU race.  Limits: m, n, k <= 65536; k and n
+ * multiples of 16 and a, b 16-byte aligned; otherwise FG_ERR_UNSUPPORTED. */
+fg_status fg_quantized_matmul_noalloc(fg_ctx *ctx, size_t m, size_t n, size_t k,
+                                      const uint8_t *a, uint8_t a_zp, float scale_a,
+                                      const int8_t *b, int8_t b_zp, float scale_b, float *c,
+                                      int accumulate, fg_stream stream);
+
 /* Generic strided form of all of the above (the reference's internal
  * drivers take lda/ldb/ldc: gemm/outer.rs:198-210).  alpha/beta point to a
  * scalar of the dtype's real type (two for complex: re, im); integer dtypes
