@@ -251,11 +251,13 @@ def gemm_f64(m, n, k, alpha, a, b, beta, c, mode=PLAIN, ozaki_slices=0):
                      C.c_double)
 
 
-def gemm_f32(m, n, k, alpha, a, b, beta, c, mode=PLAIN):
-    """C = alpha*A@B + beta*C (gemm/mod.rs:940).  mode='split': 3xBF16."""
+def gemm_f32(m, n, k, alpha, a, b, beta, c, mode=PLAIN, bf16_slices=0):
+    """C = alpha*A@B + beta*C (gemm/mod.rs:940).  mode='split': 3xBF16
+    (bf16_slices=2, default) or the 6-product 3-slice form (bf16_slices=3)."""
     _need(a, m * k, np.float32, "a"); _need(b, k * n, np.float32, "b")
     _need(c, m * n, np.float32, "c")
-    return _run_gemm(L.FG_F32, mode, 0, m, n, k, [alpha], a, b, [beta], c, 0, C.c_float)
+    return _run_gemm(L.FG_F32, mode, bf16_slices, m, n, k, [alpha], a, b, [beta], c, 0,
+                     C.c_float)
 
 
 def gemm_c64(m, n, k, alpha_re, alpha_im, a, b, beta_re, beta_im, c, mode=PLAIN,
@@ -267,11 +269,12 @@ def gemm_c64(m, n, k, alpha_re, alpha_im, a, b, beta_re, beta_im, c, mode=PLAIN,
                      [beta_re, beta_im], c, 0, C.c_double)
 
 
-def gemm_c32(m, n, k, alpha_re, alpha_im, a, b, beta_re, beta_im, c, mode=PLAIN):
+def gemm_c32(m, n, k, alpha_re, alpha_im, a, b, beta_re, beta_im, c, mode=PLAIN,
+             bf16_slices=0):
     """Complex<f32> GEMM (gemm/mod.rs:669); a, b, c complex64."""
     _need(a, m * k, np.complex64, "a"); _need(b, k * n, np.complex64, "b")
     _need(c, m * n, np.complex64, "c")
-    return _run_gemm(L.FG_C32, mode, 0, m, n, k, [alpha_re, alpha_im], a, b,
+    return _run_gemm(L.FG_C32, mode, bf16_slices, m, n, k, [alpha_re, alpha_im], a, b,
                      [beta_re, beta_im], c, 0, C.c_float)
 
 

@@ -1,0 +1,197 @@
+// gemm_ozaki.cu -- split-mode DGEMM / ZGEMM: INT8 Ozaki slicing on the
+// integer tensor cores (method and layouts in ozaki_kernels.cuh).
+//
+// Per call: row/column exponent scan (FP64), slice extraction into int8
+// digit planes (FP64 -> int8), then for each K chunk and each slice group
+// d = S+1 .. 2 (smallest weight first) ONE tcgen05 kind::i8 GEMM over the
+// concatenated K of that group, whose epilogue adds 2^-7d * 2^(e_i+f_j) * G_d
+// into C in FP64.  Every group sum G_d = sum_{s+t=d} A_s B_t is exact in
+// int32: at most S products of K_chunk * 127^2, with K_chunk chosen so that
+// S * K_chunk * 127^2 < 2^31.
+#include <algorithm>
+#include <mutex>
+
+#include "ozaki_kernels.cuh"
+#include "runtime.h"
+#include "tc_gemm.cuh"
+
+namespace fgrt {
+
+using namespace fg;
+
+using CfgOzaki = TcCfg<KIND_I8, 256, 4, 1, 1, 1, 1, EPI_OZAKI>;
+
+static int grid_for(long long total) {
+    return static_cast<int>(std::min<long long>(std::max<long long>((total + 255) / 256, 1), 8192));
+}
+
+static long long round_up(long long x, long long a) { return (x + a - 1) / a * a; }
+
+static fg_status launch_group(fg_ctx* ctx, const TcMaps& maps, TcArgs& args, cudaStream_t st) {
+    static std::once_flag once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(once, [] {
+        attr_err = cudaFuncSetAttribute(tc_gemm_kernel<CfgOzaki>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(tc_smem_bytes<CfgOzaki>()));
+    });
+    FG_CUDA(attr_err);
+    args.status = ctx->d_status;
+    args.timeout_ns = 4000000000ull;
+    const long long tiles = (long long)args.tiles_m * args.tiles_n;
+    const int grid = static_cast<int>(std::min<long long>(tiles, ctx->sm_count));
+    ProfScope prof("tc_gemm_ozaki_i8", st);
+    tc_gemm_kernel<CfgOzaki><<<grid, CfgOzaki::THREADS, tc_smem_bytes<CfgOzaki>(), st>>>(maps, args);
+    prof.stop();
+    count_launch();
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+template <int S>
+static fg_status slice_operands(const Gemm& g, bool cplx, long long Kc, long long nchunks,
+                                long long Np, int8_t* a_all, int8_t* b_all, double* rsc,
+                                double* csc, unsigned long long* cmax, unsigned long long* kmax_a,
+                                unsigned long long* kmax_b, int* shift, cudaStream_t st) {
+    const double* A = static_cast<const double*>(g.A);
+    const double* B = static_cast<const double*>(g.B);
+    const long long M = g.M, K = g.K, N = g.N;
+    const int cx = cplx ? 1 : 0;
+    const long long rows_per = 256;
+    // balancing exponents of the inner dimension
+    FG_CUDA(cudaMemsetAsync(kmax_a, 0, K * sizeof(unsigned long long), st));
+    dim3 agrid(static_cast<unsigned>((K + 255) / 256), static_cast<unsigned>((M + rows_per - 1) / rows_per));
+    ozaki_a_colmax_kernel<<<agrid, 256, 0, st>>>(A, M, K, g.lda, cx, rows_per, kmax_a);
+    ozaki_b_rowmax_kernel<<<grid_for(K * 32), 256, 0, st>>>(B, K, N, g.ldb, cx, kmax_b);
+    ozaki_shift_kernel<<<grid_for(K), 256, 0, st>>>(kmax_a, kmax_b, K, shift);
+    // row / column scales of the balanced operands
+    ozaki_row_scale_kernel<<<grid_for(M * 32), 256, 0, st>>>(A, M, K, g.lda, cx, shift, rsc);
+    FG_CUDA(cudaMemsetAsync(cmax, 0, N * sizeof(unsigned long long), st));
+    dim3 cgrid(static_cast<unsigned>((N + 255) / 256), static_cast<unsigned>((K + rows_per - 1) / rows_per));
+    ozaki_col_max_kernel<<<cgrid, 256, 0, st>>>(B, K, N, g.ldb, cx, rows_per, shift, cmax);
+    ozaki_col_scale_kernel<<<grid_for(N), 256, 0, st>>>(cmax, N, csc);
+    count_launch(6);
+    // Slice chunk by chunk so each chunk's digit planes are contiguous.
+    for (long long c = 0; c < nchunks; ++c) {
+        ozaki_slice_a_kernel<S><<<grid_for(M * Kc), 256, 0, st>>>(
+            A, M, K, g.lda, cx, shift, rsc, a_all + c * M * S * Kc, Kc, c * Kc);
+        ozaki_slice_b_kernel<S><<<grid_for(Kc * Np), 256, 0, st>>>(
+            B, K, N, g.ldb, cx, shift, csc, b_all + c * S * Kc * Np, Kc, Np, c * Kc);
+        count_launch(2);
+    }
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+fg_status launch_ozaki(fg_ctx* ctx, const Gemm& g0, cudaStream_t st) {
+    if (g0.batch > 1) {
+        for (int i = 0; i < g0.batch; ++i) {
+            Gemm s = g0;
+            long long ia = 0, ib = 0;
+            int rem = i;
+            for (int d = g0.bdims - 1; d >= 0; --d) {
+                int idx = rem % g0.bshape[d];
+                rem /= g0.bshape[d];
+                ia += idx * g0.a_istride[d];
+                ib += idx * g0.b_istride[d];
+            }
+            const size_t es = g0.dtype == FG_C64 ? 2 : 1;  // doubles per element
+            s.batch = 1;
+            s.bdims = 0;
+            s.a_count = s.b_count = 1;
+            s.A = static_cast<const double*>(g0.A) + es * ia * g0.a_mstride;
+            s.B = static_cast<const double*>(g0.B) + es * ib * g0.b_mstride;
+            s.C = static_cast<double*>(g0.C) + es * i * g0.c_stride;
+            FG_TRY(launch_ozaki(ctx, s, st));
+        }
+        return FG_OK;
+    }
+    const Gemm& g = g0;
+    const bool cplx = g.dtype == FG_C64;
+    // 9 slices by default: with K balancing this keeps the normwise error well
+    // below plain FP64's for exponent spreads up to 10^8 (8 is about equal).
+    const int S = g.slices > 0 ? g.slices : 9;
+    if (S < 3 || S > 10) return set_error(FG_ERR_INVALID, "ozaki_slices must be in 3..10");
+    if (g.alpha_im != 0.0 || g.beta_im != 0.0)
+        return set_error(FG_ERR_UNSUPPORTED, "split ZGEMM: complex alpha/beta must be real");
+    const long long M = g.M, Kw = cplx ? 2 * g.K : g.K, Nw = cplx ? 2 * g.N : g.N;
+    // int32 exactness: S products of Kc * 127^2 per group sum.
+    const long long kmax = ((2147483647ll / (16129ll * S)) / 128) * 128;
+    const long long Kp = round_up(Kw, 16);
+    const long long nchunks = (Kp + kmax - 1) / kmax;
+    const long long Kc = nchunks == 1 ? Kp : kmax;
+    const long long Np = round_up(Nw, 16);
+    const size_t a_bytes = static_cast<size_t>(nchunks * M * S * Kc);
+    const size_t b_bytes = static_cast<size_t>(nchunks * S * Kc * Np);
+    const size_t n_sc = static_cast<size_t>(cplx ? g.N : g.N);
+    Scratch sc;
+    const size_t meta = (M + n_sc) * sizeof(double) + n_sc * sizeof(unsigned long long) +
+                        2 * g.K * sizeof(unsigned long long) + g.K * sizeof(int);
+    FG_TRY(sc.alloc(round_up((long long)a_bytes, 256) + round_up((long long)b_bytes, 256) + meta, st));
+    int8_t* a_all = static_cast<int8_t*>(sc.p);
+    int8_t* b_all = a_all + round_up((long long)a_bytes, 256);
+    double* rsc = reinterpret_cast<double*>(b_all + round_up((long long)b_bytes, 256));
+    double* csc = rsc + M;
+    unsigned long long* cmax = reinterpret_cast<unsigned long long*>(csc + n_sc);
+    unsigned long long* kmax_a = cmax + n_sc;
+    unsigned long long* kmax_b = kmax_a + g.K;
+    int* shift = reinterpret_cast<int*>(kmax_b + g.K);
+    fg_status sst;
+    switch (S) {
+        case 3: sst = slice_operands<3>(g, cplx, Kc, nchunks, Np, a_all, b_all, rsc, csc, cmax, kmax_a, kmax_b, shift, st); break;
+        case 4: sst = slice_operands<4>(g, cplx, Kc, nchunks, Np, a_all, b_all, rsc, csc, cmax, kmax_a, kmax_b, shift, st); break;
+        case 5: sst = slice_operands<5>(g, cplx, Kc, nchunks, Np, a_all, b_all, rsc, csc, cmax, kmax_a, kmax_b, shift, st); break;
+        case 6: sst = slice_operands<6>(g, cplx, Kc, nchunks, Np, a_all, b_all, rsc, csc, cmax, kmax_a, kmax_b, shift, st); break;
+        case 9: sst = slice_operands<9>(g, cplx, Kc, nchunks, Np, a_all, b_all, rsc, csc, cmax, kmax_a, kmax_b, shift, st); break;
+        case 10: sst = slice_operands<10>(g, cplx, Kc, nchunks, Np, a_all, b_all, rsc, csc, cmax, kmax_a, kmax_b, shift, st); break;
+        case 7: sst = slice_operands<7>(g, cplx, Kc, nchunks, Np, a_all, b_all, rsc, csc, cmax, kmax_a, kmax_b, shift, st); break;
+        default: sst = slice_operands<8>(g, cplx, Kc, nchunks, Np, a_all, b_all, rsc, csc, cmax, kmax_a, kmax_b, shift, st); break;
+    }
+    FG_TRY(sst);
+
+    bool first = true;
+    for (long long c = 0; c < nchunks; ++c) {
+        const int8_t* ac = a_all + c * M * S * Kc;
+        const int8_t* bc = b_all + c * S * Kc * Np;
+        for (int d = S + 1; d >= 2; --d) {
+            const long long Kd = (d - 1) * Kc;
+            TcMaps maps;
+            TcArgs args{};
+            {
+                uint64_t dims[2] = {static_cast<uint64_t>(Kd), static_cast<uint64_t>(M)};
+                uint64_t strides[1] = {static_cast<uint64_t>(S * Kc)};
+                uint32_t box[2] = {128, 128};
+                FG_TRY(encode_map(&maps.a[0], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, ac, dims, strides, box));
+            }
+            {
+                uint64_t dims[2] = {static_cast<uint64_t>(Nw), static_cast<uint64_t>(Kd)};
+                uint64_t strides[1] = {static_cast<uint64_t>(Np)};
+                uint32_t box[2] = {128, 128};
+                FG_TRY(encode_map(&maps.b[0], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2,
+                                  bc + (S - d + 1) * Kc * Np, dims, strides, box));
+            }
+            args.M = static_cast<int>(M);
+            args.N = static_cast<int>(Nw);
+            args.K = static_cast<int>(Kd);
+            args.tiles_m = static_cast<int>((M + 127) / 128);
+            args.tiles_n = static_cast<int>((Nw + CfgOzaki::BN - 1) / CfgOzaki::BN);
+            args.k_blocks = static_cast<int>((Kd + CfgOzaki::BK - 1) / CfgOzaki::BK);
+            args.batch = 1;
+            args.bdims = 1;
+            args.bshape[0] = 1;
+            args.C = g.C;
+            args.ldc = cplx ? 2 * g.ldc : g.ldc;
+            args.cplx_half = cplx ? static_cast<int>(g.N) : 0;
+            args.row_scale = rsc;
+            args.col_scale = csc;
+            args.oz_w = g.alpha_re * std::ldexp(1.0, -7 * d);
+            args.oz_beta = g.beta_re;
+            args.oz_first = first ? 1 : 0;
+            args.ops[0] = TcOp{0, 0, 0, 1, 1};
+            FG_TRY(launch_group(ctx, maps, args, st));
+            first = false;
+        }
+    }
+    return FG_OK;
+}
+
+}  // namespace fgrt

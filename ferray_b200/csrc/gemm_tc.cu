@@ -21,13 +21,17 @@ using namespace fg;
 using CfgI8 = TcCfg<KIND_I8, 256, 4, 1, 1, 1, 1, EPI_I32>;
 using CfgQmm = TcCfg<KIND_I8, 256, 4, 1, 1, 1, 1, EPI_QMM>;
 using CfgI16 = TcCfg<KIND_I8, 128, 3, 2, 2, 3, 4, EPI_I16>;
+// 3 products: one accumulator (the 2-slice representation error, about
+// 2^-18 |a||b| per product, dominates whatever the accumulation does).
+// 6 products: accumulator 0 holds hi*hi, accumulator 1 the corrections.
 using CfgBf16x3 = TcCfg<KIND_BF16, 128, 3, 2, 2, 1, 3, EPI_F32, 1>;
+using CfgBf16x6 = TcCfg<KIND_BF16, 128, 2, 3, 3, 2, 6, EPI_F32, 1>;
 
 // K blocks (64 bf16 each) per TMEM accumulation chunk of the split SGEMM.
 static int split_kchunk() {
     static int v = [] {
         const char* e = getenv("FG_SPLIT_KCHUNK");
-        return e ? atoi(e) : 4;
+        return e ? atoi(e) : 2;
     }();
     return v;
 }
@@ -36,7 +40,7 @@ static unsigned long long kTimeoutNs = 4000000000ull;  // 4 s per wait
 
 template <class Cfg>
 static const char* cfg_name() {
-    if (Cfg::KIND == KIND_BF16) return "tc_gemm_3xbf16";
+    if (Cfg::KIND == KIND_BF16) return Cfg::NOPS == 6 ? "tc_gemm_6xbf16" : "tc_gemm_3xbf16";
     if (Cfg::EPI == EPI_I16) return "tc_gemm_i16";
     if (Cfg::EPI == EPI_QMM) return "tc_gemm_qmm";
     return "tc_gemm_i8";
@@ -284,36 +288,37 @@ fg_status launch_split_bf16(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
         return FG_OK;
     }
     // Real-embedded sizes for complex: (M x 2K) * (2K x 2N).
+    const int ns = g.slices == 3 ? 3 : 2;  // bf16 slices per operand
     const long long M = g.M, K = cplx ? 2 * g.K : g.K, N = cplx ? 2 * g.N : g.N;
     const long long pa = round_up(K, 8), pb = round_up(N, 8);  // bf16 elements, 16-byte pitch
     const size_t a_elems = static_cast<size_t>(pa * M * g.a_count);
     const size_t b_elems = static_cast<size_t>(pb * K * g.b_count);
     Scratch s;
-    FG_TRY(s.alloc((2 * a_elems + 2 * b_elems) * sizeof(__nv_bfloat16), st));
-    __nv_bfloat16* ahi = static_cast<__nv_bfloat16*>(s.p);
-    __nv_bfloat16* alo = ahi + a_elems;
-    __nv_bfloat16* bhi = alo + a_elems;
-    __nv_bfloat16* blo = bhi + b_elems;
+    FG_TRY(s.alloc((ns * a_elems + ns * b_elems) * sizeof(__nv_bfloat16), st));
+    BfPlanes ap{}, bp{};
+    __nv_bfloat16* base = static_cast<__nv_bfloat16*>(s.p);
+    for (int i = 0; i < ns; ++i) ap.p[i] = base + i * a_elems;
+    for (int i = 0; i < ns; ++i) bp.p[i] = base + ns * a_elems + i * b_elems;
     if (cplx) {
         if (g.M * g.K > 0) {
             split_bf16_cplx_a_kernel<<<grid_for(g.M * g.K), 256, 0, st>>>(
-                static_cast<const float2*>(g.A), g.M, g.K, g.lda, ahi, alo, pa);
+                static_cast<const float2*>(g.A), g.M, g.K, g.lda, ap, pa, ns);
             count_launch();
         }
         if (g.K * g.N > 0) {
             split_bf16_cplx_b_kernel<<<grid_for(g.K * g.N), 256, 0, st>>>(
-                static_cast<const float2*>(g.B), g.K, g.N, g.ldb, bhi, blo, pb);
+                static_cast<const float2*>(g.B), g.K, g.N, g.ldb, bp, pb, ns);
             count_launch();
         }
     } else {
         if (M * K > 0) {
-            split_bf16_kernel<<<dim3(grid_for(M * K), static_cast<unsigned>(g.a_count)), 256, 0, st>>>(
-                static_cast<const float*>(g.A), M, K, g.lda, ahi, alo, pa, g.a_mstride, pa * M);
+            split_bf16_kernel<<<dim3(grid_for(M * (K + 3) / 4), static_cast<unsigned>(g.a_count)), 256, 0, st>>>(
+                static_cast<const float*>(g.A), M, K, g.lda, ap, pa, ns, g.a_mstride, pa * M);
             count_launch();
         }
         if (K * N > 0) {
-            split_bf16_kernel<<<dim3(grid_for(K * N), static_cast<unsigned>(g.b_count)), 256, 0, st>>>(
-                static_cast<const float*>(g.B), K, N, g.ldb, bhi, blo, pb, g.b_mstride, pb * K);
+            split_bf16_kernel<<<dim3(grid_for(K * (N + 3) / 4), static_cast<unsigned>(g.b_count)), 256, 0, st>>>(
+                static_cast<const float*>(g.B), K, N, g.ldb, bp, pb, ns, g.b_mstride, pb * K);
             count_launch();
         }
     }
@@ -321,10 +326,10 @@ fg_status launch_split_bf16(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
     TcMaps maps;
     TcArgs args{};
     int r3;
-    FG_TRY(operand_map(&maps.a[0], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, ahi, K, M, pa * 2, g.a_count, pa * M * 2, 64, 128, &args.a_rank3));
-    FG_TRY(operand_map(&maps.a[1], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, alo, K, M, pa * 2, g.a_count, pa * M * 2, 64, 128, &r3));
-    FG_TRY(operand_map(&maps.b[0], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, bhi, N, K, pb * 2, g.b_count, pb * K * 2, 64, 64, &args.b_rank3));
-    FG_TRY(operand_map(&maps.b[1], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, blo, N, K, pb * 2, g.b_count, pb * K * 2, 64, 64, &r3));
+    for (int i = 0; i < ns; ++i) {
+        FG_TRY(operand_map(&maps.a[i], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, ap.p[i], K, M, pa * 2, g.a_count, pa * M * 2, 64, 128, i == 0 ? &args.a_rank3 : &r3));
+        FG_TRY(operand_map(&maps.b[i], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, bp.p[i], N, K, pb * 2, g.b_count, pb * K * 2, 64, 64, i == 0 ? &args.b_rank3 : &r3));
+    }
     args.M = static_cast<int>(M);
     args.N = static_cast<int>(N);
     args.K = static_cast<int>(K);
@@ -343,6 +348,16 @@ fg_status launch_split_bf16(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
         args.ldc = 2 * g.ldc;
     }
     args.kchunk = split_kchunk();
+    if (ns == 3) {
+        // hi*hi + (hi*mid + mid*hi) + (hi*lo + lo*hi + mid*mid), smallest first
+        args.ops[0] = TcOp{2, 0, 1, 1, 1};
+        args.ops[1] = TcOp{0, 2, 1, 1, 1};
+        args.ops[2] = TcOp{1, 1, 1, 1, 1};
+        args.ops[3] = TcOp{1, 0, 1, 1, 1};
+        args.ops[4] = TcOp{0, 1, 1, 1, 1};
+        args.ops[5] = TcOp{0, 0, 0, 1, 1};
+        return launch_cfg<CfgBf16x6>(ctx, maps, args, st);
+    }
     args.ops[0] = TcOp{1, 0, 0, 1, 1};  // lo * hi
     args.ops[1] = TcOp{0, 1, 0, 1, 1};  // hi * lo
     args.ops[2] = TcOp{0, 0, 0, 1, 1};  // hi * hi

@@ -1,0 +1,241 @@
+// ozaki_kernels.cuh -- operand slicing for the INT8 Ozaki DGEMM / ZGEMM.
+//
+// Method (Ozaki, Ogita, Oishi error-free splitting, in the INT8 form of
+// Ootomo/Ozaki/Yokota and Uchino/Ozaki/Imamura): every row i of A is scaled
+// by 2^-e_i, with e_i the frexp exponent of max_k |a_ik|, so |a_ik 2^-e_i| < 1;
+// the scaled value t is written as S signed base-128 digits by exact
+// scale-and-truncate steps, t = sum_{s=1..S} d_s 128^-s + r, |d_s| <= 127,
+// |r| < 128^-S, each digit plane stored as an int8 slice.  Before that the
+// inner dimension is balanced: AB = (A D)(D^-1 B) with D = diag(2^shift_k)
+// chosen from A's column maxima and B's row maxima, so a term a_ik b_kj is
+// represented relative to magnitudes near its own rather than to the largest
+// entry of its row (which is what keeps exponent-spread inputs accurate).  Columns of B likewise with
+// their own exponents f_j.  Then
+//     C_ij = 2^(e_i+f_j) sum_{s,t} 2^(-7(s+t)) (A_s B_t)_ij
+// and the products A_s B_t are exact int32 GEMMs on the integer tensor cores.
+// Pairs with s + t > S + 1 are dropped (each is below K * 2^-7S of
+// row-max * col-max).
+//
+// Layouts chosen so every group d = s + t is ONE plain int8 GEMM over a
+// concatenated K: A slices side by side, A_all = [A_1 | A_2 | ... | A_S]
+// (M x S*Kp), and B slices stacked in reverse, B_all = [B_S; ...; B_1]
+// (S*Kp x N).  Group d is then A_all[:, 0:(d-1)Kp] times the last (d-1)Kp
+// rows of B_all, i.e. sum_{s=1..d-1} A_s B_{d-s}.
+//
+// Complex operands use the real embedding [Ar Ai] and [[Br Bi], [-Bi Br]]
+// (M x 2K and 2K x 2N) while slicing.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace fg {
+
+// |x| as ordered bits (monotone for non-negative doubles, NaN above Inf).
+__device__ __forceinline__ unsigned long long abs_bits(double x) {
+    return static_cast<unsigned long long>(__double_as_longlong(x)) & 0x7FFFFFFFFFFFFFFFull;
+}
+
+// 2^e with frexp(max) = m * 2^e, m in [0.5, 1); zero rows get 1, non-finite
+// rows get NaN so their outputs come out NaN.
+__device__ __forceinline__ double scale_from_max_bits(unsigned long long bits) {
+    const double mx = __longlong_as_double(static_cast<long long>(bits));
+    if (mx == 0.0) return 1.0;
+    if (!isfinite(mx)) return __longlong_as_double(0x7FF8000000000000ll);
+    int e;
+    frexp(mx, &e);
+    return ldexp(1.0, e);
+}
+
+// Row maxima of a real (cplx = 0) or complex (cplx = 1: Re and Im) matrix,
+// one warp per row.
+// `shift` (may be null) holds the balancing exponent of each K index: the row
+// maxima are those of A * diag(2^shift).
+static __global__ void ozaki_row_scale_kernel(const double* __restrict__ A, long long M,
+                                              long long K, long long lda, int cplx,
+                                              const int* __restrict__ shift,
+                                              double* __restrict__ scale) {
+    const long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x % 32;
+    if (row >= M) return;
+    const long long len = cplx ? 2 * K : K;
+    const double* r = A + row * (cplx ? 2 * lda : lda);
+    unsigned long long mx = 0;
+    for (long long k = lane; k < len; k += 32) {
+        const int sh = shift ? shift[cplx ? (k >> 1) : k] : 0;
+        mx = max(mx, abs_bits(ldexp(r[k], sh)));
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+    if (lane == 0) scale[row] = scale_from_max_bits(mx);
+}
+
+// Column maxima, pass 1: each thread scans `rows_per` rows of one (complex:
+// embedded) column and folds the result into colmax_bits with atomicMax.
+// Real B: N columns.  Complex B: the embedded B' has 2N columns, column c < N
+// holds (Br, -Bi) and c >= N holds (Bi, Br) -> both have max(|Br|, |Bi|) of
+// complex column c mod N, so N maxima suffice.
+// The column maxima are those of diag(2^-shift) * B (shift may be null).
+static __global__ void ozaki_col_max_kernel(const double* __restrict__ B, long long K, long long N,
+                                            long long ldb, int cplx, long long rows_per,
+                                            const int* __restrict__ shift,
+                                            unsigned long long* __restrict__ colmax_bits) {
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= N) return;
+    const long long k0 = blockIdx.y * rows_per, k1 = min(K, k0 + rows_per);
+    unsigned long long mx = 0;
+    for (long long k = k0; k < k1; ++k) {
+        const int sh = shift ? -shift[k] : 0;
+        if (cplx) {
+            const double2 v = reinterpret_cast<const double2*>(B)[k * ldb + j];
+            mx = max(mx, max(abs_bits(ldexp(v.x, sh)), abs_bits(ldexp(v.y, sh))));
+        } else {
+            mx = max(mx, abs_bits(ldexp(B[k * ldb + j], sh)));
+        }
+    }
+    atomicMax(colmax_bits + j, mx);
+}
+
+// Balancing of the inner dimension: AB = (A D)(D^-1 B) for D = diag(2^shift_k).
+// Pass 1: column maxima of A (over rows, atomicMax of ordered bits).
+static __global__ void ozaki_a_colmax_kernel(const double* __restrict__ A, long long M, long long K,
+                                             long long lda, int cplx, long long rows_per,
+                                             unsigned long long* __restrict__ out) {
+    const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (k >= K) return;
+    const long long i0 = blockIdx.y * rows_per, i1 = min(M, i0 + rows_per);
+    unsigned long long mx = 0;
+    for (long long i = i0; i < i1; ++i) {
+        if (cplx) {
+            const double2 v = reinterpret_cast<const double2*>(A)[i * lda + k];
+            mx = max(mx, max(abs_bits(v.x), abs_bits(v.y)));
+        } else {
+            mx = max(mx, abs_bits(A[i * lda + k]));
+        }
+    }
+    atomicMax(out + k, mx);
+}
+
+// Pass 2: row maxima of B, one warp per row.
+static __global__ void ozaki_b_rowmax_kernel(const double* __restrict__ B, long long K, long long N,
+                                             long long ldb, int cplx,
+                                             unsigned long long* __restrict__ out) {
+    const long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x % 32;
+    if (row >= K) return;
+    const long long len = cplx ? 2 * N : N;
+    const double* r = B + row * (cplx ? 2 * ldb : ldb);
+    unsigned long long mx = 0;
+    for (long long j = lane; j < len; j += 32) mx = max(mx, abs_bits(r[j]));
+    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+    if (lane == 0) out[row] = mx;
+}
+
+// Pass 3: shift_k = floor((eB_k - eA_k) / 2), so column k of A D and row k of
+// D^-1 B peak at about the same magnitude.  Zero or non-finite maxima: 0.
+static __global__ void ozaki_shift_kernel(const unsigned long long* __restrict__ a_colmax,
+                                          const unsigned long long* __restrict__ b_rowmax,
+                                          long long K, int* __restrict__ shift) {
+    const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (k >= K) return;
+    const double ma = __longlong_as_double(static_cast<long long>(a_colmax[k]));
+    const double mb = __longlong_as_double(static_cast<long long>(b_rowmax[k]));
+    int sh = 0;
+    if (ma > 0.0 && mb > 0.0 && isfinite(ma) && isfinite(mb)) {
+        int ea, eb;
+        frexp(ma, &ea);
+        frexp(mb, &eb);
+        const int d = eb - ea;
+        sh = d >= 0 ? d / 2 : -((-d + 1) / 2);
+    }
+    shift[k] = sh;
+}
+
+static __global__ void ozaki_col_scale_kernel(const unsigned long long* __restrict__ colmax_bits,
+                                              long long N, double* __restrict__ scale) {
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j < N) scale[j] = scale_from_max_bits(colmax_bits[j]);
+}
+
+// Signed base-128 digits of t = x / scale, |t| < 1, by repeated exact
+// scaling and truncation: t = sum_s d_s 128^-(s+1) + r, |r| < 128^-S, all
+// digits carrying the sign of x (each step is exact in FP64).
+template <int S>
+__device__ __forceinline__ void ozaki_digits(double x, double inv_scale, int8_t (&d)[S]) {
+    double t = x * inv_scale;  // power-of-two scaling: exact
+    if (!isfinite(t)) t = 0.0;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        t *= 128.0;
+        const double q = trunc(t);
+        t -= q;
+        d[s] = static_cast<int8_t>(static_cast<int>(q));
+    }
+}
+
+// A slices: A_all[i, s*Kp + k] = digit s of A[i, k] (s = 0 most significant);
+// complex A is embedded as [Ar | Ai] (width 2K).  Kp >= width, padding zero.
+// Chunked: this launch writes embedded columns [k0, k0 + Kp) of the plane.
+template <int S>
+__global__ void ozaki_slice_a_kernel(const double* __restrict__ A, long long M, long long K,
+                                     long long lda, int cplx, const int* __restrict__ shift,
+                                     const double* __restrict__ scale,
+                                     int8_t* __restrict__ out, long long Kp, long long k0) {
+    const long long W = cplx ? 2 * K : K;
+    const long long total = M * Kp;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long i = e / Kp, kl = e - i * Kp, k = k0 + kl;
+        double x = 0.0;
+        if (k < W) {
+            if (cplx) {
+                const long long kk = k < K ? k : k - K;
+                x = ldexp(A[2 * (i * lda + kk) + (k < K ? 0 : 1)], shift[kk]);
+            } else {
+                x = ldexp(A[i * lda + k], shift[k]);
+            }
+        }
+        int8_t d[S];
+        ozaki_digits<S>(x, 1.0 / scale[i], d);
+        int8_t* o = out + i * (S * Kp) + kl;
+#pragma unroll
+        for (int s = 0; s < S; ++s) o[s * Kp] = d[s];
+    }
+}
+
+// B slices stacked in reverse: B_all[(S-1-s)*Kp + k, j] = digit s of B[k, j].
+// Complex B is embedded as [[Br, Bi], [-Bi, Br]] (2K x 2N); Np >= width.
+// Chunked: this launch writes embedded rows [k0, k0 + Kp) of the planes.
+template <int S>
+__global__ void ozaki_slice_b_kernel(const double* __restrict__ B, long long K, long long N,
+                                     long long ldb, int cplx, const int* __restrict__ shift,
+                                     const double* __restrict__ scale,
+                                     int8_t* __restrict__ out, long long Kp, long long Np,
+                                     long long k0) {
+    const long long H = cplx ? 2 * K : K;   // embedded rows
+    const long long W = cplx ? 2 * N : N;   // embedded columns
+    const long long total = Kp * Np;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long kl = e / Np, j = e - kl * Np, k = k0 + kl;
+        double x = 0.0;
+        double sc = 1.0;
+        if (k < H && j < W) {
+            if (cplx) {
+                const bool top = k < K, left = j < N;
+                const long long kk = top ? k : k - K, jj = left ? j : j - N;
+                const double2 v = reinterpret_cast<const double2*>(B)[kk * ldb + jj];
+                // top-left Br, top-right Bi, bottom-left -Bi, bottom-right Br
+                x = ldexp(top ? (left ? v.x : v.y) : (left ? -v.y : v.x), -shift[kk]);
+                sc = scale[jj];
+            } else {
+                x = ldexp(B[k * ldb + j], -shift[k]);
+                sc = scale[j];
+            }
+        }
+        int8_t d[S];
+        ozaki_digits<S>(x, 1.0 / sc, d);
+#pragma unroll
+        for (int s = 0; s < S; ++s) out[((S - 1 - s) * Kp + kl) * Np + j] = d[s];
+    }
+}
+
+}  // namespace fg

@@ -4,7 +4,8 @@
 //
 //  * split_bf16: x -> (hi, lo) with hi = bf16(x), lo = bf16(x - hi), both
 //    round-to-nearest-even, for the 3xBF16 SGEMM (x = hi + lo + r,
-//    |r| <= 2^-17 |x|).  Optional complex real-embedding: the complex
+//    |r| <= 2^-18 |x|); or three slices (hi, mid, lo), exact for f32, for the
+//    6-product variant.  Optional complex real-embedding: the complex
 //    product A*B equals the real product [Ar Ai] * [[Br Bi], [-Bi Br]],
 //    whose columns are [Re C | Im C].
 //  * split_i16: x -> (hi, lo) with x = 256*hi + lo, hi signed 8-bit,
@@ -19,71 +20,94 @@
 
 namespace fg {
 
-__device__ __forceinline__ void split_one(float x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
-    hi = __float2bfloat16_rn(x);
-    lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+// Up to three bf16 slices: o[0] = bf16(x), o[s] = bf16(x - o[0] - ... - o[s-1]),
+// every residual exact in f32.  Three slices hold all 24 bits of an f32.
+struct BfPlanes {
+    __nv_bfloat16* p[3];
+};
+
+__device__ __forceinline__ void split_n(float x, int ns, __nv_bfloat16 (&o)[3]) {
+    float r = x;
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+        if (s < ns) {
+            o[s] = __float2bfloat16_rn(r);
+            r = r - __bfloat162float(o[s]);
+        }
+    }
 }
 
-// Real operand: X (rows x cols, pitch ldx) -> hi/lo (pitch ldo).
+// Real operand: X (rows x cols, pitch ldx) -> ns planes (pitch ldo, a
+// multiple of 4).  Four consecutive elements per thread, 8-byte stores.
 static __global__ void split_bf16_kernel(const float* __restrict__ X, long long rows, long long cols,
-                                  long long ldx, __nv_bfloat16* __restrict__ hi,
-                                  __nv_bfloat16* __restrict__ lo, long long ldo,
-                                  long long x_bstride, long long o_bstride) {
+                                         long long ldx, BfPlanes out, long long ldo, int ns,
+                                         long long x_bstride, long long o_bstride) {
     const float* Xb = X + blockIdx.y * x_bstride;
-    __nv_bfloat16* hb = hi + blockIdx.y * o_bstride;
-    __nv_bfloat16* lb = lo + blockIdx.y * o_bstride;
-    const long long total = rows * cols;
+    const long long cq = (cols + 3) / 4;
+    const long long total = rows * cq;
+    const bool vec_in = (ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(Xb) & 15) == 0);
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
          e += (long long)gridDim.x * blockDim.x) {
-        long long r = e / cols, c = e - r * cols;
-        __nv_bfloat16 h, l;
-        split_one(Xb[r * ldx + c], h, l);
-        hb[r * ldo + c] = h;
-        lb[r * ldo + c] = l;
+        const long long r = e / cq, c = (e - r * cq) * 4;
+        float v[4];
+        if (vec_in && c + 3 < cols) {
+            const float4 q = *reinterpret_cast<const float4*>(Xb + r * ldx + c);
+            v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[j] = (c + j < cols) ? Xb[r * ldx + c + j] : 0.f;
+        }
+        __nv_bfloat16 o[4][3];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) split_n(v[j], ns, o[j]);
+        for (int s = 0; s < ns; ++s) {
+            __nv_bfloat16* dst = out.p[s] + blockIdx.y * o_bstride + r * ldo + c;
+            if (c + 3 < ldo) {
+                __align__(8) __nv_bfloat16 w[4] = {o[0][s], o[1][s], o[2][s], o[3][s]};
+                *reinterpret_cast<uint2*>(dst) = *reinterpret_cast<const uint2*>(w);
+            } else {
+                for (int j = 0; j < 4 && c + j < ldo; ++j) dst[j] = o[j][s];
+            }
+        }
     }
 }
 
 // Complex A (M x K, interleaved) -> real-embedded A' = [Ar | Ai] (M x 2K).
 static __global__ void split_bf16_cplx_a_kernel(const float2* __restrict__ A, long long M, long long K,
-                                         long long lda, __nv_bfloat16* __restrict__ hi,
-                                         __nv_bfloat16* __restrict__ lo, long long ldo) {
+                                                long long lda, BfPlanes out, long long ldo, int ns) {
     const long long total = M * K;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
          e += (long long)gridDim.x * blockDim.x) {
         long long r = e / K, c = e - r * K;
         float2 v = A[r * lda + c];
-        __nv_bfloat16 h, l;
-        split_one(v.x, h, l);
-        hi[r * ldo + c] = h;
-        lo[r * ldo + c] = l;
-        split_one(v.y, h, l);
-        hi[r * ldo + K + c] = h;
-        lo[r * ldo + K + c] = l;
+        __nv_bfloat16 ore[3], oim[3];
+        split_n(v.x, ns, ore);
+        split_n(v.y, ns, oim);
+        for (int s = 0; s < ns; ++s) {
+            out.p[s][r * ldo + c] = ore[s];
+            out.p[s][r * ldo + K + c] = oim[s];
+        }
     }
 }
 
 // Complex B (K x N) -> B' = [[Br, Bi], [-Bi, Br]] (2K x 2N).
 static __global__ void split_bf16_cplx_b_kernel(const float2* __restrict__ B, long long K, long long N,
-                                         long long ldb, __nv_bfloat16* __restrict__ hi,
-                                         __nv_bfloat16* __restrict__ lo, long long ldo) {
+                                                long long ldb, BfPlanes out, long long ldo, int ns) {
     const long long total = K * N;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
          e += (long long)gridDim.x * blockDim.x) {
         long long r = e / N, c = e - r * N;
         float2 v = B[r * ldb + c];
-        __nv_bfloat16 hr, lr, hi_, li;
-        split_one(v.x, hr, lr);
-        split_one(v.y, hi_, li);
-        // top block row r: [Br Bi]
-        hi[r * ldo + c] = hr;
-        lo[r * ldo + c] = lr;
-        hi[r * ldo + N + c] = hi_;
-        lo[r * ldo + N + c] = li;
-        // bottom block row K + r: [-Bi Br]  (negation is exact in bf16)
-        hi[(K + r) * ldo + c] = __hneg(hi_);
-        lo[(K + r) * ldo + c] = __hneg(li);
-        hi[(K + r) * ldo + N + c] = hr;
-        lo[(K + r) * ldo + N + c] = lr;
+        __nv_bfloat16 ore[3], oim[3];
+        split_n(v.x, ns, ore);
+        split_n(v.y, ns, oim);
+        for (int s = 0; s < ns; ++s) {
+            __nv_bfloat16* P = out.p[s];
+            P[r * ldo + c] = ore[s];             // top-left      Br
+            P[r * ldo + N + c] = oim[s];         // top-right     Bi
+            P[(K + r) * ldo + c] = __hneg(oim[s]);  // bottom-left -Bi (exact)
+            P[(K + r) * ldo + N + c] = ore[s];   // bottom-right  Br
+        }
     }
 }
 

@@ -2,12 +2,6 @@
 // FG_ERR_UNSUPPORTED (never a CPU fallback).
 #include "runtime.h"
 
-namespace fgrt {
-fg_status launch_ozaki(fg_ctx*, const Gemm&, cudaStream_t) {
-    return set_error(FG_ERR_UNSUPPORTED, "Ozaki split DGEMM/ZGEMM not built yet");
-}
-}  // namespace fgrt
-
 using namespace fgrt;
 extern "C" {
 fg_status fg_gemm_grouped(fg_ctx*, fg_dtype, fg_mode, const fg_problem*, size_t, fg_stream) {

@@ -32,7 +32,7 @@
 namespace fg {
 
 enum : int { KIND_I8 = 0, KIND_BF16 = 1 };
-enum : int { EPI_I32 = 0, EPI_I16 = 1, EPI_F32 = 2, EPI_QMM = 3 };
+enum : int { EPI_I32 = 0, EPI_I16 = 1, EPI_F32 = 2, EPI_QMM = 3, EPI_OZAKI = 4 };
 
 constexpr int TC_MAX_OPS = 8;
 constexpr int TC_MAX_OPERANDS = 4;
@@ -47,7 +47,11 @@ template <int KIND_, int BN_, int STAGES_, int NA_, int NB_, int NACC_, int NOPS
 struct TcCfg {
     static constexpr int KIND = KIND_, BM = 128, BN = BN_, STAGES = STAGES_;
     // CHUNKED: K is accumulated in TMEM in chunks of p.kchunk blocks that the
-    // epilogue sums in FP32 registers (EPI_F32 only).
+    // epilogue sums in FP32 registers (EPI_F32 only), adding all NACC
+    // accumulators of the chunk (the MMA unit rounds its FP32 accumulator
+    // toward zero at every instruction, so short chunks and a separate
+    // accumulator for the small correction products keep that error below
+    // FFMA's).
     static constexpr int CHUNKED = CHUNKED_;
     static constexpr int NA = NA_, NB = NB_, NACC = NACC_, NOPS = NOPS_, EPI = EPI_;
     static constexpr int ESIZE = KIND == KIND_I8 ? 1 : 2;  // operand bytes
@@ -96,6 +100,12 @@ struct TcArgs {
     int a_zp, b_zp;
     float scale;
     int kchunk;                // CHUNKED configs: K blocks per TMEM chunk
+    // EPI_OZAKI: C (f64) (+)= oz_w * 2^(e_i + f_j) * acc; the first group of a
+    // call applies C = oz_beta * C first.  cplx_half > 0 interleaves complex.
+    const double* row_scale;
+    const double* col_scale;
+    double oz_w, oz_beta;
+    int oz_first;
     TcOp ops[TC_MAX_OPS];
     DevStatus* status;
     unsigned long long timeout_ns;
@@ -146,6 +156,7 @@ struct TcSmem {
 template <class Cfg>
 __device__ __forceinline__ void epilogue_store(const TcArgs& p, int bz, int grow, int gcol0,
                                                const uint32_t (&v)[Cfg::NACC][32]) {
+    const uint32_t (&v_)[Cfg::NACC][32] = v;
     if (grow >= p.M) return;
     const int ncols = min(32, p.N - gcol0);
     if (ncols <= 0) return;
@@ -190,6 +201,24 @@ __device__ __forceinline__ void epilogue_store(const TcArgs& p, int bz, int grow
             float o = __fmul_rn(p.scale, static_cast<float>(static_cast<int32_t>(corr)));
             if (p.accumulate) o = __fadd_rn(crow[j], o);
             crow[j] = o;
+        }
+    } else if constexpr (Cfg::EPI == EPI_OZAKI) {
+        double* cbase = static_cast<double*>(p.C) + bz * p.strideC;
+        const double rs = p.row_scale[grow] * p.oz_w;
+        const int h = p.cplx_half;
+        for (int j = 0; j < ncols; ++j) {
+            const int col = gcol0 + j;
+            const int cc = (h > 0 && col >= h) ? col - h : col;
+            double* dst = h > 0 ? cbase + (long long)grow * p.ldc + 2 * cc + (col < h ? 0 : 1)
+                                : cbase + (long long)grow * p.ldc + col;
+            // exact int32 -> f64, then power-of-two scalings (exact) and alpha
+            double v = static_cast<double>(static_cast<int32_t>(v_[0][j])) * p.col_scale[cc] * rs;
+            if (p.oz_first) {
+                if (p.oz_beta != 0.0) v = fma(p.oz_beta, *dst, v);
+            } else {
+                v = *dst + v;
+            }
+            *dst = v;
         }
     } else {  // EPI_F32
         float* cbase = static_cast<float*>(p.C) + bz * p.strideC;
@@ -420,12 +449,17 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
                         tmem + (static_cast<uint32_t>(ew * 32) << 16) + buf * Cfg::ACC_COLS;
 #pragma unroll
                     for (int c = 0; c < Cfg::BN / 32; ++c) {
-                        uint32_t v[32];
-                        tmem_ld_32x32b_x32(row_addr + c * 32, v);
-                        tmem_wait_ld();
+                        // accumulators are summed smallest first: the last
+                        // (correction products) before acc 0 (hi * hi)
 #pragma unroll
-                        for (int j = 0; j < 32; ++j)
-                            run[c * 32 + j] = __fadd_rn(run[c * 32 + j], __uint_as_float(v[j]));
+                        for (int q = Cfg::NACC - 1; q >= 0; --q) {
+                            uint32_t v[32];
+                            tmem_ld_32x32b_x32(row_addr + q * Cfg::BN + c * 32, v);
+                            tmem_wait_ld();
+#pragma unroll
+                            for (int j = 0; j < 32; ++j)
+                                run[c * 32 + j] = __fadd_rn(run[c * 32 + j], __uint_as_float(v[j]));
+                        }
                     }
                     tc_fence_before();
                     __syncwarp();

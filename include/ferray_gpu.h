@@ -118,7 +118,7 @@ fg_status fg_host_unregister(fg_ctx *ctx, void *host);
 
 /* ------------------------------------------------------------ raw GEMMs */
 /* C = alpha*A@B + beta*C, f64.  Replaces gemm_f64 (gemm/mod.rs:197-328).
- * mode SPLIT = Ozaki INT8 with `ozaki_slices` slices (0 = default 8). */
+ * mode SPLIT = Ozaki INT8 with `ozaki_slices` slices (0 = default 9, range 3..10). */
 fg_status fg_gemm_f64(fg_ctx *ctx, fg_mode mode, int ozaki_slices, size_t m, size_t n,
                       size_t k, double alpha, const double *a, const double *b, double beta,
                       double *c, fg_stream stream);
@@ -168,7 +168,10 @@ fg_status fg_quantized_matmul_noalloc(fg_ctx *ctx, size_t m, size_t n, size_t k,
                                       int accumulate, fg_stream stream);
 
 /* Generic strided form of all of the above (the reference's internal
- * drivers take lda/ldb/ldc: gemm/outer.rs:198-210).  alpha/beta point to a
+ * drivers take lda/ldb/ldc: gemm/outer.rs:198-210).  `ozaki_slices` in split
+ * mode: f64/c64, Ozaki INT8 slices (0 = 9); f32/c32, BF16 slices per operand,
+ * 2 (three products, the default for 0) or 3 (six products, exact slicing of
+ * f32, for FP32-level accuracy at half the speed).  alpha/beta point to a
  * scalar of the dtype's real type (two for complex: re, im); integer dtypes
  * ignore them and use `accumulate`. */
 fg_status fg_gemm(fg_ctx *ctx, fg_dtype dtype, fg_mode mode, int ozaki_slices, size_t m,

@@ -1,0 +1,115 @@
+"""GPU tests of the split (INT8 Ozaki) DGEMM / ZGEMM against the
+double-double oracle.
+
+Tolerances (normwise ||C - C_ref||_F / (||A||_F ||B||_F)):
+* default (9 slices), every case: K * 2^-53, the deterministic bound a plain
+  FP64 GEMM meets, plus (S+2) * 2^(2-7S) for the digit truncation and the
+  dropped slice pairs (which matters only for tiny K);
+* default slices, operands built as diag(10^(s u)) G diag(10^(s v)) with
+  spread s in {0, 4, 8}: no worse than 2x the plain FP64 kernel's error on the
+  same operands, plus a floor of 2^-60 for cases where both are near exact;
+* fewer slices: the representation bound K * 2^(6 - 7S) (digit truncation
+  below 2^-7S of the balanced row / column maxima).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+U64 = 2.0 ** -53
+
+
+def spread_operands(rng, m, k, n, s):
+    """A = diag(10^(s u)) G diag(10^(s v)) (the split-DGEMM benchmark family)."""
+    def one(r, c):
+        g = rng.standard_normal((r, c))
+        u = rng.uniform(-1, 1, r)
+        v = rng.uniform(-1, 1, c)
+        return (10.0 ** (s * u))[:, None] * g * (10.0 ** (s * v))[None, :]
+    return one(m, k), one(k, n)
+
+
+@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (17, 13, 9), (128, 256, 128), (300, 257, 129),
+                                   (513, 257, 300), (1024, 1024, 1024)])
+def test_f64_split_bound(fg, oracle, m, n, k):
+    rng = np.random.default_rng(m + 3 * n + 7 * k)
+    a = rng.uniform(-1, 1, (m, k))
+    b = rng.uniform(-1, 1, (k, n))
+    c = np.zeros((m, n))
+    assert fg.gemm_f64(m, n, k, 1.0, a, b, 0.0, c, mode="split")
+    err = oracle.error_vs_dd(a, b, c)
+    assert err <= k * U64 + 11 * 2.0 ** (2 - 63), err
+
+
+@pytest.mark.parametrize("spread", [0, 4, 8])
+def test_f64_split_vs_plain_per_spread(fg, oracle, spread):
+    rng = np.random.default_rng(100 + spread)
+    m = n = k = 768
+    a, b = spread_operands(rng, m, k, n, spread)
+    cs, cp = np.zeros((m, n)), np.zeros((m, n))
+    assert fg.gemm_f64(m, n, k, 1.0, a, b, 0.0, cs, mode="split")
+    assert fg.gemm_f64(m, n, k, 1.0, a, b, 0.0, cp, mode="plain")
+    es = oracle.error_vs_dd(a, b, cs)
+    ep = oracle.error_vs_dd(a, b, cp)
+    assert es <= 2 * ep + 2.0 ** -60, (spread, es, ep)
+
+
+@pytest.mark.parametrize("slices", [4, 5, 6, 7])
+def test_f64_split_fewer_slices(fg, oracle, slices):
+    rng = np.random.default_rng(slices)
+    m, n, k = 200, 180, 333
+    a = rng.standard_normal((m, k))
+    b = rng.standard_normal((k, n))
+    c = np.zeros((m, n))
+    assert fg.gemm_f64(m, n, k, 1.0, a, b, 0.0, c, mode="split", ozaki_slices=slices)
+    err = oracle.error_vs_dd(a, b, c)
+    assert err <= max(k * U64, k * 2.0 ** (6 - 7 * slices)), err
+
+
+def test_f64_split_alpha_beta(fg):
+    rng = np.random.default_rng(5)
+    m, n, k = 150, 260, 190
+    a, b = rng.uniform(-1, 1, (m, k)), rng.uniform(-1, 1, (k, n))
+    c0 = rng.uniform(-1, 1, (m, n))
+    c = c0.copy()
+    assert fg.gemm_f64(m, n, k, -0.75, a, b, 1.5, c, mode="split")
+    want = -0.75 * (a @ b) + 1.5 * c0
+    assert np.max(np.abs(c - want)) < 1e-12
+
+
+def test_f64_split_nonfinite_rows_and_zero_rows(fg):
+    rng = np.random.default_rng(6)
+    m, n, k = 40, 50, 60
+    a, b = rng.uniform(-1, 1, (m, k)), rng.uniform(-1, 1, (k, n))
+    a[3, 7] = np.nan
+    a[5, :] = 0.0
+    c = np.zeros((m, n))
+    assert fg.gemm_f64(m, n, k, 1.0, a, b, 0.0, c, mode="split")
+    assert np.all(np.isnan(c[3]))
+    assert np.all(c[5] == 0.0)
+    ok = [i for i in range(m) if i != 3]
+    assert np.max(np.abs(c[ok] - (a[ok] @ b))) < 1e-13
+
+
+@pytest.mark.parametrize("m,n,k", [(17, 13, 9), (128, 96, 200), (257, 129, 300)])
+def test_c64_split(fg, oracle, m, n, k):
+    rng = np.random.default_rng(k)
+    a = rng.standard_normal((m, k)) + 1j * rng.standard_normal((m, k))
+    b = rng.standard_normal((k, n)) + 1j * rng.standard_normal((k, n))
+    cs = np.zeros((m, n), np.complex128)
+    cp = np.zeros((m, n), np.complex128)
+    assert fg.gemm_c64(m, n, k, 1.0, 0.0, a, b, 0.0, 0.0, cs, mode="split")
+    assert fg.gemm_c64(m, n, k, 1.0, 0.0, a, b, 0.0, 0.0, cp)
+    es = oracle.error_vs_dd(a, b, cs)
+    ep = oracle.error_vs_dd(a, b, cp)
+    assert es <= 2 * k * U64, es
+    assert es <= 2 * ep + 2.0 ** -60, (es, ep)
+
+
+def test_split_matmul_batched_f64(fg):
+    rng = np.random.default_rng(9)
+    a = rng.standard_normal((3, 40, 70))
+    b = rng.standard_normal((70, 30))
+    got = fg.matmul(a, b, mode="split")
+    want = np.matmul(a, b)
+    assert np.max(np.abs(got - want)) < 1e-12

@@ -183,6 +183,23 @@ def test_f32_split_3xbf16(fg, oracle, m, n, k):
     assert err <= 2.0 ** -15 + k * U32, err
 
 
+@pytest.mark.parametrize("m,n,k", [(17, 13, 9), (300, 257, 129), (1024, 1024, 1024),
+                                   (2048, 2048, 2048)])
+def test_f32_split6_accuracy(fg, oracle, m, n, k):
+    # three BF16 slices represent every f32 exactly; six products leave only
+    # terms below 2^-26 |a||b| out, so the error is FP32-accumulation level:
+    # no worse than twice the plain FFMA kernel's.
+    r = rng(m + 7 * k)
+    a = r.standard_normal((m, k)).astype(np.float32)
+    b = r.standard_normal((k, n)).astype(np.float32)
+    c6, cp = np.zeros((m, n), np.float32), np.zeros((m, n), np.float32)
+    assert fg.gemm_f32(m, n, k, 1.0, a, b, 0.0, c6, mode="split", bf16_slices=3)
+    assert fg.gemm_f32(m, n, k, 1.0, a, b, 0.0, cp)
+    e6, ep = _err(oracle, a, b, c6), _err(oracle, a, b, cp)
+    assert e6 <= k * U32, e6
+    assert e6 <= 2 * ep + 2.0 ** -30, (e6, ep)
+
+
 def test_f32_split_alpha_beta(fg):
     r = rng(2)
     m, n, k = 130, 300, 77
@@ -223,14 +240,14 @@ def test_c64_alpha_beta(fg):
 
 
 @pytest.mark.parametrize("m,n,k", [(17, 13, 9), (128, 96, 200), (257, 129, 300)])
-@pytest.mark.parametrize("mode", ["plain", "split"])
-def test_c32(fg, oracle, m, n, k, mode):
+@pytest.mark.parametrize("mode,slices", [("plain", 0), ("split", 2), ("split", 3)])
+def test_c32(fg, oracle, m, n, k, mode, slices):
     r = rng(k + 1)
     a, b = _cplx(r, (m, k), np.complex64), _cplx(r, (k, n), np.complex64)
     c = np.zeros((m, n), np.complex64)
-    assert fg.gemm_c32(m, n, k, 1.0, 0.0, a, b, 0.0, 0.0, c, mode=mode)
+    assert fg.gemm_c32(m, n, k, 1.0, 0.0, a, b, 0.0, 0.0, c, mode=mode, bf16_slices=slices)
     err = _err(oracle, a, b, c)
-    tol = 2 * k * U32 if mode == "plain" else 2.0 ** -15 + 2 * k * U32
+    tol = 2 * k * U32 if (mode == "plain" or slices == 3) else 2.0 ** -15 + 2 * k * U32
     assert err <= tol, err
 
 
