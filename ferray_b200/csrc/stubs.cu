@@ -4,17 +4,6 @@
 
 using namespace fgrt;
 extern "C" {
-fg_status fg_gemm_grouped(fg_ctx*, fg_dtype, fg_mode, const fg_problem*, size_t, fg_stream) {
-    return set_error(FG_ERR_UNSUPPORTED, "grouped GEMM not built yet");
-}
-fg_status fg_grouped_plan_create(fg_ctx*, fg_dtype, fg_mode, const fg_problem*, size_t, fg_stream,
-                                 fg_grouped_plan**) {
-    return set_error(FG_ERR_UNSUPPORTED, "grouped GEMM not built yet");
-}
-fg_status fg_grouped_plan_run(fg_grouped_plan*, fg_stream) {
-    return set_error(FG_ERR_UNSUPPORTED, "grouped GEMM not built yet");
-}
-fg_status fg_grouped_plan_destroy(fg_grouped_plan*) { return FG_OK; }
 fg_status fg_server_start(fg_ctx*, size_t, int, int, fg_server**) {
     return set_error(FG_ERR_UNSUPPORTED, "server not built yet");
 }

@@ -1,0 +1,402 @@
+// tc_grouped.cuh -- persistent grouped (ragged-batch) GEMM on tcgen05.
+//
+// One launch runs `count` independent problems of different M, N, K.  A
+// device-side problem table holds, per problem, its shape, its tile range in
+// a global tile numbering (prefix sums), its output and the TMA descriptors
+// of its operands (written to global memory before the launch).  Every CTA
+// walks the global tile list with a static stride; the three warp roles of
+// tc_gemm.cuh (TMA producer, MMA issuer, epilogue) each map a tile to its
+// problem by binary search over the prefix sums, so they agree on the
+// sequence without talking to each other.  The host orders problems by
+// decreasing K so the strided walk hands every SM a similar amount of work.
+#pragma once
+#include "tc_gemm.cuh"
+
+namespace fg {
+
+struct GroupedProblem {
+    int M, N, K;
+    int k_blocks, tiles_m, tiles_n;
+    long long tile_start;  // first global tile of this problem
+    void* C;
+    long long ldc;         // elements
+};
+
+struct GroupedArgs {
+    const GroupedProblem* problems;
+    const CUtensorMap* maps;  // per problem: NA A maps then NB B maps
+    int count;
+    long long total_tiles;
+    float alpha, beta;        // EPI_F32
+    int accumulate;           // EPI_I32
+    int kchunk;
+    TcOp ops[TC_MAX_OPS];
+    DevStatus* status;
+    unsigned long long timeout_ns;
+};
+
+__device__ __forceinline__ int find_problem(const GroupedArgs& g, long long t) {
+    int lo = 0, hi = g.count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (g.problems[mid].tile_start <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <class Cfg>
+__device__ __forceinline__ void grouped_store(const GroupedArgs& g, const GroupedProblem& pr, int grow,
+                                              int gcol0, const uint32_t (&v)[32]) {
+    if (grow >= pr.M) return;
+    const int ncols = min(32, pr.N - gcol0);
+    if (ncols <= 0) return;
+    if constexpr (Cfg::EPI == EPI_I32) {
+        int32_t* crow = static_cast<int32_t*>(pr.C) + (long long)grow * pr.ldc + gcol0;
+        for (int j = 0; j < ncols; ++j) {
+            uint32_t w = v[j];
+            if (g.accumulate) w += static_cast<uint32_t>(crow[j]);
+            crow[j] = static_cast<int32_t>(w);
+        }
+    } else {
+        float* crow = static_cast<float*>(pr.C) + (long long)grow * pr.ldc + gcol0;
+        for (int j = 0; j < ncols; ++j) {
+            float o = g.alpha * __uint_as_float(v[j]);
+            if (g.beta != 0.f) o = fmaf(g.beta, crow[j], o);
+            crow[j] = o;
+        }
+    }
+}
+
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::THREADS, 1)
+    tc_grouped_kernel(const __grid_constant__ GroupedArgs g) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* base = reinterpret_cast<uint8_t*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+    TcSmem<Cfg>& s = *reinterpret_cast<TcSmem<Cfg>*>(base);
+    const int warp = threadIdx.x / 32;
+    const int lane = threadIdx.x % 32;
+    volatile int* abort = &s.abort;
+    constexpr int NMAPS = Cfg::NA + Cfg::NB;
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < Cfg::STAGES; ++i) {
+            mbar_init(&s.full[i], 1);
+            mbar_init(&s.empty[i], 1);
+        }
+        for (int i = 0; i < 4; ++i) {
+            mbar_init(&s.acc_full[i], 1);
+            mbar_init(&s.acc_empty[i], 4);
+        }
+        mbar_init(&s.drain, 1);
+        s.abort = 0;
+        fence_mbar_init();
+    }
+    if (warp == 1) {
+        tmem_alloc(&s.tmem_base, Cfg::TMEM_COLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s.tmem_base;
+
+    if (warp == 0) {
+        if (elect_one()) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int issued_parity[Cfg::STAGES];
+            for (int i = 0; i < Cfg::STAGES; ++i) issued_parity[i] = -1;
+            bool ok = true;
+            for (long long t = blockIdx.x; t < g.total_tiles && ok; t += gridDim.x) {
+                const int pi = find_problem(g, t);
+                const GroupedProblem pr = g.problems[pi];
+                const int r = static_cast<int>(t - pr.tile_start);
+                const int tm = r / pr.tiles_n, tn = r - (r / pr.tiles_n) * pr.tiles_n;
+                const CUtensorMap* mp = g.maps + (long long)pi * NMAPS;
+                for (int kb = 0; kb < pr.k_blocks; ++kb) {
+                    if (!mbar_wait(&s.empty[stage], phase ^ 1u, g.timeout_ns, g.status, 0x31, abort)) {
+                        ok = false;
+                        break;
+                    }
+                    mbar_arrive_expect_tx(&s.full[stage], Cfg::STAGE_BYTES);
+                    const int kx = kb * Cfg::BK;
+                    for (int i = 0; i < Cfg::NA; ++i)
+                        tma_load_2d(s.a[stage][i], mp + i, kx, tm * Cfg::BM, &s.full[stage]);
+                    for (int i = 0; i < Cfg::NB; ++i) {
+#pragma unroll
+                        for (int c = 0; c < Cfg::B_CHUNKS; ++c)
+                            tma_load_2d(s.b[stage][i] + c * Cfg::B_CHUNK_BYTES, mp + Cfg::NA + i,
+                                        tn * Cfg::BN + c * Cfg::B_CHUNK_ELEMS, kx, &s.full[stage]);
+                    }
+                    issued_parity[stage] = static_cast<int>(phase);
+                    if (++stage == Cfg::STAGES) {
+                        stage = 0;
+                        phase ^= 1u;
+                    }
+                }
+            }
+            if (!ok) {
+                for (int i = 0; i < Cfg::STAGES; ++i) {
+                    if (issued_parity[i] < 0) continue;
+                    volatile int never = 0;
+                    mbar_wait(&s.full[i], static_cast<uint32_t>(issued_parity[i]), g.timeout_ns, nullptr, 0, &never);
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (elect_one()) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int it = 0;
+            bool ok = true;
+            for (long long t = blockIdx.x; t < g.total_tiles && ok; t += gridDim.x) {
+                const int pi = find_problem(g, t);
+                const int kblocks = g.problems[pi].k_blocks;
+                const int kchunk = (Cfg::CHUNKED && g.kchunk > 0) ? g.kchunk : max(kblocks, 1);
+                for (int kc0 = 0; kc0 < max(kblocks, 1) && ok; kc0 += kchunk, ++it) {
+                    const int kc1 = min(kblocks, kc0 + kchunk);
+                    const int buf = it % Cfg::ACC_BUFS;
+                    const uint32_t acc_par = static_cast<uint32_t>((it / Cfg::ACC_BUFS) & 1);
+                    if (!mbar_wait(&s.acc_empty[buf], acc_par ^ 1u, g.timeout_ns, g.status, 0x41, abort)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t acc_base = tmem + buf * Cfg::ACC_COLS;
+                    for (int kb = kc0; kb < kc1; ++kb) {
+                        if (!mbar_wait(&s.full[stage], phase, g.timeout_ns, g.status, 0x42, abort)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+#pragma unroll
+                        for (int o = 0; o < Cfg::NOPS; ++o) {
+                            const TcOp op = g.ops[o];
+                            bool first_for_acc = true;
+#pragma unroll
+                            for (int q = 0; q < o; ++q)
+                                if (g.ops[q].acc == op.acc) first_for_acc = false;
+                            const uint32_t idesc = umma_idesc(Cfg::KIND == KIND_I8 ? 2u : 1u, op.a_fmt,
+                                                              op.b_fmt, 0u, 1u, Cfg::BM, Cfg::BN);
+                            const uint32_t a_addr = smem_u32(s.a[stage][op.a]);
+                            const uint32_t b_addr = smem_u32(s.b[stage][op.b]);
+#pragma unroll
+                            for (int kk = 0; kk < Cfg::KSTEPS; ++kk) {
+                                const uint64_t ad = umma_desc_sw128(a_addr + kk * Cfg::KSTEP_BYTES, 16, 1024);
+                                const uint64_t bd = umma_desc_sw128(
+                                    b_addr + kk * (Cfg::KSTEP_BYTES / Cfg::ESIZE) * 128, Cfg::B_CHUNK_BYTES, 1024);
+                                const uint32_t acc = (kb > kc0 || kk > 0 || !first_for_acc) ? 1u : 0u;
+                                if constexpr (Cfg::KIND == KIND_I8)
+                                    tc_mma_i8(acc_base + op.acc * Cfg::BN, ad, bd, idesc, acc);
+                                else
+                                    tc_mma_f16(acc_base + op.acc * Cfg::BN, ad, bd, idesc, acc);
+                            }
+                        }
+                        tc_commit(&s.empty[stage]);
+                        if (++stage == Cfg::STAGES) {
+                            stage = 0;
+                            phase ^= 1u;
+                        }
+                    }
+                    if (!ok) break;
+                    tc_commit(&s.acc_full[buf]);
+                }
+            }
+            tc_commit(&s.drain);
+            volatile int never = 0;
+            mbar_wait(&s.drain, 0, g.timeout_ns, ok ? g.status : nullptr, 0x43, &never);
+        }
+    } else {
+        const int ew = warp & 3;
+        int it = 0;
+        bool ok = true;
+        for (long long t = blockIdx.x; t < g.total_tiles && ok; t += gridDim.x) {
+            const int pi = find_problem(g, t);
+            const GroupedProblem pr = g.problems[pi];
+            const int r = static_cast<int>(t - pr.tile_start);
+            const int tm = r / pr.tiles_n, tn = r - (r / pr.tiles_n) * pr.tiles_n;
+            const int kblocks = max(pr.k_blocks, 1);
+            const int kchunk = (Cfg::CHUNKED && g.kchunk > 0) ? g.kchunk : kblocks;
+            float run[Cfg::CHUNKED ? Cfg::BN : 1];
+            if constexpr (Cfg::CHUNKED) {
+#pragma unroll
+                for (int j = 0; j < Cfg::BN; ++j) run[j] = 0.f;
+            }
+            const int grow = tm * Cfg::BM + ew * 32 + lane;
+            for (int kc0 = 0; kc0 < kblocks; kc0 += kchunk, ++it) {
+                const int buf = it % Cfg::ACC_BUFS;
+                const uint32_t acc_par = static_cast<uint32_t>((it / Cfg::ACC_BUFS) & 1);
+                if (!mbar_wait(&s.acc_full[buf], acc_par, g.timeout_ns, g.status, 0x51, abort)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t row_addr = tmem + (static_cast<uint32_t>(ew * 32) << 16) + buf * Cfg::ACC_COLS;
+                if constexpr (Cfg::CHUNKED) {
+#pragma unroll
+                    for (int c = 0; c < Cfg::BN / 32; ++c) {
+                        uint32_t v[32];
+                        tmem_ld_32x32b_x32(row_addr + c * 32, v);
+                        tmem_wait_ld();
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) run[c * 32 + j] = __fadd_rn(run[c * 32 + j], __uint_as_float(v[j]));
+                    }
+                } else {
+#pragma unroll 1
+                    for (int c = 0; c < Cfg::BN / 32; ++c) {
+                        uint32_t v[32];
+                        tmem_ld_32x32b_x32(row_addr + c * 32, v);
+                        tmem_wait_ld();
+                        grouped_store<Cfg>(g, pr, grow, tn * Cfg::BN + c * 32, v);
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&s.acc_empty[buf]);
+            }
+            if (!ok) break;
+            if constexpr (Cfg::CHUNKED) {
+#pragma unroll
+                for (int c = 0; c < Cfg::BN / 32; ++c) {
+                    uint32_t v[32];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) v[j] = __float_as_uint(run[c * 32 + j]);
+                    grouped_store<Cfg>(g, pr, grow, tn * Cfg::BN + c * 32, v);
+                }
+            }
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem, Cfg::TMEM_COLS);
+    }
+}
+
+// ------------------------------------------------------------------ prep
+// One launch over a list of segments: copy a byte matrix into a 16-byte-
+// pitched buffer (op 0) or split an f32 matrix into bf16 hi/lo planes (op 1).
+struct PrepSeg {
+    const void* src;
+    void* dst0;
+    void* dst1;
+    long long rows, cols, ld_src, ld_dst;  // elements
+    long long start;                       // first work item of this segment
+    int op;
+};
+
+static __global__ void grouped_prep_kernel(const PrepSeg* __restrict__ segs, int nseg,
+                                           long long total) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = nseg - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (segs[mid].start <= e) lo = mid;
+            else hi = mid - 1;
+        }
+        const PrepSeg sg = segs[lo];
+        const long long w = e - sg.start;  // item = one destination element
+        const long long r = w / sg.ld_dst, c = w - r * sg.ld_dst;
+        if (sg.op == 0) {
+            const uint8_t v = c < sg.cols ? static_cast<const uint8_t*>(sg.src)[r * sg.ld_src + c] : 0;
+            static_cast<uint8_t*>(sg.dst0)[r * sg.ld_dst + c] = v;
+        } else {
+            const float x = c < sg.cols ? static_cast<const float*>(sg.src)[r * sg.ld_src + c] : 0.f;
+            const __nv_bfloat16 h = __float2bfloat16_rn(x);
+            const __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
+            static_cast<__nv_bfloat16*>(sg.dst0)[r * sg.ld_dst + c] = h;
+            static_cast<__nv_bfloat16*>(sg.dst1)[r * sg.ld_dst + c] = l;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ SIMT
+// Plain FP32 grouped GEMM (FFMA): 64x64 tiles, 256 threads, 4x4 outputs per
+// thread, persistent over the global tile list.
+struct SimtGroupedArgs {
+    const GroupedProblem* problems;
+    const void* const* a;  // per problem operand pointers and leading dims
+    const void* const* b;
+    const long long* lda;
+    const long long* ldb;
+    int count;
+    long long total_tiles;
+    float alpha, beta;
+};
+
+static __device__ __forceinline__ int find_problem_simt(const SimtGroupedArgs& g, long long t) {
+    int lo = 0, hi = g.count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (g.problems[mid].tile_start <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+static __global__ void __launch_bounds__(256) simt_grouped_sgemm(const SimtGroupedArgs g) {
+    constexpr int BM = 64, BN = 64, BK = 16;
+    __shared__ float As[BK][BM + 4];
+    __shared__ float Bs[BK][BN + 4];
+    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+    for (long long t = blockIdx.x; t < g.total_tiles; t += gridDim.x) {
+        const int pi = find_problem_simt(g, t);
+        const GroupedProblem pr = g.problems[pi];
+        const float* A = static_cast<const float*>(g.a[pi]);
+        const float* B = static_cast<const float*>(g.b[pi]);
+        const long long lda = g.lda[pi], ldb = g.ldb[pi];
+        const int r = static_cast<int>(t - pr.tile_start);
+        const int m0 = (r / pr.tiles_n) * BM, n0 = (r % pr.tiles_n) * BN;
+        float acc[4][4] = {};
+        for (int k0 = 0; k0 < pr.K; k0 += BK) {
+            // A tile 64x16: 1024 elements, 4 per thread (row-major reads along k)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int e = tid + q * 256;
+                const int ar = e / BK, ac = e % BK;
+                const int gr = m0 + ar, gk = k0 + ac;
+                As[ac][ar] = (gr < pr.M && gk < pr.K) ? A[(long long)gr * lda + gk] : 0.f;
+                const int br = e / BN, bc = e % BN;
+                const int gk2 = k0 + br, gn = n0 + bc;
+                Bs[br][bc] = (gk2 < pr.K && gn < pr.N) ? B[(long long)gk2 * ldb + gn] : 0.f;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int kk = 0; kk < BK; ++kk) {
+                float af[4], bf[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    af[i] = As[kk][ty * 4 + i];
+                    bf[i] = Bs[kk][tx * 4 + i];
+                }
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(af[i], bf[j], acc[i][j]);
+            }
+            __syncthreads();
+        }
+        float* C = static_cast<float*>(pr.C);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int gr = m0 + ty * 4 + i;
+            if (gr >= pr.M) continue;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int gc = n0 + tx * 4 + j;
+                if (gc >= pr.N) continue;
+                float* p = C + (long long)gr * pr.ldc + gc;
+                float o = g.alpha * acc[i][j];
+                if (g.beta != 0.f) o = fmaf(g.beta, *p, o);
+                *p = o;
+            }
+        }
+    }
+}
+
+}  // namespace fg
