@@ -29,7 +29,8 @@ __all__ = [
     "OutOfMemory", "BudgetExceeded", "DeviceTimeout", "DeviceError", "Context", "DeviceArray",
     "default_context", "gemm_f64", "gemm_f32", "gemm_c64", "gemm_c32", "gemm_i8",
     "gemm_i8_signed", "gemm_i16", "quantized_matmul", "matmul", "matmul_complex",
-    "gemm_batched_strided", "gemm_grouped", "GroupedPlan", "launch_count", "PLAIN", "SPLIT",
+    "gemm_batched_strided", "gemm_grouped", "GroupedPlan", "Server", "launch_count", "PLAIN",
+    "SPLIT",
 ]
 
 PLAIN, SPLIT = "plain", "split"
@@ -416,3 +417,50 @@ class GroupedPlan:
         if self.handle:
             self.ctx._lib.fg_grouped_plan_destroy(self.handle)
             self.handle = None
+
+
+_REQ_DTYPE = {np.dtype(np.float64): L.FG_F64, np.dtype(np.float32): L.FG_F32,
+              np.dtype(np.complex128): L.FG_C64, np.dtype(np.complex64): L.FG_C32,
+              np.dtype(np.int8): L.FG_I8, np.dtype(np.uint8): L.FG_U8I8,
+              np.dtype(np.int16): L.FG_I16}
+
+
+class Server:
+    """Continuous-batching matmul server (fg_server_*): requests are
+    C = A @ B on DeviceArrays; many host threads may submit concurrently."""
+
+    def __init__(self, hbm_budget_bytes=40 << 30, streams=4, max_group=256, ctx=None):
+        self.ctx = ctx or default_context()
+        self._lib = self.ctx._lib
+        h = C.c_void_p()
+        check(self._lib.fg_server_start(self.ctx.handle, int(hbm_budget_bytes), int(streams),
+                                        int(max_group), C.byref(h)), "fg_server_start")
+        self.handle = h
+
+    def submit(self, a, b, c, mode=PLAIN):
+        m, k = a.shape
+        n = b.shape[1]
+        dt = _REQ_DTYPE[np.dtype(a.dtype)]
+        req = L.fg_request(dt, _mode(mode), m, n, k, a.ptr, b.ptr, c.ptr, 0)
+        t = C.c_uint64()
+        check(self._lib.fg_server_submit(self.handle, C.byref(req), C.byref(t)), "submit")
+        return t.value
+
+    def wait(self, ticket, timeout_ms=-1):
+        check(self._lib.fg_server_wait(self.handle, ticket, int(timeout_ms)), "wait")
+
+    def stats(self):
+        s = L.fg_server_stats()
+        check(self._lib.fg_server_stats_get(self.handle, C.byref(s)), "stats")
+        return {f: getattr(s, f) for f, _ in L.fg_server_stats._fields_}
+
+    def stop(self):
+        if getattr(self, "handle", None):
+            self._lib.fg_server_stop(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.stop()
+        except Exception:
+            pass

@@ -14,6 +14,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstring>
 #include <mutex>
 #include <numeric>
 #include <vector>
@@ -45,64 +46,285 @@ fg_status set_smem_attr() {
 
 }  // namespace
 
-struct fg_grouped_plan {
+// A grouped batch lowered to device form.  build() is host-only (ordering,
+// tiling, layout sizes); bind() fixes the device base address, encodes the
+// TMA descriptors and writes the tables into a host image laid out exactly
+// like the front of the device region; launch() copies that image with one
+// async memcpy and issues the prep and grouped kernels on a stream.
+struct fgrt::GroupedJob {
     fg_ctx* ctx = nullptr;
     fg_dtype dtype = FG_F32;
     fg_mode mode = FG_MODE_PLAIN;
     int kind = 0;  // 0 = FFMA, 1 = i8 tensor, 2 = bf16x3 tensor
-    void* mem = nullptr;  // one device allocation: tables, maps, segments, arena
-    GroupedArgs targs{};
-    SimtGroupedArgs sargs{};
-    PrepSeg* d_segs = nullptr;
-    int nseg = 0;
-    long long prep_total = 0;
+    struct Opnd {
+        const void* src = nullptr;
+        long long off0 = -1, off1 = -1, ld = 0;
+    };
     struct Zero {
         void* c;
         long long m, n, ldc;
-        int accumulate;
     };
-    std::vector<Zero> zeros;  // K == 0 problems
+    std::vector<fg_problem> probs_in;  // ordered, K > 0
+    std::vector<GroupedProblem> probs;
+    std::vector<Opnd> oa, ob;
+    std::vector<Zero> zeros;
     long long total_tiles = 0;
+    long long arena = 0;
+    int nseg = 0;
+    size_t sz_probs = 0, sz_maps = 0, sz_ptrs = 0, sz_segs = 0;
+    // bound state
+    void* dev = nullptr;
+    const void* host = nullptr;
+    GroupedArgs targs{};
+    SimtGroupedArgs sargs{};
+    PrepSeg* d_segs = nullptr;
+    size_t host_bytes() const { return sz_probs + sz_maps + sz_ptrs + sz_segs; }
+    size_t dev_bytes() const { return host_bytes() + static_cast<size_t>(arena); }
+};
+
+struct fg_grouped_plan {
+    fgrt::GroupedJob job;
+    void* mem = nullptr;
+    void* host = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t graph = nullptr;
 };
 
 namespace fgrt {
 
-static fg_status launch_plan(fg_grouped_plan* p, cudaStream_t st) {
-    fg_ctx* ctx = p->ctx;
-    for (auto& z : p->zeros) {
-        if (z.accumulate) continue;
-        if (p->dtype == FG_F32) {
-            scale_kernel<float><<<std::min<long long>((z.m * z.n + 255) / 256 + 1, 1024), 256, 0, st>>>(
-                static_cast<float*>(z.c), z.m, z.n, z.ldc, p->targs.beta);
-        } else {
-            scale_kernel<int><<<std::min<long long>((z.m * z.n + 255) / 256 + 1, 1024), 256, 0, st>>>(
-                static_cast<int*>(z.c), z.m, z.n, z.ldc, 0);
+GroupedJob* grouped_job_new() { return new GroupedJob(); }
+void grouped_job_free(GroupedJob* j) { delete j; }
+size_t grouped_job_dev_bytes(const GroupedJob* j) { return j->dev_bytes(); }
+size_t grouped_job_host_bytes(const GroupedJob* j) { return j->host_bytes(); }
+
+fg_status grouped_job_build(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, const fg_problem* table,
+                            size_t count, GroupedJob* j) {
+    if (!ctx || (!table && count)) return set_error(FG_ERR_INVALID, "null argument");
+    if (dtype != FG_F32 && dtype != FG_I8 && dtype != FG_U8I8)
+        return set_error(FG_ERR_DTYPE, "grouped GEMM: dtype must be FG_F32, FG_I8 or FG_U8I8");
+    if (count > (1u << 30)) return set_error(FG_ERR_UNSUPPORTED, "too many problems");
+    *j = GroupedJob();
+    j->ctx = ctx;
+    j->dtype = dtype;
+    j->mode = mode;
+    j->kind = dtype == FG_F32 ? (mode == FG_MODE_SPLIT ? 2 : 0) : 1;
+    std::vector<int> order;
+    for (size_t i = 0; i < count; ++i) {
+        const fg_problem& q = table[i];
+        if (q.m < 0 || q.n < 0 || q.k < 0)
+            return set_error(FG_ERR_SHAPE, "grouped GEMM: negative dimension in problem " + std::to_string(i));
+        if (q.m == 0 || q.n == 0) continue;
+        if (!q.c || (q.k > 0 && (!q.a || !q.b)) || q.ldc < q.n || (q.k > 0 && (q.lda < q.k || q.ldb < q.n)))
+            return set_error(FG_ERR_INVALID, "grouped GEMM: bad pointer or leading dimension in problem " + std::to_string(i));
+        if (q.m > (1 << 30) || q.n > (1 << 30) || q.k > (1 << 30) ||
+            (j->kind == 1 && q.k > (dtype == FG_I8 ? 131072 : 65536)))
+            return set_error(FG_ERR_UNSUPPORTED, "grouped GEMM: problem " + std::to_string(i) + " too large");
+        if (q.k == 0) {
+            j->zeros.push_back({q.c, q.m, q.n, q.ldc});
+            continue;
         }
+        order.push_back(static_cast<int>(i));
+    }
+    // longest K first: the static strided tile walk then balances SMs
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return table[x].k > table[y].k; });
+    const int np = static_cast<int>(order.size());
+    const int bm = j->kind == 0 ? 64 : 128, bn = bm;
+    j->probs_in.resize(np);
+    j->probs.resize(np);
+    j->oa.resize(np);
+    j->ob.resize(np);
+    int nseg = 0;
+    for (int x = 0; x < np; ++x) {
+        const fg_problem& q = table[order[x]];
+        j->probs_in[x] = q;
+        GroupedProblem& g = j->probs[x];
+        g.M = static_cast<int>(q.m);
+        g.N = static_cast<int>(q.n);
+        g.K = static_cast<int>(q.k);
+        g.tiles_m = static_cast<int>((q.m + bm - 1) / bm);
+        g.tiles_n = static_cast<int>((q.n + bn - 1) / bn);
+        g.tile_start = j->total_tiles;
+        j->total_tiles += (long long)g.tiles_m * g.tiles_n;
+        g.C = q.c;
+        g.ldc = q.ldc;
+        auto& oa = j->oa[x];
+        auto& ob = j->ob[x];
+        oa.src = q.a;
+        ob.src = q.b;
+        if (j->kind == 1) {
+            g.k_blocks = static_cast<int>((q.k + 127) / 128);
+            if ((reinterpret_cast<uintptr_t>(q.a) & 15) || (q.lda % 16)) {
+                oa.ld = rup(q.k, 16);
+                oa.off0 = j->arena;
+                j->arena = rup(j->arena + oa.ld * q.m, 256);
+                ++nseg;
+            } else {
+                oa.ld = q.lda;
+            }
+            if ((reinterpret_cast<uintptr_t>(q.b) & 15) || (q.ldb % 16)) {
+                ob.ld = rup(q.n, 16);
+                ob.off0 = j->arena;
+                j->arena = rup(j->arena + ob.ld * q.k, 256);
+                ++nseg;
+            } else {
+                ob.ld = q.ldb;
+            }
+        } else if (j->kind == 2) {
+            g.k_blocks = static_cast<int>((q.k + 63) / 64);
+            oa.ld = rup(q.k, 8);
+            oa.off0 = j->arena;
+            j->arena = rup(j->arena + 2 * oa.ld * q.m, 256);
+            oa.off1 = j->arena;
+            j->arena = rup(j->arena + 2 * oa.ld * q.m, 256);
+            ob.ld = rup(q.n, 8);
+            ob.off0 = j->arena;
+            j->arena = rup(j->arena + 2 * ob.ld * q.k, 256);
+            ob.off1 = j->arena;
+            j->arena = rup(j->arena + 2 * ob.ld * q.k, 256);
+            nseg += 2;
+        } else {
+            g.k_blocks = static_cast<int>((q.k + 15) / 16);
+            oa.ld = q.lda;
+            ob.ld = q.ldb;
+        }
+    }
+    j->nseg = nseg;
+    const int nmaps = j->kind == 2 ? 4 : 2;
+    const size_t npp = static_cast<size_t>(std::max(np, 1));
+    j->sz_probs = rup(sizeof(GroupedProblem) * npp, 256);
+    j->sz_maps = j->kind == 0 ? 0 : rup(sizeof(CUtensorMap) * nmaps * npp, 256);
+    j->sz_ptrs = j->kind == 0 ? rup((2 * sizeof(void*) + 2 * sizeof(long long)) * npp, 256) : 0;
+    j->sz_segs = rup(sizeof(PrepSeg) * std::max(nseg, 1), 256);
+    return FG_OK;
+}
+
+fg_status grouped_job_bind(GroupedJob* j, void* dev_base, void* host_stage) {
+    const int np = static_cast<int>(j->probs.size());
+    const size_t npp = static_cast<size_t>(std::max(np, 1));
+    char* dbase = static_cast<char*>(dev_base);
+    char* hbase = static_cast<char*>(host_stage);
+    const size_t o_maps = j->sz_probs, o_ptrs = o_maps + j->sz_maps, o_segs = o_ptrs + j->sz_ptrs;
+    char* d_arena = dbase + j->host_bytes();
+    std::memcpy(hbase, j->probs.data(), sizeof(GroupedProblem) * np);
+    CUtensorMap* hmaps = reinterpret_cast<CUtensorMap*>(hbase + o_maps);
+    PrepSeg* hsegs = reinterpret_cast<PrepSeg*>(hbase + o_segs);
+    int si = 0;
+    for (int x = 0; x < np; ++x) {
+        const fg_problem& q = j->probs_in[x];
+        const auto& oa = j->oa[x];
+        const auto& ob = j->ob[x];
+        if (j->kind == 1) {
+            const void* pa = q.a;
+            const void* pb = q.b;
+            if (oa.off0 >= 0) {
+                pa = d_arena + oa.off0;
+                hsegs[si++] = PrepSeg{q.a, const_cast<void*>(pa), nullptr, q.m, q.k, q.lda, oa.ld, 0, 0};
+            }
+            if (ob.off0 >= 0) {
+                pb = d_arena + ob.off0;
+                hsegs[si++] = PrepSeg{q.b, const_cast<void*>(pb), nullptr, q.k, q.n, q.ldb, ob.ld, 0, 0};
+            }
+            uint64_t da[2] = {(uint64_t)q.k, (uint64_t)q.m}, sa[1] = {(uint64_t)oa.ld};
+            uint64_t db[2] = {(uint64_t)q.n, (uint64_t)q.k}, sb[1] = {(uint64_t)ob.ld};
+            uint32_t box[2] = {128, 128};
+            FG_TRY(encode_map(&hmaps[2 * x], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, pa, da, sa, box));
+            FG_TRY(encode_map(&hmaps[2 * x + 1], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, pb, db, sb, box));
+        } else if (j->kind == 2) {
+            void* ah = d_arena + oa.off0;
+            void* al = d_arena + oa.off1;
+            void* bh = d_arena + ob.off0;
+            void* bl = d_arena + ob.off1;
+            hsegs[si++] = PrepSeg{q.a, ah, al, q.m, q.k, q.lda, oa.ld, 0, 1};
+            hsegs[si++] = PrepSeg{q.b, bh, bl, q.k, q.n, q.ldb, ob.ld, 0, 1};
+            uint64_t da[2] = {(uint64_t)q.k, (uint64_t)q.m}, sa[1] = {(uint64_t)(2 * oa.ld)};
+            uint64_t db[2] = {(uint64_t)q.n, (uint64_t)q.k}, sb[1] = {(uint64_t)(2 * ob.ld)};
+            uint32_t boxa[2] = {64, 128}, boxb[2] = {64, 64};
+            FG_TRY(encode_map(&hmaps[4 * x + 0], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, ah, da, sa, boxa));
+            FG_TRY(encode_map(&hmaps[4 * x + 1], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, al, da, sa, boxa));
+            FG_TRY(encode_map(&hmaps[4 * x + 2], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, bh, db, sb, boxb));
+            FG_TRY(encode_map(&hmaps[4 * x + 3], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, bl, db, sb, boxb));
+        }
+    }
+    if (j->kind == 0) {
+        const void** pa = reinterpret_cast<const void**>(hbase + o_ptrs);
+        const void** pb = pa + npp;
+        long long* la = reinterpret_cast<long long*>(pb + npp);
+        long long* lb = la + npp;
+        for (int x = 0; x < np; ++x) {
+            pa[x] = j->oa[x].src;
+            pb[x] = j->ob[x].src;
+            la[x] = j->oa[x].ld;
+            lb[x] = j->ob[x].ld;
+        }
+        const void** dpa = reinterpret_cast<const void**>(dbase + o_ptrs);
+        j->sargs.problems = reinterpret_cast<const GroupedProblem*>(dbase);
+        j->sargs.a = dpa;
+        j->sargs.b = dpa + npp;
+        j->sargs.lda = reinterpret_cast<const long long*>(dpa + 2 * npp);
+        j->sargs.ldb = reinterpret_cast<const long long*>(dpa + 2 * npp) + npp;
+        j->sargs.count = np;
+        j->sargs.total_tiles = j->total_tiles;
+        j->sargs.alpha = 1.f;
+        j->sargs.beta = 0.f;
+    }
+    j->d_segs = reinterpret_cast<PrepSeg*>(dbase + o_segs);
+    j->targs = GroupedArgs{};
+    j->targs.problems = reinterpret_cast<const GroupedProblem*>(dbase);
+    j->targs.maps = reinterpret_cast<const CUtensorMap*>(dbase + o_maps);
+    j->targs.count = np;
+    j->targs.total_tiles = j->total_tiles;
+    j->targs.alpha = 1.f;
+    j->targs.beta = 0.f;
+    j->targs.status = j->ctx->d_status;
+    j->targs.timeout_ns = 4000000000ull;
+    j->targs.kchunk = 2;
+    if (j->kind == 1) {
+        j->targs.ops[0] = TcOp{0, 0, 0, j->dtype == FG_I8 ? 1 : 0, 1};
+        FG_TRY(set_smem_attr<CfgGroupedI8>());
+    } else if (j->kind == 2) {
+        j->targs.ops[0] = TcOp{1, 0, 0, 1, 1};
+        j->targs.ops[1] = TcOp{0, 1, 0, 1, 1};
+        j->targs.ops[2] = TcOp{0, 0, 0, 1, 1};
+        FG_TRY(set_smem_attr<CfgGroupedBf16>());
+    }
+    j->dev = dev_base;
+    j->host = host_stage;
+    return FG_OK;
+}
+
+// Kernels only (tables already on the device).
+static fg_status grouped_job_kernels(GroupedJob* j, cudaStream_t st) {
+    fg_ctx* ctx = j->ctx;
+    for (auto& z : j->zeros) {
+        const long long blocks = std::min<long long>((z.m * z.n + 255) / 256 + 1, 1024);
+        if (j->dtype == FG_F32)
+            scale_kernel<float><<<blocks, 256, 0, st>>>(static_cast<float*>(z.c), z.m, z.n, z.ldc, 0.f);
+        else
+            scale_kernel<int><<<blocks, 256, 0, st>>>(static_cast<int*>(z.c), z.m, z.n, z.ldc, 0);
         count_launch();
     }
-    if (p->nseg > 0) {
-        const int grid = static_cast<int>(std::min<long long>((p->prep_total + 255) / 256, 8 * 148 * 4));
-        grouped_prep_kernel<<<grid, 256, 0, st>>>(p->d_segs, p->nseg, p->prep_total);
+    if (j->nseg > 0) {
+        ProfScope prof("grouped_prep", st);
+        grouped_prep_kernel<<<std::min(j->nseg, 65535), 256, 0, st>>>(j->d_segs, j->nseg, 0);
+        prof.stop();
         count_launch();
     }
-    if (p->total_tiles == 0) {
+    if (j->total_tiles == 0) {
         FG_CUDA(cudaGetLastError());
         return FG_OK;
     }
-    const int grid = static_cast<int>(std::min<long long>(p->total_tiles, ctx->sm_count));
-    if (p->kind == 0) {
+    const int grid = static_cast<int>(std::min<long long>(j->total_tiles, ctx->sm_count));
+    if (j->kind == 0) {
         ProfScope prof("simt_grouped_sgemm", st);
-        simt_grouped_sgemm<<<std::min<long long>(p->total_tiles, ctx->sm_count * 4), 256, 0, st>>>(p->sargs);
+        simt_grouped_sgemm<<<std::min<long long>(j->total_tiles, ctx->sm_count * 4), 256, 0, st>>>(j->sargs);
         prof.stop();
-    } else if (p->kind == 1) {
+    } else if (j->kind == 1) {
         ProfScope prof("tc_grouped_i8", st);
-        tc_grouped_kernel<CfgGroupedI8><<<grid, CfgGroupedI8::THREADS, tc_smem_bytes<CfgGroupedI8>(), st>>>(p->targs);
+        tc_grouped_kernel<CfgGroupedI8><<<grid, CfgGroupedI8::THREADS, tc_smem_bytes<CfgGroupedI8>(), st>>>(j->targs);
         prof.stop();
     } else {
         ProfScope prof("tc_grouped_3xbf16", st);
-        tc_grouped_kernel<CfgGroupedBf16><<<grid, CfgGroupedBf16::THREADS, tc_smem_bytes<CfgGroupedBf16>(), st>>>(p->targs);
+        tc_grouped_kernel<CfgGroupedBf16><<<grid, CfgGroupedBf16::THREADS, tc_smem_bytes<CfgGroupedBf16>(), st>>>(j->targs);
         prof.stop();
     }
     count_launch();
@@ -110,249 +332,52 @@ static fg_status launch_plan(fg_grouped_plan* p, cudaStream_t st) {
     return FG_OK;
 }
 
-static fg_status build_plan(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, const fg_problem* table,
-                            size_t count, cudaStream_t st, fg_grouped_plan** out) {
-    if (!ctx || !out || (!table && count)) return set_error(FG_ERR_INVALID, "null argument");
-    if (dtype != FG_F32 && dtype != FG_I8 && dtype != FG_U8I8)
-        return set_error(FG_ERR_DTYPE, "grouped GEMM: dtype must be FG_F32, FG_I8 or FG_U8I8");
-    if (count > (1u << 30)) return set_error(FG_ERR_UNSUPPORTED, "too many problems");
-    FG_CUDA(cudaSetDevice(ctx->device));
-    auto* p = new fg_grouped_plan();
-    p->ctx = ctx;
-    p->dtype = dtype;
-    p->mode = mode;
-    p->kind = dtype == FG_F32 ? (mode == FG_MODE_SPLIT ? 2 : 0) : 1;
-    p->targs.alpha = 1.f;
-    p->targs.beta = 0.f;
-    p->sargs.alpha = 1.f;
-    p->sargs.beta = 0.f;
-
-    // validate, drop empty problems, order by decreasing K
-    std::vector<int> order;
-    for (size_t i = 0; i < count; ++i) {
-        const fg_problem& q = table[i];
-        if (q.m < 0 || q.n < 0 || q.k < 0) {
-            delete p;
-            return set_error(FG_ERR_SHAPE, "grouped GEMM: negative dimension in problem " + std::to_string(i));
-        }
-        if (q.m == 0 || q.n == 0) continue;
-        if (!q.c || (q.k > 0 && (!q.a || !q.b)) || q.ldc < q.n || (q.k > 0 && (q.lda < q.k || q.ldb < q.n))) {
-            delete p;
-            return set_error(FG_ERR_INVALID, "grouped GEMM: bad pointer or leading dimension in problem " + std::to_string(i));
-        }
-        if (q.m > (1 << 30) || q.n > (1 << 30) || q.k > (1 << 30) ||
-            (p->kind == 1 && q.k > (dtype == FG_I8 ? 131072 : 65536))) {
-            delete p;
-            return set_error(FG_ERR_UNSUPPORTED, "grouped GEMM: problem " + std::to_string(i) + " too large");
-        }
-        if (q.k == 0) {
-            p->zeros.push_back({q.c, q.m, q.n, q.ldc, 0});
-            continue;
-        }
-        order.push_back(static_cast<int>(i));
-    }
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return table[x].k > table[y].k; });
-    const int np = static_cast<int>(order.size());
-
-    // layout of the single device allocation
-    const int nmaps = p->kind == 2 ? 4 : 2;
-    const int bm = p->kind == 0 ? 64 : 128, bn = p->kind == 0 ? 64 : 128;
-    std::vector<GroupedProblem> probs(np);
-    std::vector<PrepSeg> segs;
-    long long arena = 0;
-    struct Opnd {
-        const void* src;
-        long long off0 = -1, off1 = -1, ld;
-    };
-    std::vector<Opnd> oa(np), ob(np);
-    long long tiles = 0;
-    for (int j = 0; j < np; ++j) {
-        const fg_problem& q = table[order[j]];
-        GroupedProblem& g = probs[j];
-        g.M = static_cast<int>(q.m);
-        g.N = static_cast<int>(q.n);
-        g.K = static_cast<int>(q.k);
-        g.tiles_m = static_cast<int>((q.m + bm - 1) / bm);
-        g.tiles_n = static_cast<int>((q.n + bn - 1) / bn);
-        g.tile_start = tiles;
-        tiles += (long long)g.tiles_m * g.tiles_n;
-        g.C = q.c;
-        g.ldc = q.ldc;
-        oa[j].src = q.a;
-        ob[j].src = q.b;
-        if (p->kind == 1) {
-            g.k_blocks = static_cast<int>((q.k + 127) / 128);
-            if ((reinterpret_cast<uintptr_t>(q.a) & 15) || (q.lda % 16)) {
-                oa[j].ld = rup(q.k, 16);
-                oa[j].off0 = arena;
-                arena = rup(arena + oa[j].ld * q.m, 256);
-            } else {
-                oa[j].ld = q.lda;
-            }
-            if ((reinterpret_cast<uintptr_t>(q.b) & 15) || (q.ldb % 16)) {
-                ob[j].ld = rup(q.n, 16);
-                ob[j].off0 = arena;
-                arena = rup(arena + ob[j].ld * q.k, 256);
-            } else {
-                ob[j].ld = q.ldb;
-            }
-        } else if (p->kind == 2) {
-            g.k_blocks = static_cast<int>((q.k + 63) / 64);
-            oa[j].ld = rup(q.k, 8);
-            oa[j].off0 = arena;
-            arena = rup(arena + 2 * oa[j].ld * q.m, 256);
-            oa[j].off1 = arena;
-            arena = rup(arena + 2 * oa[j].ld * q.m, 256);
-            ob[j].ld = rup(q.n, 8);
-            ob[j].off0 = arena;
-            arena = rup(arena + 2 * ob[j].ld * q.k, 256);
-            ob[j].off1 = arena;
-            arena = rup(arena + 2 * ob[j].ld * q.k, 256);
-        } else {
-            g.k_blocks = static_cast<int>((q.k + 15) / 16);
-            oa[j].ld = q.lda;
-            ob[j].ld = q.ldb;
-        }
-    }
-    p->total_tiles = tiles;
-    const size_t sz_probs = rup(sizeof(GroupedProblem) * std::max(np, 1), 256);
-    const size_t sz_maps = rup(sizeof(CUtensorMap) * nmaps * std::max(np, 1), 256);
-    const size_t sz_ptrs = rup((2 * sizeof(void*) + 2 * sizeof(long long)) * std::max(np, 1), 256);
-    // segments are built after the arena base is known
-    const size_t max_segs = static_cast<size_t>(2 * np);
-    const size_t sz_segs = rup(sizeof(PrepSeg) * std::max<size_t>(max_segs, 1), 256);
-    const size_t total = sz_probs + sz_maps + sz_ptrs + sz_segs + arena;
-    cudaError_t e = cudaMalloc(&p->mem, total);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        delete p;
-        return set_error(FG_ERR_OOM, "grouped plan: allocation of " + std::to_string(total) + " bytes failed");
-    }
-    char* base = static_cast<char*>(p->mem);
-    GroupedProblem* d_probs = reinterpret_cast<GroupedProblem*>(base);
-    CUtensorMap* d_maps = reinterpret_cast<CUtensorMap*>(base + sz_probs);
-    char* d_ptrs = base + sz_probs + sz_maps;
-    p->d_segs = reinterpret_cast<PrepSeg*>(d_ptrs + sz_ptrs);
-    char* d_arena = d_ptrs + sz_ptrs + sz_segs;
-
-    std::vector<CUtensorMap> maps(static_cast<size_t>(nmaps) * np);
-    long long seg_total = 0;
-    auto add_seg = [&](const void* src, void* d0, void* d1, long long rows, long long cols,
-                       long long lds, long long ldd, int op) {
-        PrepSeg sgm{src, d0, d1, rows, cols, lds, ldd, seg_total, op};
-        segs.push_back(sgm);
-        seg_total += rows * ldd;
-    };
-    fg_status fs = FG_OK;
-    for (int j = 0; j < np && fs == FG_OK; ++j) {
-        const fg_problem& q = table[order[j]];
-        if (p->kind == 1) {
-            const void* pa = q.a;
-            const void* pb = q.b;
-            if (oa[j].off0 >= 0) {
-                pa = d_arena + oa[j].off0;
-                add_seg(q.a, const_cast<void*>(pa), nullptr, q.m, q.k, q.lda, oa[j].ld, 0);
-            }
-            if (ob[j].off0 >= 0) {
-                pb = d_arena + ob[j].off0;
-                add_seg(q.b, const_cast<void*>(pb), nullptr, q.k, q.n, q.ldb, ob[j].ld, 0);
-            }
-            uint64_t da[2] = {(uint64_t)q.k, (uint64_t)q.m}, sa[1] = {(uint64_t)oa[j].ld};
-            uint64_t db[2] = {(uint64_t)q.n, (uint64_t)q.k}, sb[1] = {(uint64_t)ob[j].ld};
-            uint32_t box[2] = {128, 128};
-            fs = encode_map(&maps[2 * j], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, pa, da, sa, box);
-            if (fs == FG_OK) fs = encode_map(&maps[2 * j + 1], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, pb, db, sb, box);
-        } else if (p->kind == 2) {
-            void* ah = d_arena + oa[j].off0;
-            void* al = d_arena + oa[j].off1;
-            void* bh = d_arena + ob[j].off0;
-            void* bl = d_arena + ob[j].off1;
-            add_seg(q.a, ah, al, q.m, q.k, q.lda, oa[j].ld, 1);
-            add_seg(q.b, bh, bl, q.k, q.n, q.ldb, ob[j].ld, 1);
-            uint64_t da[2] = {(uint64_t)q.k, (uint64_t)q.m}, sa[1] = {(uint64_t)(2 * oa[j].ld)};
-            uint64_t db[2] = {(uint64_t)q.n, (uint64_t)q.k}, sb[1] = {(uint64_t)(2 * ob[j].ld)};
-            uint32_t boxa[2] = {64, 128}, boxb[2] = {64, 64};
-            fs = encode_map(&maps[4 * j + 0], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, ah, da, sa, boxa);
-            if (fs == FG_OK) fs = encode_map(&maps[4 * j + 1], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, al, da, sa, boxa);
-            if (fs == FG_OK) fs = encode_map(&maps[4 * j + 2], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, bh, db, sb, boxb);
-            if (fs == FG_OK) fs = encode_map(&maps[4 * j + 3], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, bl, db, sb, boxb);
-        }
-    }
-    if (fs != FG_OK) {
-        cudaFree(p->mem);
-        delete p;
-        return fs;
-    }
-    p->nseg = static_cast<int>(segs.size());
-    p->prep_total = seg_total;
-    // tables -> device (synchronous: the host vectors go away)
-    cudaError_t ce = cudaSuccess;
-    if (np) ce = cudaMemcpyAsync(d_probs, probs.data(), sizeof(GroupedProblem) * np, cudaMemcpyHostToDevice, st);
-    if (ce == cudaSuccess && !maps.empty())
-        ce = cudaMemcpyAsync(d_maps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice, st);
-    if (ce == cudaSuccess && !segs.empty())
-        ce = cudaMemcpyAsync(p->d_segs, segs.data(), sizeof(PrepSeg) * segs.size(), cudaMemcpyHostToDevice, st);
-    std::vector<const void*> pa(np), pb(np);
-    std::vector<long long> la(np), lb(np);
-    for (int j = 0; j < np; ++j) {
-        pa[j] = oa[j].src;
-        pb[j] = ob[j].src;
-        la[j] = oa[j].ld;
-        lb[j] = ob[j].ld;
-    }
-    const void** d_pa = reinterpret_cast<const void**>(d_ptrs);
-    const void** d_pb = d_pa + std::max(np, 1);
-    long long* d_la = reinterpret_cast<long long*>(d_pb + std::max(np, 1));
-    long long* d_lb = d_la + std::max(np, 1);
-    if (ce == cudaSuccess && np) ce = cudaMemcpyAsync(d_pa, pa.data(), sizeof(void*) * np, cudaMemcpyHostToDevice, st);
-    if (ce == cudaSuccess && np) ce = cudaMemcpyAsync(d_pb, pb.data(), sizeof(void*) * np, cudaMemcpyHostToDevice, st);
-    if (ce == cudaSuccess && np) ce = cudaMemcpyAsync(d_la, la.data(), sizeof(long long) * np, cudaMemcpyHostToDevice, st);
-    if (ce == cudaSuccess && np) ce = cudaMemcpyAsync(d_lb, lb.data(), sizeof(long long) * np, cudaMemcpyHostToDevice, st);
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
-    if (ce != cudaSuccess) {
-        cudaFree(p->mem);
-        delete p;
-        return cuda_error(ce, "grouped plan upload");
-    }
-    p->targs.problems = d_probs;
-    p->targs.maps = d_maps;
-    p->targs.count = np;
-    p->targs.total_tiles = tiles;
-    p->targs.status = ctx->d_status;
-    p->targs.timeout_ns = 4000000000ull;
-    p->targs.kchunk = 2;
-    if (p->kind == 1) {
-        p->targs.ops[0] = TcOp{0, 0, 0, dtype == FG_I8 ? 1 : 0, 1};
-        fs = set_smem_attr<CfgGroupedI8>();
-    } else if (p->kind == 2) {
-        p->targs.ops[0] = TcOp{1, 0, 0, 1, 1};
-        p->targs.ops[1] = TcOp{0, 1, 0, 1, 1};
-        p->targs.ops[2] = TcOp{0, 0, 0, 1, 1};
-        fs = set_smem_attr<CfgGroupedBf16>();
-    }
-    p->sargs.problems = d_probs;
-    p->sargs.a = d_pa;
-    p->sargs.b = d_pb;
-    p->sargs.lda = d_la;
-    p->sargs.ldb = d_lb;
-    p->sargs.count = np;
-    p->sargs.total_tiles = tiles;
-    if (fs != FG_OK) {
-        cudaFree(p->mem);
-        delete p;
-        return fs;
-    }
-    *out = p;
-    return FG_OK;
+fg_status grouped_job_launch(GroupedJob* j, cudaStream_t st) {
+    if (j->host_bytes() && !j->probs.empty())
+        FG_CUDA(cudaMemcpyAsync(j->dev, j->host, j->host_bytes(), cudaMemcpyHostToDevice, st));
+    return grouped_job_kernels(j, st);
 }
 
 static void free_plan(fg_grouped_plan* p) {
     if (!p) return;
-    cudaSetDevice(p->ctx->device);
+    if (p->job.ctx) cudaSetDevice(p->job.ctx->device);
     if (p->exec) cudaGraphExecDestroy(p->exec);
     if (p->graph) cudaGraphDestroy(p->graph);
     if (p->mem) cudaFree(p->mem);
+    if (p->host) cudaFreeHost(p->host);
     delete p;
+}
+
+// Plan: build + device/pinned memory + synchronous table upload.
+static fg_status make_plan(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, const fg_problem* table,
+                           size_t count, cudaStream_t st, fg_grouped_plan** out) {
+    if (!ctx) return set_error(FG_ERR_INVALID, "null context");
+    FG_CUDA(cudaSetDevice(ctx->device));
+    auto* p = new fg_grouped_plan();
+    fg_status s = grouped_job_build(ctx, dtype, mode, table, count, &p->job);
+    if (s != FG_OK) {
+        delete p;
+        return s;
+    }
+    cudaError_t e = cudaMalloc(&p->mem, std::max<size_t>(p->job.dev_bytes(), 256));
+    if (e == cudaSuccess) e = cudaMallocHost(&p->host, std::max<size_t>(p->job.host_bytes(), 256));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        free_plan(p);
+        return set_error(FG_ERR_OOM, "grouped plan: allocation failed");
+    }
+    s = grouped_job_bind(&p->job, p->mem, p->host);
+    if (s == FG_OK && !p->job.probs.empty()) {
+        e = cudaMemcpyAsync(p->mem, p->host, p->job.host_bytes(), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) s = cuda_error(e, "grouped plan upload");
+    }
+    if (s != FG_OK) {
+        free_plan(p);
+        return s;
+    }
+    *out = p;
+    return FG_OK;
 }
 
 }  // namespace fgrt
@@ -366,8 +391,8 @@ fg_status fg_gemm_grouped(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, const fg_pr
     if (!ctx) return set_error(FG_ERR_INVALID, "null context");
     cudaStream_t st = stream_of(ctx, stream);
     fg_grouped_plan* p = nullptr;
-    FG_TRY(build_plan(ctx, dtype, mode, table, count, st, &p));
-    fg_status s = launch_plan(p, st);
+    FG_TRY(make_plan(ctx, dtype, mode, table, count, st, &p));
+    fg_status s = grouped_job_kernels(&p->job, st);
     cudaError_t e = cudaStreamSynchronize(st);  // the plan's memory is freed next
     free_plan(p);
     if (s != FG_OK) return s;
@@ -379,27 +404,30 @@ fg_status fg_grouped_plan_create(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, cons
                                  size_t count, fg_stream stream, fg_grouped_plan** out) {
     if (!out) return set_error(FG_ERR_INVALID, "null out");
     *out = nullptr;
+    if (!ctx) return set_error(FG_ERR_INVALID, "null context");
     cudaStream_t st = stream_of(ctx, stream);
     fg_grouped_plan* p = nullptr;
-    FG_TRY(build_plan(ctx, dtype, mode, table, count, st, &p));
+    FG_TRY(make_plan(ctx, dtype, mode, table, count, st, &p));
     // Capture the launch sequence once; runs replay it.
     cudaStream_t cap;
     cudaError_t e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
     fg_status s = FG_OK;
     if (e == cudaSuccess) {
-        const int prof = g_prof_on.exchange(0);  // no event records inside the graph
-        s = launch_plan(p, cap);
-        g_prof_on.store(prof);
-        cudaGraph_t graph = nullptr;
-        cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
-        if (e2 == cudaSuccess) {
-            p->graph = graph;
-            e2 = cudaGraphInstantiate(&p->exec, graph, 0);
+        e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            const int prof = g_prof_on.exchange(0);  // no event records inside the graph
+            s = grouped_job_kernels(&p->job, cap);
+            g_prof_on.store(prof);
+            cudaGraph_t graph = nullptr;
+            cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
+            if (e2 == cudaSuccess) {
+                p->graph = graph;
+                e2 = cudaGraphInstantiate(&p->exec, graph, 0);
+            }
+            e = e2;
         }
-        if (e == cudaSuccess) e = e2;
+        cudaStreamDestroy(cap);
     }
-    cudaStreamDestroy(cap);
     if (s != FG_OK || e != cudaSuccess) {
         free_plan(p);
         return s != FG_OK ? s : cuda_error(e, "grouped plan capture");
@@ -410,12 +438,12 @@ fg_status fg_grouped_plan_create(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, cons
 
 fg_status fg_grouped_plan_run(fg_grouped_plan* p, fg_stream stream) {
     if (!p) return set_error(FG_ERR_INVALID, "null plan");
-    FG_CUDA(cudaSetDevice(p->ctx->device));
-    cudaStream_t st = stream_of(p->ctx, stream);
-    ProfScope prof(p->kind == 0 ? "grouped_plan_ffma" : p->kind == 1 ? "grouped_plan_i8" : "grouped_plan_3xbf16", st);
+    FG_CUDA(cudaSetDevice(p->job.ctx->device));
+    cudaStream_t st = stream_of(p->job.ctx, stream);
+    ProfScope prof(p->job.kind == 0 ? "grouped_plan_ffma" : p->job.kind == 1 ? "grouped_plan_i8" : "grouped_plan_3xbf16", st);
     FG_CUDA(cudaGraphLaunch(p->exec, st));
     prof.stop();
-    count_launch(1 + (p->nseg > 0 ? 1 : 0) + p->zeros.size());
+    count_launch(1 + (p->job.nseg > 0 ? 1 : 0) + p->job.zeros.size());
     return FG_OK;
 }
 

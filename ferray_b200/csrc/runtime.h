@@ -155,6 +155,18 @@ fg_status launch_qmm(fg_ctx* ctx, long long M, long long N, long long K, const u
                      int a_zp, float scale, const int8_t* b, int b_zp, float* c,
                      int accumulate, cudaStream_t st);
 
+// Grouped batches in device form (grouped.cu): build (host layout) ->
+// bind (device base + host staging image) -> launch (async upload + kernels).
+struct GroupedJob;
+GroupedJob* grouped_job_new();
+void grouped_job_free(GroupedJob* j);
+fg_status grouped_job_build(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, const fg_problem* table,
+                            size_t count, GroupedJob* j);
+size_t grouped_job_dev_bytes(const GroupedJob* j);
+size_t grouped_job_host_bytes(const GroupedJob* j);
+fg_status grouped_job_bind(GroupedJob* j, void* dev_base, void* host_stage);
+fg_status grouped_job_launch(GroupedJob* j, cudaStream_t st);
+
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no
 // link-time dependency on libcuda).
 fg_status encode_map(CUtensorMap* map, CUtensorMapDataType dt, int rank, const void* base,

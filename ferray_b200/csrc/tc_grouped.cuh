@@ -45,27 +45,35 @@ __device__ __forceinline__ int find_problem(const GroupedArgs& g, long long t) {
     return lo;
 }
 
+// Stores one warp's 32 rows x 32 columns: lane l holds row row0 + l.  The
+// block goes through a padded shared-memory tile so that the global stores
+// (and the reads of C for accumulate / beta) are 128-byte row segments.
 template <class Cfg>
-__device__ __forceinline__ void grouped_store(const GroupedArgs& g, const GroupedProblem& pr, int grow,
-                                              int gcol0, const uint32_t (&v)[32]) {
-    if (grow >= pr.M) return;
-    const int ncols = min(32, pr.N - gcol0);
-    if (ncols <= 0) return;
-    if constexpr (Cfg::EPI == EPI_I32) {
-        int32_t* crow = static_cast<int32_t*>(pr.C) + (long long)grow * pr.ldc + gcol0;
-        for (int j = 0; j < ncols; ++j) {
-            uint32_t w = v[j];
-            if (g.accumulate) w += static_cast<uint32_t>(crow[j]);
-            crow[j] = static_cast<int32_t>(w);
-        }
-    } else {
-        float* crow = static_cast<float*>(pr.C) + (long long)grow * pr.ldc + gcol0;
-        for (int j = 0; j < ncols; ++j) {
-            float o = g.alpha * __uint_as_float(v[j]);
-            if (g.beta != 0.f) o = fmaf(g.beta, crow[j], o);
-            crow[j] = o;
+__device__ __forceinline__ void grouped_store(const GroupedArgs& g, const GroupedProblem& pr, int row0,
+                                              int col0, const uint32_t (&v)[32], uint32_t (*stg)[33],
+                                              int lane) {
+#pragma unroll
+    for (int j = 0; j < 32; ++j) stg[lane][j] = v[j];
+    __syncwarp();
+    const int col = col0 + lane;
+    const int rows = min(32, pr.M - row0);
+    if (col < pr.N) {
+        for (int r = 0; r < rows; ++r) {
+            const long long off = (long long)(row0 + r) * pr.ldc + col;
+            if constexpr (Cfg::EPI == EPI_I32) {
+                int32_t* p = static_cast<int32_t*>(pr.C) + off;
+                uint32_t w = stg[r][lane];
+                if (g.accumulate) w += static_cast<uint32_t>(*p);
+                *p = static_cast<int32_t>(w);
+            } else {
+                float* p = static_cast<float*>(pr.C) + off;
+                float o = g.alpha * __uint_as_float(stg[r][lane]);
+                if (g.beta != 0.f) o = fmaf(g.beta, *p, o);
+                *p = o;
+            }
         }
     }
+    __syncwarp();
 }
 
 template <class Cfg>
@@ -210,6 +218,8 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
         }
     } else {
         const int ew = warp & 3;
+        __shared__ uint32_t epi_stage[4][32][33];
+        uint32_t (*stg)[33] = epi_stage[ew];
         int it = 0;
         bool ok = true;
         for (long long t = blockIdx.x; t < g.total_tiles && ok; t += gridDim.x) {
@@ -224,7 +234,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
 #pragma unroll
                 for (int j = 0; j < Cfg::BN; ++j) run[j] = 0.f;
             }
-            const int grow = tm * Cfg::BM + ew * 32 + lane;
+            const int row0 = tm * Cfg::BM + ew * 32;
             for (int kc0 = 0; kc0 < kblocks; kc0 += kchunk, ++it) {
                 const int buf = it % Cfg::ACC_BUFS;
                 const uint32_t acc_par = static_cast<uint32_t>((it / Cfg::ACC_BUFS) & 1);
@@ -249,7 +259,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
                         uint32_t v[32];
                         tmem_ld_32x32b_x32(row_addr + c * 32, v);
                         tmem_wait_ld();
-                        grouped_store<Cfg>(g, pr, grow, tn * Cfg::BN + c * 32, v);
+                        grouped_store<Cfg>(g, pr, row0, tn * Cfg::BN + c * 32, v, stg, lane);
                     }
                 }
                 tc_fence_before();
@@ -263,7 +273,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
                     uint32_t v[32];
 #pragma unroll
                     for (int j = 0; j < 32; ++j) v[j] = __float_as_uint(run[c * 32 + j]);
-                    grouped_store<Cfg>(g, pr, grow, tn * Cfg::BN + c * 32, v);
+                    grouped_store<Cfg>(g, pr, row0, tn * Cfg::BN + c * 32, v, stg, lane);
                 }
             }
         }
@@ -280,37 +290,52 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
 // ------------------------------------------------------------------ prep
 // One launch over a list of segments: copy a byte matrix into a 16-byte-
 // pitched buffer (op 0) or split an f32 matrix into bf16 hi/lo planes (op 1).
+// Work is one destination row per warp: the warp finds its segment once
+// (binary search over the segments' first rows) and its lanes stride over
+// the row, so loads and stores are coalesced along the row.
 struct PrepSeg {
     const void* src;
     void* dst0;
     void* dst1;
     long long rows, cols, ld_src, ld_dst;  // elements
-    long long start;                       // first work item of this segment
+    long long start;                       // first global row of this segment
     int op;
 };
 
 static __global__ void grouped_prep_kernel(const PrepSeg* __restrict__ segs, int nseg,
-                                           long long total) {
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-         e += (long long)gridDim.x * blockDim.x) {
-        int lo = 0, hi = nseg - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (segs[mid].start <= e) lo = mid;
-            else hi = mid - 1;
-        }
-        const PrepSeg sg = segs[lo];
-        const long long w = e - sg.start;  // item = one destination element
-        const long long r = w / sg.ld_dst, c = w - r * sg.ld_dst;
-        if (sg.op == 0) {
-            const uint8_t v = c < sg.cols ? static_cast<const uint8_t*>(sg.src)[r * sg.ld_src + c] : 0;
-            static_cast<uint8_t*>(sg.dst0)[r * sg.ld_dst + c] = v;
-        } else {
-            const float x = c < sg.cols ? static_cast<const float*>(sg.src)[r * sg.ld_src + c] : 0.f;
-            const __nv_bfloat16 h = __float2bfloat16_rn(x);
-            const __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
-            static_cast<__nv_bfloat16*>(sg.dst0)[r * sg.ld_dst + c] = h;
-            static_cast<__nv_bfloat16*>(sg.dst1)[r * sg.ld_dst + c] = l;
+                                           long long total_rows) {
+    // One block per segment (grid-stride over segments).  Each thread owns
+    // groups of 4 destination elements (ld_dst is a multiple of 4): it issues
+    // the 4 source loads independently and writes one 4- or 8-byte word, so
+    // many loads are in flight per thread.
+    (void)total_rows;
+    for (int si = blockIdx.x; si < nseg; si += gridDim.x) {
+        const PrepSeg sg = segs[si];
+        const long long q = sg.ld_dst / 4;  // groups per row
+        const long long groups = sg.rows * q;
+        for (long long e = threadIdx.x; e < groups; e += blockDim.x) {
+            const long long r = e / q, c = (e - r * q) * 4;
+            if (sg.op == 0) {
+                const uint8_t* src = static_cast<const uint8_t*>(sg.src) + r * sg.ld_src;
+                uint32_t w = 0;
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (c + j < sg.cols) w |= static_cast<uint32_t>(src[c + j]) << (8 * j);
+                *reinterpret_cast<uint32_t*>(static_cast<uint8_t*>(sg.dst0) + r * sg.ld_dst + c) = w;
+            } else {
+                const float* src = static_cast<const float*>(sg.src) + r * sg.ld_src;
+                __align__(8) __nv_bfloat16 h[4], l[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const float x = c + j < sg.cols ? src[c + j] : 0.f;
+                    h[j] = __float2bfloat16_rn(x);
+                    l[j] = __float2bfloat16_rn(x - __bfloat162float(h[j]));
+                }
+                *reinterpret_cast<uint2*>(static_cast<__nv_bfloat16*>(sg.dst0) + r * sg.ld_dst + c) =
+                    *reinterpret_cast<const uint2*>(h);
+                *reinterpret_cast<uint2*>(static_cast<__nv_bfloat16*>(sg.dst1) + r * sg.ld_dst + c) =
+                    *reinterpret_cast<const uint2*>(l);
+            }
         }
     }
 }
