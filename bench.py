@@ -49,6 +49,11 @@ def parse():
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the DGEMM / grouped / serving side measurements")
+    ap.add_argument("--serving", action="store_true", help="only the served-stream sweep")
+    ap.add_argument("--rates", default="1000,3000,10000,30000,100000")
+    ap.add_argument("--requests", type=int, default=2000)
     return ap.parse_args()
 
 
@@ -189,6 +194,15 @@ def cpu_baseline(n):
 
 def main():
     args = parse()
+    if args.serving:
+        import bench_serving
+        import ferray_b200 as fg
+        from ferray_b200 import _lib as L
+        ctx = fg.Context(0)
+        rates = [float(x) for x in args.rates.split(",")]
+        res = bench_serving.sweep(fg, L, ctx._lib, ctx, rates, args.requests)
+        print(json.dumps({"serving": res}), flush=True)
+        return
     if args.impl == "reference":
         reference_arm(args)
         return
