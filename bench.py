@@ -170,6 +170,97 @@ def reference_arm(args):
     print(json.dumps(out), flush=True)
 
 
+def _time_calls(torch, stream, fn, steps, warmup):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def side_measurements(fg, L, lib, ctx, stream, n):
+    """The other configs, one short measurement each (device-timed):
+    DGEMM plain vs Ozaki split at N=n with their DD-oracle errors; square i8
+    at N=n (bit-exact on a sampled block); the 4096-problem ragged batch as one
+    grouped graph replay vs a loop of per-problem launches; the served stream
+    at 10k req/s, server vs plain one-call-at-a-time."""
+    import torch
+    import oracle
+    import bench_serving
+    sh = C.c_void_p(stream.cuda_stream)
+    res = {}
+    rng = np.random.default_rng(SEED)
+    # --- DGEMM plain vs split (spread 0 operands, N(0,1))
+    a = rng.standard_normal((n, n))
+    b = rng.standard_normal((n, n))
+    da, db = fg.DeviceArray.from_numpy(a, ctx), fg.DeviceArray.from_numpy(b, ctx)
+    dc = fg.DeviceArray((n, n), np.float64, ctx)
+    rows, cols = oracle.sample_indices(n, n, 48, 48, seed=11)
+    ref = oracle.dd_sampled(a, b, rows, cols)
+    na, nb = oracle.fro(a), oracle.fro(b)
+    d = {}
+    for name, mode in (("plain", L.FG_MODE_PLAIN), ("split_ozaki9", L.FG_MODE_SPLIT)):
+        ms = _time_calls(torch, stream, lambda: lib.fg_gemm_f64(ctx.handle, mode, 0, n, n, n, 1.0, da.ptr,
+                                                                  db.ptr, 0.0, dc.ptr, sh), 3, 1)
+        err = oracle.normwise_error(dc.to_numpy()[np.ix_(rows, cols)], ref, n, n, na, nb)
+        d[name] = {"tflops": round(2.0 * n ** 3 / ms / 1e9, 2), "ms": round(ms, 3), "normwise_err": err}
+    d["split_over_plain"] = round(d["split_ozaki9"]["tflops"] / d["plain"]["tflops"], 2)
+    res["dgemm_f64_%d" % n] = d
+    del da, db, dc
+    # --- square i8
+    a8 = rng.integers(-128, 128, (n, n), dtype=np.int8)
+    b8 = rng.integers(-128, 128, (n, n), dtype=np.int8)
+    da, db = fg.DeviceArray.from_numpy(a8, ctx), fg.DeviceArray.from_numpy(b8, ctx)
+    dc = fg.DeviceArray((n, n), np.int32, ctx)
+    ms = _time_calls(torch, stream, lambda: lib.fg_gemm_i8_signed(ctx.handle, n, n, n, da.ptr, db.ptr,
+                                                                    dc.ptr, 0, sh), 10, 3)
+    r8, c8 = oracle.sample_indices(n, n, 32, 32, seed=5)
+    got = dc.to_numpy()[np.ix_(r8, c8)]
+    want = (a8[r8].astype(np.int64) @ b8[:, c8].astype(np.int64)).astype(np.int32)
+    res["i8_square_%d" % n] = {"tops": round(2.0 * n ** 3 / ms / 1e9, 1), "ms": round(ms, 4),
+                               "bit_exact_sampled": bool(np.array_equal(got, want))}
+    del da, db, dc
+    # --- ragged grouped batch, 4096 problems, dims log-uniform in [8, 512]
+    dims = np.rint(np.exp(rng.uniform(np.log(8), np.log(512), (4096, 3)))).astype(int)
+    gflop = float(sum(2.0 * m * nn * k for m, nn, k in dims)) / 1e9
+    g = {}
+    for name, dt, mode in (("i8", L.FG_I8, 0), ("f32_split", L.FG_F32, 1), ("f32_plain", L.FG_F32, 0)):
+        es = 1 if dt == L.FG_I8 else 4
+        bufs, tab = [], (L.fg_problem * len(dims))()
+        for i, (m, nn, k) in enumerate(dims):
+            ta = torch.randint(-100, 100, (m * k * es,), dtype=torch.int8, device="cuda")
+            tb = torch.randint(-100, 100, (k * nn * es,), dtype=torch.int8, device="cuda")
+            if es == 4:
+                ta, tb = torch.randn(m * k, device="cuda"), torch.randn(k * nn, device="cuda")
+            tc = torch.zeros(m * nn * 4, dtype=torch.int8, device="cuda")
+            bufs.append((ta, tb, tc))
+            tab[i] = L.fg_problem(m, nn, k, ta.data_ptr(), tb.data_ptr(), tc.data_ptr(), k, nn, nn)
+        h = C.c_void_p()
+        assert lib.fg_grouped_plan_create(ctx.handle, dt, mode, tab, len(dims), sh, C.byref(h)) == 0
+        ms_g = _time_calls(torch, stream, lambda: lib.fg_grouped_plan_run(h, sh), 10, 3)
+        al, be = (C.c_float * 1)(1.0), (C.c_float * 1)(0.0)
+
+        def loop():
+            for (m, nn, k), (ta, tb, tc) in zip(dims, bufs):
+                lib.fg_gemm(ctx.handle, dt, mode, 0, int(m), int(nn), int(k), al, ta.data_ptr(), int(k),
+                            tb.data_ptr(), int(nn), be, tc.data_ptr(), int(nn), 0, sh)
+        ms_l = _time_calls(torch, stream, loop, 1, 1)
+        lib.fg_grouped_plan_destroy(h)
+        g[name] = {"grouped_ms": round(ms_g, 4), "grouped_tflops": round(gflop / ms_g, 2),
+                   "loop_ms": round(ms_l, 3), "speedup_vs_loop": round(ms_l / ms_g, 1)}
+        del bufs
+    res["ragged_4096"] = {"gflop": round(gflop, 2), **g}
+    torch.cuda.empty_cache()
+    # --- served stream, one rate
+    res["serving_10k_req_s"] = bench_serving.sweep(fg, L, lib, ctx, [10000.0], 1500)[0]
+    return res
+
+
 def cpu_baseline(n):
     """Oracle port of ferray's SGEMM on the host: a ~10 s bounded sample."""
     import oracle
@@ -285,6 +376,25 @@ def main():
     c_plain = dc.to_numpy()[np.ix_(rows, cols)]
     err_split = oracle.normwise_error(c_split, ref, n, n, na, nb)
     err_plain = oracle.normwise_error(c_plain, ref, n, n, na, nb)
+    # the 6-product (3 BF16 slices) variant, reported beside the 3-product form
+    al32, be32 = (C.c_float * 1)(1.0), (C.c_float * 1)(0.0)
+
+    def step6():
+        st = lib.fg_gemm(ctx.handle, L.FG_F32, L.FG_MODE_SPLIT, 3, n, n, n, al32, da.ptr, n, db.ptr, n,
+                         be32, dc.ptr, n, 0, sh)
+        if st != 0:
+            raise RuntimeError(lib.fg_last_error().decode())
+    for _ in range(2):
+        step6()
+    torch.cuda.synchronize()
+    e6a, e6b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e6a.record(stream)
+    for _ in range(3):
+        step6()
+    e6b.record(stream)
+    torch.cuda.synchronize()
+    ms_split6 = e6a.elapsed_time(e6b) / 3
+    err_split6 = oracle.normwise_error(dc.to_numpy()[np.ix_(rows, cols)], ref, n, n, na, nb)
 
     flops = 2.0 * n ** 3
     tf_split = flops / (ms_split * 1e-3) / 1e12
@@ -364,6 +474,10 @@ def main():
                   "normwise_err": err_plain, "kernel": "simt_sgemm"},
         "split_over_plain": round(tf_split / tf_plain, 3),
         "err_split_over_plain": round(err_split / err_plain, 3) if err_plain else None,
+        "split6": {"tflops": round(flops / (ms_split6 * 1e-3) / 1e12, 3), "ms": round(ms_split6, 4),
+                   "normwise_err": err_split6,
+                   "err_over_plain": round(err_split6 / err_plain, 3) if err_plain else None,
+                   "note": "3 BF16 slices, 6 products: exact slicing of f32"},
         "roofline": roofline,
         "kernels": {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in prof_split.items()},
         "gpu_launches": int(launches),
@@ -372,6 +486,8 @@ def main():
     }
     if not args.no_cpu and world == 1:
         out["cpu_baseline"] = cpu_baseline(n)
+    if not args.no_extra and world == 1:
+        out["other_configs"] = side_measurements(fg, L, lib, ctx, stream, n)
     print(json.dumps(out), flush=True)
     if dist:
         dist.destroy_process_group()
