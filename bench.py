@@ -54,7 +54,44 @@ def parse():
     ap.add_argument("--serving", action="store_true", help="only the served-stream sweep")
     ap.add_argument("--rates", default="1000,3000,10000,30000,100000")
     ap.add_argument("--requests", type=int, default=2000)
+    ap.add_argument("--peaks", action="store_true",
+                    help="measure library reference rates (cuBLAS via torch) for INT8, FP64, FP32")
+    ap.add_argument("--side", default="",
+                    help="run one side measurement only: dgemm, i8, ragged or serving")
     return ap.parse_args()
+
+
+def reference_peaks(n=8192):
+    """Library reference rates on this GPU (burst, best of 5, CUDA events):
+    torch._int_mm (cuBLASLt INT8 -> INT32), torch.matmul in f64 and in f32
+    with TF32 off.  They are the denominators for the kernels whose dtype
+    MEASURED_PEAKS.json does not cover."""
+    import torch
+    torch.backends.cuda.matmul.allow_tf32 = False
+    out = {}
+    cases = {"int8_tops": (torch.int8, lambda a, b: torch._int_mm(a, b)),
+             "fp64_tflops": (torch.float64, torch.matmul),
+             "fp32_tflops": (torch.float32, torch.matmul)}
+    for name, (dt, fn) in cases.items():
+        if dt == torch.int8:
+            a = torch.randint(-128, 128, (n, n), dtype=dt, device="cuda")
+            b = torch.randint(-128, 128, (n, n), dtype=dt, device="cuda")
+        else:
+            a = torch.randn(n, n, dtype=dt, device="cuda")
+            b = torch.randn(n, n, dtype=dt, device="cuda")
+        for _ in range(3):
+            fn(a, b)
+        best = 1e30
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        out[name] = round(2.0 * n ** 3 / best / 1e9, 1)
+        del a, b
+    return {"reference_peaks": out, "n": n, "how": "best of 5 after 3 warm-ups, CUDA events"}
 
 
 def dist_env():
@@ -183,7 +220,7 @@ def _time_calls(torch, stream, fn, steps, warmup):
     return e0.elapsed_time(e1) / steps
 
 
-def side_measurements(fg, L, lib, ctx, stream, n):
+def side_measurements(fg, L, lib, ctx, stream, n, only=""):
     """The other configs, one short measurement each (device-timed):
     DGEMM plain vs Ozaki split at N=n with their DD-oracle errors; square i8
     at N=n (bit-exact on a sampled block); the 4096-problem ragged batch as one
@@ -195,69 +232,73 @@ def side_measurements(fg, L, lib, ctx, stream, n):
     sh = C.c_void_p(stream.cuda_stream)
     res = {}
     rng = np.random.default_rng(SEED)
-    # --- DGEMM plain vs split (spread 0 operands, N(0,1))
-    a = rng.standard_normal((n, n))
-    b = rng.standard_normal((n, n))
-    da, db = fg.DeviceArray.from_numpy(a, ctx), fg.DeviceArray.from_numpy(b, ctx)
-    dc = fg.DeviceArray((n, n), np.float64, ctx)
-    rows, cols = oracle.sample_indices(n, n, 48, 48, seed=11)
-    ref = oracle.dd_sampled(a, b, rows, cols)
-    na, nb = oracle.fro(a), oracle.fro(b)
-    d = {}
-    for name, mode in (("plain", L.FG_MODE_PLAIN), ("split_ozaki9", L.FG_MODE_SPLIT)):
-        ms = _time_calls(torch, stream, lambda: lib.fg_gemm_f64(ctx.handle, mode, 0, n, n, n, 1.0, da.ptr,
-                                                                  db.ptr, 0.0, dc.ptr, sh), 3, 1)
-        err = oracle.normwise_error(dc.to_numpy()[np.ix_(rows, cols)], ref, n, n, na, nb)
-        d[name] = {"tflops": round(2.0 * n ** 3 / ms / 1e9, 2), "ms": round(ms, 3), "normwise_err": err}
-    d["split_over_plain"] = round(d["split_ozaki9"]["tflops"] / d["plain"]["tflops"], 2)
-    res["dgemm_f64_%d" % n] = d
-    del da, db, dc
-    # --- square i8
-    a8 = rng.integers(-128, 128, (n, n), dtype=np.int8)
-    b8 = rng.integers(-128, 128, (n, n), dtype=np.int8)
-    da, db = fg.DeviceArray.from_numpy(a8, ctx), fg.DeviceArray.from_numpy(b8, ctx)
-    dc = fg.DeviceArray((n, n), np.int32, ctx)
-    ms = _time_calls(torch, stream, lambda: lib.fg_gemm_i8_signed(ctx.handle, n, n, n, da.ptr, db.ptr,
-                                                                    dc.ptr, 0, sh), 10, 3)
-    r8, c8 = oracle.sample_indices(n, n, 32, 32, seed=5)
-    got = dc.to_numpy()[np.ix_(r8, c8)]
-    want = (a8[r8].astype(np.int64) @ b8[:, c8].astype(np.int64)).astype(np.int32)
-    res["i8_square_%d" % n] = {"tops": round(2.0 * n ** 3 / ms / 1e9, 1), "ms": round(ms, 4),
-                               "bit_exact_sampled": bool(np.array_equal(got, want))}
-    del da, db, dc
-    # --- ragged grouped batch, 4096 problems, dims log-uniform in [8, 512]
-    dims = np.rint(np.exp(rng.uniform(np.log(8), np.log(512), (4096, 3)))).astype(int)
-    gflop = float(sum(2.0 * m * nn * k for m, nn, k in dims)) / 1e9
-    g = {}
-    for name, dt, mode in (("i8", L.FG_I8, 0), ("f32_split", L.FG_F32, 1), ("f32_plain", L.FG_F32, 0)):
-        es = 1 if dt == L.FG_I8 else 4
-        bufs, tab = [], (L.fg_problem * len(dims))()
-        for i, (m, nn, k) in enumerate(dims):
-            ta = torch.randint(-100, 100, (m * k * es,), dtype=torch.int8, device="cuda")
-            tb = torch.randint(-100, 100, (k * nn * es,), dtype=torch.int8, device="cuda")
-            if es == 4:
-                ta, tb = torch.randn(m * k, device="cuda"), torch.randn(k * nn, device="cuda")
-            tc = torch.zeros(m * nn * 4, dtype=torch.int8, device="cuda")
-            bufs.append((ta, tb, tc))
-            tab[i] = L.fg_problem(m, nn, k, ta.data_ptr(), tb.data_ptr(), tc.data_ptr(), k, nn, nn)
-        h = C.c_void_p()
-        assert lib.fg_grouped_plan_create(ctx.handle, dt, mode, tab, len(dims), sh, C.byref(h)) == 0
-        ms_g = _time_calls(torch, stream, lambda: lib.fg_grouped_plan_run(h, sh), 10, 3)
-        al, be = (C.c_float * 1)(1.0), (C.c_float * 1)(0.0)
+    if not only or only == "dgemm":
+        # --- DGEMM plain vs split (spread 0 operands, N(0,1))
+        a = rng.standard_normal((n, n))
+        b = rng.standard_normal((n, n))
+        da, db = fg.DeviceArray.from_numpy(a, ctx), fg.DeviceArray.from_numpy(b, ctx)
+        dc = fg.DeviceArray((n, n), np.float64, ctx)
+        rows, cols = oracle.sample_indices(n, n, 48, 48, seed=11)
+        ref = oracle.dd_sampled(a, b, rows, cols)
+        na, nb = oracle.fro(a), oracle.fro(b)
+        d = {}
+        for name, mode in (("plain", L.FG_MODE_PLAIN), ("split_ozaki9", L.FG_MODE_SPLIT)):
+            ms = _time_calls(torch, stream, lambda: lib.fg_gemm_f64(ctx.handle, mode, 0, n, n, n, 1.0, da.ptr,
+                                                                      db.ptr, 0.0, dc.ptr, sh), 3, 1)
+            err = oracle.normwise_error(dc.to_numpy()[np.ix_(rows, cols)], ref, n, n, na, nb)
+            d[name] = {"tflops": round(2.0 * n ** 3 / ms / 1e9, 2), "ms": round(ms, 3), "normwise_err": err}
+        d["split_over_plain"] = round(d["split_ozaki9"]["tflops"] / d["plain"]["tflops"], 2)
+        res["dgemm_f64_%d" % n] = d
+        del da, db, dc
+    if not only or only == "i8":
+        # --- square i8
+        a8 = rng.integers(-128, 128, (n, n), dtype=np.int8)
+        b8 = rng.integers(-128, 128, (n, n), dtype=np.int8)
+        da, db = fg.DeviceArray.from_numpy(a8, ctx), fg.DeviceArray.from_numpy(b8, ctx)
+        dc = fg.DeviceArray((n, n), np.int32, ctx)
+        ms = _time_calls(torch, stream, lambda: lib.fg_gemm_i8_signed(ctx.handle, n, n, n, da.ptr, db.ptr,
+                                                                        dc.ptr, 0, sh), 10, 3)
+        r8, c8 = oracle.sample_indices(n, n, 32, 32, seed=5)
+        got = dc.to_numpy()[np.ix_(r8, c8)]
+        want = (a8[r8].astype(np.int64) @ b8[:, c8].astype(np.int64)).astype(np.int32)
+        res["i8_square_%d" % n] = {"tops": round(2.0 * n ** 3 / ms / 1e9, 1), "ms": round(ms, 4),
+                                   "bit_exact_sampled": bool(np.array_equal(got, want))}
+        del da, db, dc
+    if not only or only == "ragged":
+        # --- ragged grouped batch, 4096 problems, dims log-uniform in [8, 512]
+        dims = np.rint(np.exp(rng.uniform(np.log(8), np.log(512), (4096, 3)))).astype(int)
+        gflop = float(sum(2.0 * m * nn * k for m, nn, k in dims)) / 1e9
+        g = {}
+        for name, dt, mode in (("i8", L.FG_I8, 0), ("f32_split", L.FG_F32, 1), ("f32_plain", L.FG_F32, 0)):
+            es = 1 if dt == L.FG_I8 else 4
+            bufs, tab = [], (L.fg_problem * len(dims))()
+            for i, (m, nn, k) in enumerate(dims):
+                ta = torch.randint(-100, 100, (m * k * es,), dtype=torch.int8, device="cuda")
+                tb = torch.randint(-100, 100, (k * nn * es,), dtype=torch.int8, device="cuda")
+                if es == 4:
+                    ta, tb = torch.randn(m * k, device="cuda"), torch.randn(k * nn, device="cuda")
+                tc = torch.zeros(m * nn * 4, dtype=torch.int8, device="cuda")
+                bufs.append((ta, tb, tc))
+                tab[i] = L.fg_problem(m, nn, k, ta.data_ptr(), tb.data_ptr(), tc.data_ptr(), k, nn, nn)
+            h = C.c_void_p()
+            assert lib.fg_grouped_plan_create(ctx.handle, dt, mode, tab, len(dims), sh, C.byref(h)) == 0
+            ms_g = _time_calls(torch, stream, lambda: lib.fg_grouped_plan_run(h, sh), 10, 3)
+            al, be = (C.c_float * 1)(1.0), (C.c_float * 1)(0.0)
 
-        def loop():
-            for (m, nn, k), (ta, tb, tc) in zip(dims, bufs):
-                lib.fg_gemm(ctx.handle, dt, mode, 0, int(m), int(nn), int(k), al, ta.data_ptr(), int(k),
-                            tb.data_ptr(), int(nn), be, tc.data_ptr(), int(nn), 0, sh)
-        ms_l = _time_calls(torch, stream, loop, 1, 1)
-        lib.fg_grouped_plan_destroy(h)
-        g[name] = {"grouped_ms": round(ms_g, 4), "grouped_tflops": round(gflop / ms_g, 2),
-                   "loop_ms": round(ms_l, 3), "speedup_vs_loop": round(ms_l / ms_g, 1)}
-        del bufs
-    res["ragged_4096"] = {"gflop": round(gflop, 2), **g}
-    torch.cuda.empty_cache()
-    # --- served stream, one rate
-    res["serving_10k_req_s"] = bench_serving.sweep(fg, L, lib, ctx, [10000.0], 1500)[0]
+            def loop():
+                for (m, nn, k), (ta, tb, tc) in zip(dims, bufs):
+                    lib.fg_gemm(ctx.handle, dt, mode, 0, int(m), int(nn), int(k), al, ta.data_ptr(), int(k),
+                                tb.data_ptr(), int(nn), be, tc.data_ptr(), int(nn), 0, sh)
+            ms_l = _time_calls(torch, stream, loop, 1, 1)
+            lib.fg_grouped_plan_destroy(h)
+            g[name] = {"grouped_ms": round(ms_g, 4), "grouped_tflops": round(gflop / ms_g, 2),
+                       "loop_ms": round(ms_l, 3), "speedup_vs_loop": round(ms_l / ms_g, 1)}
+            del bufs
+        res["ragged_4096"] = {"gflop": round(gflop, 2), **g}
+        torch.cuda.empty_cache()
+    if not only or only == "serving":
+        # --- served stream, one rate
+        res["serving_10k_req_s"] = bench_serving.sweep(fg, L, lib, ctx, [10000.0], 1500)[0]
     return res
 
 
@@ -285,6 +326,18 @@ def cpu_baseline(n):
 
 def main():
     args = parse()
+    if args.peaks:
+        print(json.dumps(reference_peaks(args.n)), flush=True)
+        return
+    if args.side:
+        import torch
+        import ferray_b200 as fg
+        from ferray_b200 import _lib as L
+        ctx = fg.Context(0)
+        stream = torch.cuda.Stream()
+        print(json.dumps(side_measurements(fg, L, ctx._lib, ctx, stream, args.n, args.side)),
+              flush=True)
+        return
     if args.serving:
         import bench_serving
         import ferray_b200 as fg
