@@ -30,7 +30,7 @@ __all__ = [
     "default_context", "gemm_f64", "gemm_f32", "gemm_c64", "gemm_c32", "gemm_i8",
     "gemm_i8_signed", "gemm_i16", "quantized_matmul", "matmul", "matmul_complex",
     "gemm_batched_strided", "gemm_grouped", "GroupedPlan", "Server", "launch_count", "PLAIN",
-    "SPLIT",
+    "SPLIT", "TUNE_OPS", "tune_lookup", "tune_forced",
 ]
 
 PLAIN, SPLIT = "plain", "split"
@@ -383,6 +383,32 @@ def _table(problems):
         tab[i] = L.fg_problem(m, n, k, a.ptr if _is_dev(a) else a, b.ptr if _is_dev(b) else b,
                               c.ptr if _is_dev(c) else c, k, n, n)
     return tab
+
+
+TUNE_OPS = {"i8": 0, "split_f32": 1, "f64": 2, "f32": 3}
+
+
+def tune_lookup(op, m, n, k):
+    """(variant, splits) the autotuned table picks for a problem size."""
+    v, s = C.c_int(), C.c_int()
+    check(L.load().fg_tune_lookup(TUNE_OPS[op], m, n, k, C.byref(v), C.byref(s)), "tune_lookup")
+    return v.value, s.value
+
+
+class tune_forced:
+    """Context manager forcing (variant, splits) for one family, process-wide
+    (the autotuner's and the tests' way to reach every variant)."""
+
+    def __init__(self, op, variant, splits=1):
+        self.op, self.variant, self.splits = TUNE_OPS[op], variant, splits
+
+    def __enter__(self):
+        check(L.load().fg_tune_force(self.op, self.variant, self.splits), "tune_force")
+        return self
+
+    def __exit__(self, *exc):
+        L.load().fg_tune_force(self.op, -1, 1)
+        return False
 
 
 def gemm_grouped(problems, dtype=np.float32, mode=PLAIN):

@@ -65,6 +65,10 @@ SIGNATURES = {
     "fg_profile_enable": (_i, [_i]),
     "fg_profile_collect": (_i, [C.POINTER(fg_profile_entry), _i, C.POINTER(_i)]),
     "fg_device_info": (_i, [_p, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(_sz)]),
+    "fg_selftest_wait_timeout": (_i, [_p, C.c_uint32, _p]),
+    "fg_tune_lookup": (_i, [_i, _sz, _sz, _sz, C.POINTER(_i), C.POINTER(_i)]),
+    "fg_tune_force": (_i, [_i, _i, _i]),
+    "fg_tune_variants": (_i, [_i, C.POINTER(_i)]),
     "fg_buffer_alloc": (_i, [_p, _sz, C.POINTER(_p)]),
     "fg_buffer_free": (_i, [_p, _p]),
     "fg_upload": (_i, [_p, _p, _p, _sz, _p]),

@@ -26,7 +26,7 @@ def sources():
 
 
 def headers():
-    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h", ".inc"))]
     return hs + [os.path.join(ROOT, "include", "ferray_gpu.h")]
 
 

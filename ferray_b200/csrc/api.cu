@@ -82,6 +82,23 @@ static int grid_for(long long total) {
 }
 
 // K == 0: C = beta*C (floats) or C = 0 / unchanged (integers), per batch.
+// One thread waits, with the kernels' bounded wait, on an mbarrier that
+// nothing ever arrives on: the wait gives up after timeout_ns, records
+// FG_DEV_ERR_TIMEOUT at site 0x7F in the context's status word and the
+// kernel returns normally (no fault, the context stays usable).
+static __global__ void wait_probe_kernel(fg::DevStatus* st, uint64_t timeout_ns) {
+    __shared__ uint64_t bar;
+    __shared__ int abort_flag;
+    if (threadIdx.x == 0) {
+        fg::mbar_init(&bar, 1);
+        abort_flag = 0;
+        fg::fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) fg::mbar_wait(&bar, 0, timeout_ns, st, 0x7F, &abort_flag);
+    __syncthreads();
+}
+
 static fg_status k_zero(const Gemm& g, cudaStream_t st) {
     for (int i = 0; i < g.batch; ++i) {
         switch (g.dtype) {
@@ -286,6 +303,17 @@ fg_status fg_sync(fg_ctx* ctx, fg_stream stream) {
                          "kernel reported error " + std::to_string(h.code) + " at site " +
                              std::to_string(h.where) + " (block " + std::to_string(h.block) + ")");
     }
+    return FG_OK;
+}
+
+fg_status fg_selftest_wait_timeout(fg_ctx* ctx, uint32_t timeout_us, fg_stream stream) {
+    if (!ctx) return set_error(FG_ERR_INVALID, "null context");
+    if (timeout_us == 0 || timeout_us > 1000000)
+        return set_error(FG_ERR_INVALID, "fg_selftest_wait_timeout: timeout outside 1 us .. 1 s");
+    FG_CUDA(cudaSetDevice(ctx->device));
+    wait_probe_kernel<<<1, 32, 0, stream_of(ctx, stream)>>>(ctx->d_status, 1000ull * timeout_us);
+    count_launch();
+    FG_CUDA(cudaGetLastError());
     return FG_OK;
 }
 

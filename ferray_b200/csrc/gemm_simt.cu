@@ -3,6 +3,9 @@
 #include "prep_kernels.cuh"
 #include "runtime.h"
 #include "simt_gemm.cuh"
+#include "tune.h"
+
+#include <algorithm>
 
 namespace fgrt {
 
@@ -20,6 +23,49 @@ static BatchMap batch_map(const Gemm& g) {
     return bm;
 }
 
+static int grid_for(long long total) {
+    return static_cast<int>(std::min<long long>(std::max<long long>((total + 255) / 256, 1), 4096));
+}
+
+// Plain real GEMM with the tuned tile variant and split-K count.  Split-K
+// writes `splits` partial products into a workspace and a combine pass
+// applies alpha / beta (the partial sums are added in split order).
+template <typename T, int TM>
+static fg_status launch_simt_real(const Gemm& g, BatchMap bm, int splits_want, cudaStream_t st) {
+    constexpr int BT = 16 * TM;
+    constexpr long long KUNIT = 64;  // split granularity in K
+    const long long kunits = (g.K + KUNIT - 1) / KUNIT;
+    int kps = static_cast<int>(kunits);
+    const int splits = plan_splits(splits_want, static_cast<int>(kunits), g.M * g.N * g.batch,
+                                   sizeof(T), &kps);
+    if ((long long)splits * g.batch > 65535) return set_error(FG_ERR_UNSUPPORTED, "batch above 65535");
+    dim3 grid((g.N + BT - 1) / BT, (g.M + BT - 1) / BT, g.batch * splits);
+    const T* A = static_cast<const T*>(g.A);
+    const T* B = static_cast<const T*>(g.B);
+    if (splits <= 1) {
+        simt_gemm_real<T, 8, TM><<<grid, 256, 0, st>>>((int)g.M, (int)g.N, (int)g.K, (T)g.alpha_re, A,
+                                                       g.lda, B, g.ldb, (T)g.beta_re,
+                                                       static_cast<T*>(g.C), g.ldc, bm, g.batch, (int)g.K);
+        count_launch();
+        FG_CUDA(cudaGetLastError());
+        return FG_OK;
+    }
+    Scratch ws;
+    const long long out_elems = g.M * g.N * g.batch;
+    FG_TRY(ws.alloc(static_cast<size_t>(splits * out_elems) * sizeof(T), st));
+    BatchMap wbm = bm;
+    wbm.c_bstride = g.M * g.N;
+    simt_gemm_real<T, 8, TM><<<grid, 256, 0, st>>>((int)g.M, (int)g.N, (int)g.K, T(1), A, g.lda, B,
+                                                   g.ldb, T(0), static_cast<T*>(ws.p), g.N, wbm,
+                                                   g.batch, (int)(kps * KUNIT));
+    splitk_reduce_kernel<T><<<grid_for(out_elems), 256, 0, st>>>(
+        static_cast<const T*>(ws.p), splits, g.M, g.N, g.batch, static_cast<T*>(g.C), g.ldc,
+        g.c_stride, (T)g.alpha_re, (T)g.beta_re, 0);
+    count_launch(2);
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
 fg_status launch_simt(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
     (void)ctx;
     const BatchMap bm = batch_map(g);
@@ -28,18 +74,14 @@ fg_status launch_simt(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
     ProfScope prof(g.dtype <= FG_C32 ? names[g.dtype] : "simt", st);
     switch (g.dtype) {
         case FG_F64: {
-            dim3 grid((g.N + 127) / 128, (g.M + 127) / 128, g.batch);
-            simt_gemm_real<double, 8><<<grid, 256, 0, st>>>(
-                (int)g.M, (int)g.N, (int)g.K, g.alpha_re, static_cast<const double*>(g.A), g.lda,
-                static_cast<const double*>(g.B), g.ldb, g.beta_re, static_cast<double*>(g.C), g.ldc, bm);
-            break;
+            const TuneChoice c = tune_lookup(TUNE_F64, g.M, g.N, g.K);
+            return c.variant == 1 ? launch_simt_real<double, 4>(g, bm, c.splits, st)
+                                  : launch_simt_real<double, 8>(g, bm, c.splits, st);
         }
         case FG_F32: {
-            dim3 grid((g.N + 127) / 128, (g.M + 127) / 128, g.batch);
-            simt_gemm_real<float, 8><<<grid, 256, 0, st>>>(
-                (int)g.M, (int)g.N, (int)g.K, (float)g.alpha_re, static_cast<const float*>(g.A), g.lda,
-                static_cast<const float*>(g.B), g.ldb, (float)g.beta_re, static_cast<float*>(g.C), g.ldc, bm);
-            break;
+            const TuneChoice c = tune_lookup(TUNE_F32, g.M, g.N, g.K);
+            return c.variant == 1 ? launch_simt_real<float, 4>(g, bm, c.splits, st)
+                                  : launch_simt_real<float, 8>(g, bm, c.splits, st);
         }
         case FG_C64: {
             dim3 grid((g.N + 63) / 64, (g.M + 63) / 64, g.batch);

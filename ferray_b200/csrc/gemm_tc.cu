@@ -13,18 +13,23 @@
 #include "prep_kernels.cuh"
 #include "runtime.h"
 #include "tc_gemm.cuh"
+#include "tune.h"
 
 namespace fgrt {
 
 using namespace fg;
 
+// i8 variants (tuned): 128 x 256 tiles, 4 stages; 128 x 128 tiles,
+// 6 stages, for problems with few output tiles.
 using CfgI8 = TcCfg<KIND_I8, 256, 4, 1, 1, 1, 1, EPI_I32>;
+using CfgI8n128 = TcCfg<KIND_I8, 128, 6, 1, 1, 1, 1, EPI_I32>;
 using CfgQmm = TcCfg<KIND_I8, 256, 4, 1, 1, 1, 1, EPI_QMM>;
 using CfgI16 = TcCfg<KIND_I8, 128, 3, 2, 2, 3, 4, EPI_I16>;
 // 3 products: one accumulator (the 2-slice representation error, about
 // 2^-18 |a||b| per product, dominates whatever the accumulation does).
 // 6 products: accumulator 0 holds hi*hi, accumulator 1 the corrections.
 using CfgBf16x3 = TcCfg<KIND_BF16, 128, 3, 2, 2, 1, 3, EPI_F32, 1>;
+using CfgBf16x3n64 = TcCfg<KIND_BF16, 64, 4, 2, 2, 1, 3, EPI_F32, 1>;
 using CfgBf16x6 = TcCfg<KIND_BF16, 128, 2, 3, 3, 2, 6, EPI_F32, 1>;
 
 // K blocks (64 bf16 each) per TMEM accumulation chunk of the split SGEMM.
@@ -46,6 +51,10 @@ static const char* cfg_name() {
     return "tc_gemm_i8";
 }
 
+static int grid_for_total(long long total) {
+    return static_cast<int>(std::min<long long>(std::max<long long>((total + 255) / 256, 1), 4096));
+}
+
 template <class Cfg>
 static fg_status launch_cfg(fg_ctx* ctx, const TcMaps& maps, TcArgs& args, cudaStream_t st) {
     static std::once_flag once;
@@ -57,12 +66,44 @@ static fg_status launch_cfg(fg_ctx* ctx, const TcMaps& maps, TcArgs& args, cudaS
     FG_CUDA(attr_err);
     args.status = ctx->d_status;
     args.timeout_ns = kTimeoutNs;
-    const long long tiles = (long long)args.batch * args.tiles_m * args.tiles_n;
+    const long long tiles =
+        (long long)std::max(args.splits, 1) * args.batch * args.tiles_m * args.tiles_n;
     if (tiles == 0) return FG_OK;
     const int grid = static_cast<int>(std::min<long long>(tiles, ctx->sm_count));
     ProfScope prof(cfg_name<Cfg>(), st);
     tc_gemm_kernel<Cfg><<<grid, Cfg::THREADS, tc_smem_bytes<Cfg>(), st>>>(maps, args);
     prof.stop();
+    count_launch();
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+// Launches Cfg with up to `want` K splits (tuned).  With more than one
+// split the kernel writes dense partial products [split][batch][M][N] into a
+// workspace and splitk_reduce_kernel combines them into C (wrapping int32
+// sum + accumulate, or alpha * sum + beta * C).
+template <class Cfg, typename T>
+static fg_status launch_splitk(fg_ctx* ctx, const TcMaps& maps, TcArgs& args, int want, T* C,
+                               long long ldc, long long strideC, T alpha, T beta, int accumulate,
+                               cudaStream_t st) {
+    const long long M = args.M, N = args.N, out_elems = M * N * args.batch;
+    int kps = args.k_blocks;
+    const int splits = plan_splits(want, args.k_blocks, out_elems, sizeof(T), &kps);
+    if (splits <= 1) return launch_cfg<Cfg>(ctx, maps, args, st);
+    Scratch ws;
+    FG_TRY(ws.alloc(static_cast<size_t>(splits * out_elems) * sizeof(T), st));
+    args.splits = splits;
+    args.kb_per_split = kps;
+    args.C = ws.p;
+    args.ldc = N;
+    args.strideC = M * N;
+    args.accumulate = 0;
+    args.alpha = 1.f;
+    args.beta = 0.f;
+    FG_TRY(launch_cfg<Cfg>(ctx, maps, args, st));
+    splitk_reduce_kernel<T><<<grid_for_total(out_elems), 256, 0, st>>>(
+        static_cast<const T*>(ws.p), splits, M, N, args.batch, C, ldc, strideC, alpha, beta,
+        accumulate);
     count_launch();
     FG_CUDA(cudaGetLastError());
     return FG_OK;
@@ -178,10 +219,18 @@ fg_status launch_int_tc(fg_ctx* ctx, const Gemm& g0, cudaStream_t st) {
                            128, 128, &args.a_rank3));
         FG_TRY(operand_map(&maps.b[0], CU_TENSOR_MAP_DATA_TYPE_UINT8, pb, g.N, g.K, ldb, g.b_count, msb,
                            128, 128, &args.b_rank3));
-        args.tiles_n = static_cast<int>((g.N + CfgI8::BN - 1) / CfgI8::BN);
         args.k_blocks = static_cast<int>((g.K + CfgI8::BK - 1) / CfgI8::BK);
         args.ops[0] = TcOp{0, 0, 0, g.dtype == FG_I8 ? 1 : 0, 1};
-        return launch_cfg<CfgI8>(ctx, maps, args, st);
+        const TuneChoice c = tune_lookup(TUNE_I8, g.M, g.N, g.K);
+        int32_t* C = static_cast<int32_t*>(g.C);
+        if (c.variant == 1) {
+            args.tiles_n = static_cast<int>((g.N + CfgI8n128::BN - 1) / CfgI8n128::BN);
+            return launch_splitk<CfgI8n128, int32_t>(ctx, maps, args, c.splits, C, g.ldc, g.c_stride,
+                                                     0, 0, g.accumulate, st);
+        }
+        args.tiles_n = static_cast<int>((g.N + CfgI8::BN - 1) / CfgI8::BN);
+        return launch_splitk<CfgI8, int32_t>(ctx, maps, args, c.splits, C, g.ldc, g.c_stride, 0, 0,
+                                             g.accumulate, st);
     }
     if (g.dtype == FG_I16) {
         // Byte slices, rows padded to 16 bytes.
@@ -361,7 +410,18 @@ fg_status launch_split_bf16(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
     args.ops[0] = TcOp{1, 0, 0, 1, 1};  // lo * hi
     args.ops[1] = TcOp{0, 1, 0, 1, 1};  // hi * lo
     args.ops[2] = TcOp{0, 0, 0, 1, 1};  // hi * hi
-    return launch_cfg<CfgBf16x3>(ctx, maps, args, st);
+    // Tuned tile variant / split-K (real products only; the complex
+    // embedding's interleaving epilogue runs unsplit with 128-wide tiles).
+    const TuneChoice c = cplx ? TuneChoice{0, 1} : tune_lookup(TUNE_SPLIT_F32, M, N, K);
+    float* C = static_cast<float*>(g.C);
+    const float alpha = args.alpha, beta = args.beta;
+    if (c.variant == 1) {
+        args.tiles_n = static_cast<int>((N + CfgBf16x3n64::BN - 1) / CfgBf16x3n64::BN);
+        return launch_splitk<CfgBf16x3n64, float>(ctx, maps, args, c.splits, C, g.ldc, g.c_stride,
+                                                  alpha, beta, 0, st);
+    }
+    return launch_splitk<CfgBf16x3, float>(ctx, maps, args, c.splits, C, g.ldc, g.c_stride, alpha,
+                                           beta, 0, st);
 }
 
 }  // namespace fgrt

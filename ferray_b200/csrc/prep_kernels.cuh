@@ -17,6 +17,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <type_traits>
 
 namespace fg {
 
@@ -171,6 +172,35 @@ static __global__ void scale_kernel(T* __restrict__ C, long long rows, long long
          e += (long long)gridDim.x * blockDim.x) {
         long long r = e / cols, c = e - r * cols;
         C[r * ldc + c] = beta == T(0) ? T(0) : beta * C[r * ldc + c];
+    }
+}
+
+// Split-K combine: ws holds `splits` partial products [s][z][M][N] (dense,
+// s-major); C[z] = alpha * (ws[0] + ... + ws[S-1]) + beta * C[z] for floats
+// (partials added in split order, round to nearest; beta == 0 leaves C
+// unread), and C[z] = sum (+ C[z] when accumulate) mod 2^32 for int32.
+template <typename T>
+static __global__ void splitk_reduce_kernel(const T* __restrict__ ws, int splits, long long M,
+                                            long long N, int batch, T* __restrict__ C,
+                                            long long ldc, long long strideC, T alpha, T beta,
+                                            int accumulate) {
+    const long long mn = M * N, total = mn * batch, sstride = total;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long z = e / mn, rem = e - z * mn, r = rem / N, c = rem - r * N;
+        T* dst = C + z * strideC + r * ldc + c;
+        if constexpr (std::is_integral<T>::value) {  // int32
+            uint32_t s = 0;
+            for (int q = 0; q < splits; ++q) s += static_cast<uint32_t>(ws[q * sstride + e]);
+            if (accumulate) s += static_cast<uint32_t>(*dst);
+            *dst = static_cast<T>(s);
+        } else {
+            T s = ws[e];
+            for (int q = 1; q < splits; ++q) s = s + ws[q * sstride + e];
+            T o = alpha * s;
+            if (beta != T(0)) o = fma(beta, *dst, o);
+            *dst = o;
+        }
     }
 }
 

@@ -40,28 +40,29 @@ __device__ __forceinline__ void batch_offsets(const BatchMap& bm, int bz, long l
 }
 
 // ----------------------------------------------------------------- real
-template <typename T, int BK>
-struct SimtReal {
-    static constexpr int BM = 128, BN = 128, TM = 8, TN = 8, THREADS = 256;
-    static constexpr int PAD = 4;
-};
-
-template <typename T, int BK>
+// Tile BM = BN = 16 * TM (TM = 8: 128 x 128, TM = 4: 64 x 64 for small
+// problems).  Split-K: blockIdx.z = split * nbatch + batch index; split s
+// covers K columns [s * ksplit, (s + 1) * ksplit) and writes output matrix
+// blockIdx.z (the host points C at a partial-sum workspace then).
+template <typename T, int BK, int TM>
 __global__ void __launch_bounds__(256)
     simt_gemm_real(int M, int N, int K, T alpha, const T* __restrict__ A, long long lda,
                    const T* __restrict__ B, long long ldb, T beta, T* __restrict__ C,
-                   long long ldc, BatchMap bm) {
-    constexpr int BM = 128, BN = 128, PAD = 4;
+                   long long ldc, BatchMap bm, int nbatch, int ksplit) {
+    constexpr int BM = 16 * TM, BN = 16 * TM, PAD = 4, H = TM / 2;
     constexpr int A_PER = BM * BK / 256;  // A elements each thread loads per K block
     constexpr int B_PER = BK * BN / 256;
     __shared__ __align__(16) T As[2][BK][BM + PAD];
     __shared__ __align__(16) T Bs[2][BK][BN + PAD];
 
+    const int zb = blockIdx.z % nbatch, zs = blockIdx.z / nbatch;
     long long oa, ob;
-    batch_offsets(bm, blockIdx.z, oa, ob);
-    A += oa;
-    B += ob;
+    batch_offsets(bm, zb, oa, ob);
+    const int k_begin = zs * ksplit;
+    A += oa + k_begin;
+    B += ob + (long long)k_begin * ldb;
     C += blockIdx.z * bm.c_bstride;
+    K = min(K - k_begin, ksplit);
 
     const int tid = threadIdx.x;
     const int tx = tid % 16, ty = tid / 16;
@@ -96,11 +97,11 @@ __global__ void __launch_bounds__(256)
         for (int j = 0; j < B_PER; ++j) Bs[buf][b_r][b_c + j] = rb[j];
     };
 
-    T acc[8][8];
+    T acc[TM][TM];
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
+    for (int i = 0; i < TM; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = T(0);
+        for (int j = 0; j < TM; ++j) acc[i][j] = T(0);
 
     const int kblocks = (K + BK - 1) / BK;
     load_global(0);
@@ -111,30 +112,30 @@ __global__ void __launch_bounds__(256)
         if (kb + 1 < kblocks) load_global((kb + 1) * BK);
 #pragma unroll
         for (int kk = 0; kk < BK; ++kk) {
-            T af[8], bf[8];
+            T af[TM], bf[TM];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                af[i] = As[cur][kk][ty * 4 + i];
-                af[4 + i] = As[cur][kk][64 + ty * 4 + i];
-                bf[i] = Bs[cur][kk][tx * 4 + i];
-                bf[4 + i] = Bs[cur][kk][64 + tx * 4 + i];
+            for (int i = 0; i < H; ++i) {
+                af[i] = As[cur][kk][ty * H + i];
+                af[H + i] = As[cur][kk][BM / 2 + ty * H + i];
+                bf[i] = Bs[cur][kk][tx * H + i];
+                bf[H + i] = Bs[cur][kk][BN / 2 + tx * H + i];
             }
 #pragma unroll
-            for (int i = 0; i < 8; ++i)
+            for (int i = 0; i < TM; ++i)
 #pragma unroll
-                for (int j = 0; j < 8; ++j) acc[i][j] = fma(af[i], bf[j], acc[i][j]);
+                for (int j = 0; j < TM; ++j) acc[i][j] = fma(af[i], bf[j], acc[i][j]);
         }
         if (kb + 1 < kblocks) store_shared(cur ^ 1);
         __syncthreads();
     }
 
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const int r = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
+    for (int i = 0; i < TM; ++i) {
+        const int r = m0 + (i < H ? ty * H + i : BM / 2 + ty * H + (i - H));
         if (r >= M) continue;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int c = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + (j - 4));
+        for (int j = 0; j < TM; ++j) {
+            const int c = n0 + (j < H ? tx * H + j : BN / 2 + tx * H + (j - H));
             if (c >= N) continue;
             T* p = C + (long long)r * ldc + c;
             T v = alpha * acc[i][j];

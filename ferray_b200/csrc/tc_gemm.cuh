@@ -100,6 +100,10 @@ struct TcArgs {
     int a_zp, b_zp;
     float scale;
     int kchunk;                // CHUNKED configs: K blocks per TMEM chunk
+    // split-K: work unit t covers K blocks [s*kb_per_split, (s+1)*kb_per_split)
+    // of one tile, s = t / (batch*tiles); its partial result goes to output
+    // matrix s*batch + bz.  splits <= 1: no split (zero-initialised args).
+    int splits, kb_per_split;
     // EPI_OZAKI: C (f64) (+)= oz_w * 2^(e_i + f_j) * acc; the first group of a
     // call applies C = oz_beta * C first.  cplx_half > 0 interleaves complex.
     const double* row_scale;
@@ -125,6 +129,24 @@ __device__ __forceinline__ void tile_coords(const TcArgs& p, int t, int& bz, int
     int q = r - g * per_group;
     tm = first_m + q % gm;
     tn = q / gm;
+}
+
+// Work unit t -> output matrix index, batch index, tile and K-block range.
+__device__ __forceinline__ void unit_coords(const TcArgs& p, int t, int& zo, int& bz, int& tm,
+                                            int& tn, int& kb0, int& kb1) {
+    if (p.splits > 1) {
+        const int per_split = p.batch * p.tiles_m * p.tiles_n;
+        const int s = t / per_split;
+        tile_coords(p, t - s * per_split, bz, tm, tn);
+        zo = s * p.batch + bz;
+        kb0 = s * p.kb_per_split;
+        kb1 = min(p.k_blocks, kb0 + p.kb_per_split);
+    } else {
+        tile_coords(p, t, bz, tm, tn);
+        zo = bz;
+        kb0 = 0;
+        kb1 = p.k_blocks;
+    }
 }
 
 __device__ __forceinline__ void batch_operands(const TcArgs& p, int bz, int& za, int& zb) {
@@ -275,7 +297,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
 
     const int warp = threadIdx.x / 32;
     const int lane = threadIdx.x % 32;
-    const int total_tiles = p.batch * p.tiles_m * p.tiles_n;
+    const int total_tiles = max(p.splits, 1) * p.batch * p.tiles_m * p.tiles_n;
     volatile int* abort = &s.abort;
 
     if (threadIdx.x == 0) {
@@ -313,10 +335,10 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
             for (int i = 0; i < Cfg::STAGES; ++i) issued_parity[i] = -1;
             bool ok = true;
             for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x) {
-                int bz, tm, tn, za, zb;
-                tile_coords(p, t, bz, tm, tn);
+                int zo, bz, tm, tn, za, zb, kb0, kb1;
+                unit_coords(p, t, zo, bz, tm, tn, kb0, kb1);
                 batch_operands(p, bz, za, zb);
-                for (int kb = 0; kb < p.k_blocks; ++kb) {
+                for (int kb = kb0; kb < kb1; ++kb) {
                     if (!mbar_wait(&s.empty[stage], phase ^ 1u, p.timeout_ns, p.status, 0x01,
                                    abort)) {
                         ok = false;
@@ -365,10 +387,12 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
             uint32_t phase = 0;
             int it = 0;  // accumulator units (tile x K chunk) issued so far
             bool ok = true;
-            const int kchunk = (Cfg::CHUNKED && p.kchunk > 0) ? p.kchunk : p.k_blocks;
             for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x) {
-                for (int kc0 = 0; kc0 < p.k_blocks && ok; kc0 += kchunk, ++it) {
-                    const int kc1 = min(p.k_blocks, kc0 + kchunk);
+                int zo, bz, tm, tn, kb0, kb1;
+                unit_coords(p, t, zo, bz, tm, tn, kb0, kb1);
+                const int kchunk = (Cfg::CHUNKED && p.kchunk > 0) ? p.kchunk : kb1 - kb0;
+                for (int kc0 = kb0; kc0 < kb1 && ok; kc0 += kchunk, ++it) {
+                    const int kc1 = min(kb1, kc0 + kchunk);
                     const int buf = it % Cfg::ACC_BUFS;
                     const uint32_t acc_par = static_cast<uint32_t>((it / Cfg::ACC_BUFS) & 1);
                     if (!mbar_wait(&s.acc_empty[buf], acc_par ^ 1u, p.timeout_ns, p.status, 0x11, abort)) {
@@ -431,13 +455,15 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
             // runs drift.  Each K chunk is accumulated in TMEM from zero and
             // the chunk sums are added here in FP32 registers with
             // round-to-nearest.
-            const int kchunk = p.kchunk > 0 ? p.kchunk : p.k_blocks;
             bool ok = true;
             for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x) {
+                int zo, bz, tm, tn, kb0, kb1;
+                unit_coords(p, t, zo, bz, tm, tn, kb0, kb1);
+                const int kchunk = p.kchunk > 0 ? p.kchunk : kb1 - kb0;
                 float run[Cfg::BN];
 #pragma unroll
                 for (int j = 0; j < Cfg::BN; ++j) run[j] = 0.f;
-                for (int kc0 = 0; kc0 < p.k_blocks; kc0 += kchunk, ++it) {
+                for (int kc0 = kb0; kc0 < kb1; kc0 += kchunk, ++it) {
                     const int buf = it % Cfg::ACC_BUFS;
                     const uint32_t acc_par = static_cast<uint32_t>((it / Cfg::ACC_BUFS) & 1);
                     if (!mbar_wait(&s.acc_full[buf], acc_par, p.timeout_ns, p.status, 0x21, abort)) {
@@ -466,15 +492,13 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
                     if (lane == 0) mbar_arrive(&s.acc_empty[buf]);
                 }
                 if (!ok) break;
-                int bz, tm, tn;
-                tile_coords(p, t, bz, tm, tn);
                 const int grow = tm * Cfg::BM + ew * 32 + lane;
 #pragma unroll
                 for (int c = 0; c < Cfg::BN / 32; ++c) {
                     uint32_t v[Cfg::NACC][32];
 #pragma unroll
                     for (int j = 0; j < 32; ++j) v[0][j] = __float_as_uint(run[c * 32 + j]);
-                    epilogue_store<Cfg>(p, bz, grow, tn * Cfg::BN + c * 32, v);
+                    epilogue_store<Cfg>(p, zo, grow, tn * Cfg::BN + c * 32, v);
                 }
             }
         } else {
@@ -483,8 +507,8 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
                 const uint32_t acc_par = static_cast<uint32_t>((it / Cfg::ACC_BUFS) & 1);
                 if (!mbar_wait(&s.acc_full[buf], acc_par, p.timeout_ns, p.status, 0x21, abort)) break;
                 tc_fence_after();
-                int bz, tm, tn;
-                tile_coords(p, t, bz, tm, tn);
+                int zo, bz, tm, tn, kb0, kb1;
+                unit_coords(p, t, zo, bz, tm, tn, kb0, kb1);
                 const int grow = tm * Cfg::BM + ew * 32 + lane;
                 const uint32_t row_addr = tmem + (static_cast<uint32_t>(ew * 32) << 16) + buf * Cfg::ACC_COLS;
 #pragma unroll 1
@@ -493,7 +517,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
 #pragma unroll
                     for (int a = 0; a < Cfg::NACC; ++a) tmem_ld_32x32b_x32(row_addr + a * Cfg::BN + c * 32, v[a]);
                     tmem_wait_ld();
-                    epilogue_store<Cfg>(p, bz, grow, tn * Cfg::BN + c * 32, v);
+                    epilogue_store<Cfg>(p, zo, grow, tn * Cfg::BN + c * 32, v);
                 }
                 tc_fence_before();
                 __syncwarp();

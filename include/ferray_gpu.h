@@ -103,6 +103,32 @@ fg_status fg_profile_collect(fg_profile_entry *out, int capacity, int *count);
 fg_status fg_device_info(fg_ctx *ctx, int *sm_count, int *cc_major, int *cc_minor,
                          size_t *hbm_bytes);
 
+/* Failure-detection self test: launches one kernel whose bounded device
+ * wait nothing satisfies; it gives up after `timeout_us` (1 us .. 1 s), so
+ * the next fg_sync returns FG_ERR_TIMEOUT and the context stays usable.
+ * The same bounded wait guards every pipeline barrier of the GEMM kernels. */
+fg_status fg_selftest_wait_timeout(fg_ctx *ctx, uint32_t timeout_us, fg_stream stream);
+
+/* ------------------------------------------------------------ autotune */
+/* Tile variant and split-K count per GEMM family come from a table indexed
+ * by the size buckets of m, n, k (<=128, <=256, ..., <=4096, >4096), written
+ * by ferray_b200/autotune.py from timings on a B200 and compiled in.  The
+ * reference's blocking is fixed constants (MC 64, KC 256, NC 512,
+ * gemm/outer.rs:66-68); this table is what replaces them. */
+typedef enum fg_tune_op {
+    FG_TUNE_I8 = 0,        /* i8 x i8 / u8 x i8 -> i32 (tensor cores)       */
+    FG_TUNE_SPLIT_F32 = 1, /* 3xBF16 split SGEMM (tensor cores)             */
+    FG_TUNE_F64 = 2,       /* plain DGEMM (FP64 pipe)                       */
+    FG_TUNE_F32 = 3        /* plain SGEMM (FFMA)                            */
+} fg_tune_op;
+/* The (variant, splits) the dispatch uses for a problem of this size. */
+fg_status fg_tune_lookup(int op, size_t m, size_t n, size_t k, int *variant, int *splits);
+/* Forces (variant, splits) for every later call of `op`, process-wide;
+ * variant < 0 returns to the table.  For the tuner, not for serving. */
+fg_status fg_tune_force(int op, int variant, int splits);
+/* Number of kernel variants of `op`. */
+fg_status fg_tune_variants(int op, int *count);
+
 /* ------------------------------------------------------------ buffers */
 /* Device-resident buffers: the device counterpart of ferray-core's
  * Array storage (ferray-core/src/array/owned.rs:21, buffer.rs:25-49). */

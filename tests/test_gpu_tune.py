@@ -1,0 +1,125 @@
+"""Every autotuned kernel variant and split-K count, forced, against the
+oracle: integers bit-exact, floats within the normwise bounds of the plain
+and split paths (test_gpu_parity.py states them), including alpha / beta,
+accumulate and broadcast batches, so any table the tuner writes is correct
+by construction."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+U64, U32 = 2.0 ** -53, 2.0 ** -24
+SPLITS = [1, 2, 3, 16]
+SHAPES = [(1, 1, 1), (70, 33, 300), (128, 128, 1024), (130, 200, 2100)]
+_DD = {}
+
+
+def dd(oracle, a, b, key):
+    """double-double A@B, computed once per input set"""
+    if key not in _DD:
+        _DD[key] = oracle.dd_full(a, b)
+    return _DD[key]
+
+
+def rng(seed=0):
+    return np.random.default_rng(seed)
+
+
+@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("splits", SPLITS)
+@pytest.mark.parametrize("m,n,k", SHAPES)
+def test_i8_variants_bit_exact(fg, oracle, variant, splits, m, n, k):
+    r = rng(m + n + k)
+    a = r.integers(-128, 128, (m, k), dtype=np.int8)
+    b = r.integers(-128, 128, (k, n), dtype=np.int8)
+    c0 = r.integers(-2 ** 31, 2 ** 31, (m, n), dtype=np.int64).astype(np.int32)
+    with fg.tune_forced("i8", variant, splits):
+        c = np.zeros((m, n), np.int32)
+        assert fg.gemm_i8_signed(m, n, k, a, b, c)
+        np.testing.assert_array_equal(c, oracle.gemm_i8_signed(a, b))
+        c = c0.copy()
+        assert fg.gemm_i8_signed(m, n, k, a, b, c, accumulate=True)
+        np.testing.assert_array_equal(c, oracle.gemm_i8_signed(a, b, c=c0, accumulate=True))
+        au = r.integers(0, 256, (m, k), dtype=np.uint8)
+        c = np.zeros((m, n), np.int32)
+        assert fg.gemm_i8(m, n, k, au, b, c)
+        np.testing.assert_array_equal(c, oracle.gemm_i8(au, b, variant="vnni"))
+
+
+@pytest.mark.parametrize("variant,splits", [(0, 4), (1, 3)])
+def test_i8_split_broadcast_batch(fg, oracle, variant, splits):
+    r = rng(9)
+    a = r.integers(-128, 128, (3, 1, 40, 520), dtype=np.int8)
+    b = r.integers(-128, 128, (2, 520, 72), dtype=np.int8)
+    want = np.einsum("...ik,...kj->...ij", a.astype(np.int64), b.astype(np.int64))
+    want = ((want + 2 ** 31) % 2 ** 32 - 2 ** 31).astype(np.int32)
+    with fg.tune_forced("i8", variant, splits):
+        got = fg.matmul(fg.DeviceArray.from_numpy(a), fg.DeviceArray.from_numpy(b)).to_numpy()
+    np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("splits", SPLITS)
+@pytest.mark.parametrize("m,n,k", SHAPES)
+def test_split_f32_variants(fg, oracle, variant, splits, m, n, k):
+    r = rng(m * 3 + k)
+    a = r.standard_normal((m, k), dtype=np.float32)
+    b = r.standard_normal((k, n), dtype=np.float32)
+    c0 = r.standard_normal((m, n), dtype=np.float32)
+    with fg.tune_forced("split_f32", variant, splits):
+        c = np.zeros((m, n), np.float32)
+        assert fg.gemm_f32(m, n, k, 1.0, a, b, 0.0, c, mode="split")
+        exact = dd(oracle, a, b, ("s", m, n, k))
+        scale = np.linalg.norm(a.astype(np.float64)) * np.linalg.norm(b.astype(np.float64))
+        assert np.linalg.norm(c - exact) / scale <= 2.0 ** -15 + k * U32
+        c = c0.copy()
+        assert fg.gemm_f32(m, n, k, 0.5, a, b, -2.0, c, mode="split")
+        ref = 0.5 * exact - 2.0 * c0.astype(np.float64)
+        assert np.linalg.norm(c - ref) / scale <= 2.0 ** -15 + k * U32 + 4 * U32
+
+
+@pytest.mark.parametrize("op,dt,u", [("f64", np.float64, U64), ("f32", np.float32, U32)])
+@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("splits", SPLITS)
+@pytest.mark.parametrize("m,n,k", SHAPES)
+def test_plain_variants(fg, oracle, op, dt, u, variant, splits, m, n, k):
+    r = rng(m + 5 * n)
+    a = r.uniform(-1, 1, (m, k)).astype(dt)
+    b = r.uniform(-1, 1, (k, n)).astype(dt)
+    c0 = r.uniform(-1, 1, (m, n)).astype(dt)
+    gemm = fg.gemm_f64 if dt == np.float64 else fg.gemm_f32
+    with fg.tune_forced(op, variant, splits):
+        c = np.zeros((m, n), dt)
+        assert gemm(m, n, k, 1.0, a, b, 0.0, c)
+        exact = dd(oracle, a, b, (op, m, n, k))
+        scale = np.linalg.norm(a.astype(np.float64)) * np.linalg.norm(b.astype(np.float64))
+        assert np.linalg.norm(c - exact) / scale <= k * u
+        c = c0.copy()
+        assert gemm(m, n, k, 0.5, a, b, 2.0, c)
+        ref = 0.5 * exact + 2.0 * c0.astype(np.float64)
+        assert np.linalg.norm(c - ref) / scale <= (k + 4) * u
+
+
+@pytest.mark.parametrize("variant,splits", [(0, 2), (1, 4)])
+def test_plain_split_broadcast_batch(fg, oracle, variant, splits):
+    r = rng(4)
+    a = r.uniform(-1, 1, (2, 3, 33, 700))
+    b = r.uniform(-1, 1, (3, 700, 45))
+    with fg.tune_forced("f64", variant, splits):
+        got = fg.matmul(fg.DeviceArray.from_numpy(a), fg.DeviceArray.from_numpy(b)).to_numpy()
+    want = np.matmul(a, b)
+    assert np.max(np.abs(got - want)) <= 700 * U64 * 700
+
+
+def test_default_table_choices_are_valid_on_device(fg):
+    # every bucket's compiled-in choice runs and agrees with the forced baseline
+    r = rng(1)
+    m, n, k = 100, 90, 2000
+    a = r.integers(-128, 128, (m, k), dtype=np.int8)
+    b = r.integers(-128, 128, (k, n), dtype=np.int8)
+    c1 = np.zeros((m, n), np.int32)
+    c2 = np.zeros((m, n), np.int32)
+    assert fg.gemm_i8_signed(m, n, k, a, b, c1)
+    with fg.tune_forced("i8", 0, 1):
+        assert fg.gemm_i8_signed(m, n, k, a, b, c2)
+    np.testing.assert_array_equal(c1, c2)
