@@ -166,7 +166,7 @@ def tune_op(fg, L, ctx, op, sm_count, log):
                             t = bench.time(m, n, k)
                             ok = (v, s) == (0, 1) or _agree(op, ref, bench.result(m, n), k)
                             cands.append({"variant": v, "splits": s, "ms": round(t * 1e3, 5),
-                                          "agrees": ok})
+                                          "agrees": bool(ok)})
                     base = next(c for c in cands if (c["variant"], c["splits"]) == (0, 1))
                     best = min((c for c in cands if c["agrees"]), key=lambda c: c["ms"])
                     if best["ms"] * MARGIN >= base["ms"]:
