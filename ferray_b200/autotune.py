@@ -36,7 +36,7 @@ REPR = [128, 256, 512, 1024, 2048, 4096, 8192]
 SPLITS = [1, 2, 4, 8, 16]
 MARGIN = 1.03  # a candidate must beat the untuned kernel by 3%
 # tile edge per variant (output tiles per block row / column)
-TILES = {"i8": [(128, 256), (128, 128)], "split_f32": [(128, 128), (128, 64)],
+TILES = {"i8": [(128, 256), (128, 128), (256, 256)], "split_f32": [(128, 128), (128, 64)],
          "f64": [(128, 128), (64, 64)], "f32": [(128, 128), (64, 64)]}
 # K per split unit: one tcgen05 K block, or the SIMT split granularity
 KUNIT = {"i8": 128, "split_f32": 64, "f64": 64, "f32": 64}
@@ -189,6 +189,8 @@ def main(argv=None):
     ap.add_argument("--out", default=".")
     ap.add_argument("--ops", default=",".join(OPS))
     ap.add_argument("--default", action="store_true", help="write the untuned table")
+    ap.add_argument("--merge", default=None,
+                    help="tune_table.json whose choices are kept for the ops not retuned")
     args = ap.parse_args(argv)
     os.makedirs(args.out, exist_ok=True)
     if args.default:
@@ -209,6 +211,18 @@ def main(argv=None):
     report = {"gpu": gpu, "sm_count": info["sm_count"],
               "date": datetime.datetime.utcnow().strftime("%Y-%m-%d %H:%M UTC"),
               "buckets": REPR, "ops": {}}
+    if args.merge:
+        old = json.load(open(args.merge))
+        for op, rows in old["ops"].items():
+            if op in args.ops.split(","):
+                continue
+            recs = []
+            for r in rows:
+                m, n, k, v, sp = r[:5]
+                choice[op][REPR.index(m)][REPR.index(n)][REPR.index(k)] = (v, sp)
+                recs.append(r)
+            report["ops"][op] = recs
+        report["merged_from"] = {"date": old.get("date"), "ops": sorted(report["ops"])}
     t0 = time.time()
     for op in args.ops.split(","):
         choice[op], recs = tune_op(fg, L, ctx, op, info["sm_count"], print)
@@ -219,7 +233,8 @@ def main(argv=None):
     # compact copy (committed beside the table): per bucket the choice and
     # the untuned / tuned times
     compact = dict(report)
-    compact["ops"] = {op: [[r["m"], r["n"], r["k"], r["choice"][0], r["choice"][1],
+    compact["ops"] = {op: [r if isinstance(r, list) else
+                           [r["m"], r["n"], r["k"], r["choice"][0], r["choice"][1],
                             r["untuned_ms"], r["tuned_ms"], len(r["candidates"]), r["rejected"]]
                            for r in recs] for op, recs in report["ops"].items()}
     compact["columns"] = ["m", "n", "k", "variant", "splits", "untuned_ms", "tuned_ms",

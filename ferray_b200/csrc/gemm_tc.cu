@@ -13,6 +13,7 @@
 #include "prep_kernels.cuh"
 #include "runtime.h"
 #include "tc_gemm.cuh"
+#include "tc_gemm2.cuh"
 #include "tune.h"
 
 namespace fgrt {
@@ -23,6 +24,8 @@ using namespace fg;
 // 6 stages, for problems with few output tiles.
 using CfgI8 = TcCfg<KIND_I8, 256, 4, 1, 1, 1, 1, EPI_I32>;
 using CfgI8n128 = TcCfg<KIND_I8, 128, 6, 1, 1, 1, 1, EPI_I32>;
+// 256 x 256 tiles on CTA pairs (cta_group::2), 6 stages of 32 KB per CTA.
+using CfgI8Pair = Tc2Cfg<KIND_I8, 256, 6, 1, 1, 1, 1, EPI_I32>;
 using CfgQmm = TcCfg<KIND_I8, 256, 4, 1, 1, 1, 1, EPI_QMM>;
 using CfgI16 = TcCfg<KIND_I8, 128, 3, 2, 2, 3, 4, EPI_I16>;
 // 3 products: one accumulator (the 2-slice representation error, about
@@ -45,6 +48,7 @@ static unsigned long long kTimeoutNs = 4000000000ull;  // 4 s per wait
 
 template <class Cfg>
 static const char* cfg_name() {
+    if (Cfg::BM == 256) return Cfg::KIND == KIND_BF16 ? "tc_gemm2_3xbf16" : "tc_gemm2_i8";
     if (Cfg::KIND == KIND_BF16) return Cfg::NOPS == 6 ? "tc_gemm_6xbf16" : "tc_gemm_3xbf16";
     if (Cfg::EPI == EPI_I16) return "tc_gemm_i16";
     if (Cfg::EPI == EPI_QMM) return "tc_gemm_qmm";
@@ -78,6 +82,51 @@ static fg_status launch_cfg(fg_ctx* ctx, const TcMaps& maps, TcArgs& args, cudaS
     return FG_OK;
 }
 
+// CTA-pair kernels: a persistent grid of as many pairs as can be resident
+// (cudaOccupancyMaxActiveClusters; at most one pair per TPC).
+template <class Cfg>
+static fg_status launch_pair(fg_ctx* ctx, const TcMaps& maps, TcArgs& args, cudaStream_t st) {
+    static std::once_flag once;
+    static cudaError_t attr_err = cudaSuccess;
+    static int max_pairs = 0;
+    std::call_once(once, [ctx] {
+        attr_err = cudaFuncSetAttribute(tc_gemm2_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(tc2_smem_bytes<Cfg>()));
+        if (attr_err != cudaSuccess) return;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(static_cast<unsigned>(ctx->sm_count & ~1), 1, 1);
+        cfg.blockDim = dim3(Cfg::THREADS, 1, 1);
+        cfg.dynamicSmemBytes = tc2_smem_bytes<Cfg>();
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, tc_gemm2_kernel<Cfg>, &cfg) == cudaSuccess && n > 0)
+            max_pairs = n;
+        else
+            cudaGetLastError();
+        if (max_pairs <= 0) max_pairs = ctx->sm_count / 2;
+    });
+    FG_CUDA(attr_err);
+    args.status = ctx->d_status;
+    args.timeout_ns = kTimeoutNs;
+    const long long units =
+        (long long)std::max(args.splits, 1) * args.batch * args.tiles_m * args.tiles_n;
+    if (units == 0) return FG_OK;
+    const int grid = 2 * static_cast<int>(std::min<long long>(units, max_pairs));
+    ProfScope prof(cfg_name<Cfg>(), st);
+    tc_gemm2_kernel<Cfg><<<grid, Cfg::THREADS, tc2_smem_bytes<Cfg>(), st>>>(maps, args);
+    prof.stop();
+    count_launch();
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+template <class Cfg>
+static fg_status launch_any(fg_ctx* ctx, const TcMaps& maps, TcArgs& args, cudaStream_t st) {
+    if constexpr (Cfg::BM == 256)
+        return launch_pair<Cfg>(ctx, maps, args, st);
+    else
+        return launch_cfg<Cfg>(ctx, maps, args, st);
+}
+
 // Launches Cfg with up to `want` K splits (tuned).  With more than one
 // split the kernel writes dense partial products [split][batch][M][N] into a
 // workspace and splitk_reduce_kernel combines them into C (wrapping int32
@@ -89,7 +138,7 @@ static fg_status launch_splitk(fg_ctx* ctx, const TcMaps& maps, TcArgs& args, in
     const long long M = args.M, N = args.N, out_elems = M * N * args.batch;
     int kps = args.k_blocks;
     const int splits = plan_splits(want, args.k_blocks, out_elems, sizeof(T), &kps);
-    if (splits <= 1) return launch_cfg<Cfg>(ctx, maps, args, st);
+    if (splits <= 1) return launch_any<Cfg>(ctx, maps, args, st);
     Scratch ws;
     FG_TRY(ws.alloc(static_cast<size_t>(splits * out_elems) * sizeof(T), st));
     args.splits = splits;
@@ -100,7 +149,7 @@ static fg_status launch_splitk(fg_ctx* ctx, const TcMaps& maps, TcArgs& args, in
     args.accumulate = 0;
     args.alpha = 1.f;
     args.beta = 0.f;
-    FG_TRY(launch_cfg<Cfg>(ctx, maps, args, st));
+    FG_TRY(launch_any<Cfg>(ctx, maps, args, st));
     splitk_reduce_kernel<T><<<grid_for_total(out_elems), 256, 0, st>>>(
         static_cast<const T*>(ws.p), splits, M, N, args.batch, C, ldc, strideC, alpha, beta,
         accumulate);
@@ -223,6 +272,12 @@ fg_status launch_int_tc(fg_ctx* ctx, const Gemm& g0, cudaStream_t st) {
         args.ops[0] = TcOp{0, 0, 0, g.dtype == FG_I8 ? 1 : 0, 1};
         const TuneChoice c = tune_lookup(TUNE_I8, g.M, g.N, g.K);
         int32_t* C = static_cast<int32_t*>(g.C);
+        if (c.variant == 2) {
+            args.tiles_m = static_cast<int>((g.M + CfgI8Pair::BM - 1) / CfgI8Pair::BM);
+            args.tiles_n = static_cast<int>((g.N + CfgI8Pair::BN - 1) / CfgI8Pair::BN);
+            return launch_splitk<CfgI8Pair, int32_t>(ctx, maps, args, c.splits, C, g.ldc, g.c_stride,
+                                                     0, 0, g.accumulate, st);
+        }
         if (c.variant == 1) {
             args.tiles_n = static_cast<int>((g.N + CfgI8n128::BN - 1) / CfgI8n128::BN);
             return launch_splitk<CfgI8n128, int32_t>(ctx, maps, args, c.splits, C, g.ldc, g.c_stride,

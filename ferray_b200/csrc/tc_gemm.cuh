@@ -205,10 +205,15 @@ __device__ __forceinline__ void epilogue_store(const TcArgs& p, int bz, int grow
                 *reinterpret_cast<uint4*>(crow + j) = w;
             }
         } else {
-            for (int j = 0; j < ncols; ++j) {
-                uint32_t w = out[j];
-                if (p.accumulate) w += static_cast<uint32_t>(crow[j]);
-                crow[j] = static_cast<int32_t>(w);
+            // fully unrolled with a predicate: a runtime trip count would
+            // index `out` dynamically and move it to local memory
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                if (j < ncols) {
+                    uint32_t w = out[j];
+                    if (p.accumulate) w += static_cast<uint32_t>(crow[j]);
+                    crow[j] = static_cast<int32_t>(w);
+                }
             }
         }
     } else if constexpr (Cfg::EPI == EPI_QMM) {
@@ -216,7 +221,9 @@ __device__ __forceinline__ void epilogue_store(const TcArgs& p, int bz, int grow
         const uint32_t rs = static_cast<uint32_t>(p.row_sum[grow]);
         const uint32_t azp = static_cast<uint32_t>(p.a_zp), bzp = static_cast<uint32_t>(p.b_zp);
         const uint32_t kab = static_cast<uint32_t>(p.K) * azp * bzp;
-        for (int j = 0; j < ncols; ++j) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            if (j >= ncols) break;
             uint32_t cs = static_cast<uint32_t>(p.col_sum[gcol0 + j]);
             uint32_t corr = v[0][j] - azp * cs - bzp * rs + kab;
             // Separate roundings, as gemm/mod.rs:566-571 computes them (no FMA).
@@ -228,7 +235,9 @@ __device__ __forceinline__ void epilogue_store(const TcArgs& p, int bz, int grow
         double* cbase = static_cast<double*>(p.C) + bz * p.strideC;
         const double rs = p.row_scale[grow] * p.oz_w;
         const int h = p.cplx_half;
-        for (int j = 0; j < ncols; ++j) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            if (j >= ncols) break;
             const int col = gcol0 + j;
             const int cc = (h > 0 && col >= h) ? col - h : col;
             double* dst = h > 0 ? cbase + (long long)grow * p.ldc + 2 * cc + (col < h ? 0 : 1)
@@ -248,7 +257,9 @@ __device__ __forceinline__ void epilogue_store(const TcArgs& p, int bz, int grow
             // Column j of the real-embedded product is Re (j < h) or Im (j >= h)
             // of complex column j mod h; C is interleaved (re, im).
             const int h = p.cplx_half;
-            for (int j = 0; j < ncols; ++j) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                if (j >= ncols) break;
                 int col = gcol0 + j;
                 int cc = col < h ? col : col - h;
                 float* dst = cbase + (long long)grow * p.ldc + 2 * cc + (col < h ? 0 : 1);
@@ -275,10 +286,13 @@ __device__ __forceinline__ void epilogue_store(const TcArgs& p, int bz, int grow
                 *reinterpret_cast<float4*>(crow + j) = w;
             }
         } else {
-            for (int j = 0; j < ncols; ++j) {
-                float o = out[j];
-                if (p.beta != 0.f) o = fmaf(p.beta, crow[j], o);
-                crow[j] = o;
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                if (j < ncols) {
+                    float o = out[j];
+                    if (p.beta != 0.f) o = fmaf(p.beta, crow[j], o);
+                    crow[j] = o;
+                }
             }
         }
     }
@@ -331,8 +345,9 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
         if (elect_one()) {
             int stage = 0;
             uint32_t phase = 0;
-            int issued_parity[Cfg::STAGES];
-            for (int i = 0; i < Cfg::STAGES; ++i) issued_parity[i] = -1;
+            // per stage: bit = a load was issued, bit = its phase parity
+            // (register bitmasks; an indexed array would live in local memory)
+            uint32_t issued_mask = 0, issued_par = 0;
             bool ok = true;
             for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x) {
                 int zo, bz, tm, tn, za, zb, kb0, kb1;
@@ -363,7 +378,8 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
                                 tma_load_2d(dst, &maps.b[i], nx, kx, &s.full[stage]);
                         }
                     }
-                    issued_parity[stage] = static_cast<int>(phase);
+                    issued_mask |= 1u << stage;
+                    issued_par = (issued_par & ~(1u << stage)) | (phase << stage);
                     if (++stage == Cfg::STAGES) {
                         stage = 0;
                         phase ^= 1u;
@@ -373,10 +389,9 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
             if (!ok) {
                 // Let every load this thread issued land before the CTA exits.
                 for (int i = 0; i < Cfg::STAGES; ++i) {
-                    if (issued_parity[i] < 0) continue;
+                    if (!((issued_mask >> i) & 1u)) continue;
                     volatile int never = 0;
-                    mbar_wait(&s.full[i], static_cast<uint32_t>(issued_parity[i]), p.timeout_ns,
-                              nullptr, 0, &never);
+                    mbar_wait(&s.full[i], (issued_par >> i) & 1u, p.timeout_ns, nullptr, 0, &never);
                 }
             }
         }
