@@ -99,8 +99,8 @@ __device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap* map) {
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
 
-// 2-D tiled load global -> shared, completion counted on `bar` (no cluster
-// multicast anywhere in this code base).
+// 2-D tiled load global -> shared, completion counted on `bar` (no TMA load
+// in this code base uses cluster multicast).
 __device__ __forceinline__ void tma_load_2d(void* smem_dst, const CUtensorMap* map, int x, int y,
                                             uint64_t* bar) {
     asm volatile(

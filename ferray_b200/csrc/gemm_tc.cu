@@ -33,6 +33,8 @@ using CfgI16 = TcCfg<KIND_I8, 128, 3, 2, 2, 3, 4, EPI_I16>;
 // 6 products: accumulator 0 holds hi*hi, accumulator 1 the corrections.
 using CfgBf16x3 = TcCfg<KIND_BF16, 128, 3, 2, 2, 1, 3, EPI_F32, 1>;
 using CfgBf16x3n64 = TcCfg<KIND_BF16, 64, 4, 2, 2, 1, 3, EPI_F32, 1>;
+// 256 x 128 tiles on CTA pairs, 4 stages of 48 KB per CTA.
+using CfgBf16x3Pair = Tc2Cfg<KIND_BF16, 128, 4, 2, 2, 1, 3, EPI_F32, 1>;
 using CfgBf16x6 = TcCfg<KIND_BF16, 128, 2, 3, 3, 2, 6, EPI_F32, 1>;
 
 // K blocks (64 bf16 each) per TMEM accumulation chunk of the split SGEMM.
@@ -470,6 +472,12 @@ fg_status launch_split_bf16(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
     const TuneChoice c = cplx ? TuneChoice{0, 1} : tune_lookup(TUNE_SPLIT_F32, M, N, K);
     float* C = static_cast<float*>(g.C);
     const float alpha = args.alpha, beta = args.beta;
+    if (c.variant == 2) {
+        args.tiles_m = static_cast<int>((M + CfgBf16x3Pair::BM - 1) / CfgBf16x3Pair::BM);
+        args.tiles_n = static_cast<int>((N + CfgBf16x3Pair::BN - 1) / CfgBf16x3Pair::BN);
+        return launch_splitk<CfgBf16x3Pair, float>(ctx, maps, args, c.splits, C, g.ldc, g.c_stride,
+                                                   alpha, beta, 0, st);
+    }
     if (c.variant == 1) {
         args.tiles_n = static_cast<int>((N + CfgBf16x3n64::BN - 1) / CfgBf16x3n64::BN);
         return launch_splitk<CfgBf16x3n64, float>(ctx, maps, args, c.splits, C, g.ldc, g.c_stride,

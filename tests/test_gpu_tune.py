@@ -58,9 +58,9 @@ def test_i8_split_broadcast_batch(fg, oracle, variant, splits):
     np.testing.assert_array_equal(got, want)
 
 
-@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("variant", [0, 1, 2])
 @pytest.mark.parametrize("splits", SPLITS)
-@pytest.mark.parametrize("m,n,k", SHAPES)
+@pytest.mark.parametrize("m,n,k", SHAPES + [(300, 200, 700)])
 def test_split_f32_variants(fg, oracle, variant, splits, m, n, k):
     r = rng(m * 3 + k)
     a = r.standard_normal((m, k), dtype=np.float32)
