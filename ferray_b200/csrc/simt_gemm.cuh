@@ -31,11 +31,16 @@ __device__ __forceinline__ void batch_offsets(const BatchMap& bm, int bz, long l
     oa = 0;
     ob = 0;
     int rem = bz;
-    for (int d = bm.bdims - 1; d >= 0; --d) {
-        int idx = rem % bm.bshape[d];
-        rem /= bm.bshape[d];
-        oa += idx * bm.a_bstride[d];
-        ob += idx * bm.b_bstride[d];
+    // unrolled over the 4 possible dims: constant indices keep the
+    // parameter struct out of local memory
+#pragma unroll
+    for (int d = 3; d >= 0; --d) {
+        if (d < bm.bdims) {
+            const int idx = rem % bm.bshape[d];
+            rem /= bm.bshape[d];
+            oa += idx * bm.a_bstride[d];
+            ob += idx * bm.b_bstride[d];
+        }
     }
 }
 
@@ -44,8 +49,10 @@ __device__ __forceinline__ void batch_offsets(const BatchMap& bm, int bz, long l
 // problems).  Split-K: blockIdx.z = split * nbatch + batch index; split s
 // covers K columns [s * ksplit, (s + 1) * ksplit) and writes output matrix
 // blockIdx.z (the host points C at a partial-sum workspace then).
+// Two resident blocks per SM for the f32 128 x 128 tile (at most 128
+// registers a thread); the f64 one needs more registers than that.
 template <typename T, int BK, int TM>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, (sizeof(T) == 4 && TM == 8) ? 2 : 1)
     simt_gemm_real(int M, int N, int K, T alpha, const T* __restrict__ A, long long lda,
                    const T* __restrict__ B, long long ldb, T beta, T* __restrict__ C,
                    long long ldc, BatchMap bm, int nbatch, int ksplit) {
