@@ -265,6 +265,8 @@ fg_status fg_init(int device, fg_ctx** out) {
     ctx->cc_minor = prop.minor;
     ctx->hbm_bytes = prop.totalGlobalMem;
     cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->pipe_comp, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->pipe_out, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_status, sizeof(fg::DevStatus));
     if (e == cudaSuccess) e = cudaMemset(ctx->d_status, 0, sizeof(fg::DevStatus));
     if (e != cudaSuccess) {
@@ -285,7 +287,11 @@ fg_status fg_shutdown(fg_ctx* ctx) {
     if (!ctx) return FG_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    if (ctx->pipe_comp) cudaStreamSynchronize(ctx->pipe_comp);
+    if (ctx->pipe_out) cudaStreamSynchronize(ctx->pipe_out);
     cudaFree(ctx->d_status);
+    if (ctx->pipe_comp) cudaStreamDestroy(ctx->pipe_comp);
+    if (ctx->pipe_out) cudaStreamDestroy(ctx->pipe_out);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return FG_OK;
@@ -458,21 +464,24 @@ fg_status fg_quantized_matmul(fg_ctx* ctx, size_t m, size_t n, size_t k, const u
                       b_zp, c, accumulate, st);
 }
 
+// Host-pointer GEMM, pipelined over row panels of A and C: B goes up first,
+// then panel i of A (and of C when it is read) on the copy-in stream; the
+// GEMM of panel i runs on the compute stream once its inputs have landed and
+// its C panel comes back on the copy-out stream while later panels are still
+// uploading, so the host<->device copies (full duplex) overlap each other
+// and the GEMMs.  Panels are whole 256-row tiles; small problems use one.
 fg_status fg_gemm_host(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, int slices, size_t m,
                        size_t n, size_t k, const void* alpha, const void* a, const void* b,
                        const void* beta, void* c, int accumulate) {
     if (!ctx) return set_error(FG_ERR_INVALID, "null context");
     if (!valid_dtype(dtype)) return set_error(FG_ERR_DTYPE, "unknown dtype");
     if (m == 0 || n == 0) return FG_OK;
+    if (!c || (k > 0 && (!a || !b))) return set_error(FG_ERR_INVALID, "null operand pointer");
     FG_CUDA(cudaSetDevice(ctx->device));
-    cudaStream_t st = ctx->stream;
-    const size_t ia = in_size(dtype) * m * k, ib = in_size(dtype) * k * n, ic = out_size(dtype) * m * n;
-    Scratch sa, sb, sc;
-    FG_TRY(sa.alloc(ia, st));
-    FG_TRY(sb.alloc(ib, st));
-    FG_TRY(sc.alloc(ic, st));
-    if (ia) FG_CUDA(cudaMemcpyAsync(sa.p, a, ia, cudaMemcpyHostToDevice, st));
-    if (ib) FG_CUDA(cudaMemcpyAsync(sb.p, b, ib, cudaMemcpyHostToDevice, st));
+    std::lock_guard<std::mutex> lk(ctx->host_mu);
+    cudaStream_t s_in = ctx->stream, s_cmp = ctx->pipe_comp, s_out = ctx->pipe_out;
+    const size_t ein = in_size(dtype), eout = out_size(dtype);
+    const size_t ia = ein * m * k, ib = ein * k * n, ic = eout * m * n;
     bool reads_c = accumulate != 0;
     if (!is_integer(dtype) && beta) {
         const double* bd = static_cast<const double*>(beta);
@@ -485,11 +494,59 @@ fg_status fg_gemm_host(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, int slices, si
             default: break;
         }
     }
-    if (reads_c) FG_CUDA(cudaMemcpyAsync(sc.p, c, ic, cudaMemcpyHostToDevice, st));
-    FG_TRY(fg_gemm(ctx, dtype, mode, slices, m, n, k, alpha, sa.p, k, sb.p, n, beta, sc.p, n,
-                   accumulate, st));
-    FG_CUDA(cudaMemcpyAsync(c, sc.p, ic, cudaMemcpyDeviceToHost, st));
-    return fg_sync(ctx, st);
+    Scratch sa, sb, sc;
+    FG_TRY(sa.alloc(ia, s_in));
+    FG_TRY(sb.alloc(ib, s_in));
+    FG_TRY(sc.alloc(ic, s_in));
+    // Destroyed before the scratch (declared after it): whatever path
+    // leaves, the frees queued on s_in wait for the compute and copy-out
+    // streams.
+    struct Join {
+        cudaStream_t in, cmp, out;
+        ~Join() {
+            for (cudaStream_t s : {cmp, out}) {
+                cudaEvent_t e;
+                if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess) {
+                    cudaEventRecord(e, s);
+                    cudaStreamWaitEvent(in, e, 0);
+                    cudaEventDestroy(e);
+                }
+            }
+        }
+    } join{s_in, s_cmp, s_out};
+    const size_t total = ia + ib + ic;
+    const size_t kPanelBytes = 64u << 20;
+    long long panels = total <= kPanelBytes ? 1 : std::min<long long>(8, (total + kPanelBytes - 1) / kPanelBytes);
+    long long rows = ((long long)m + panels - 1) / panels;
+    rows = (rows + 255) / 256 * 256;
+    panels = ((long long)m + rows - 1) / rows;
+    if (ib) FG_CUDA(cudaMemcpyAsync(sb.p, b, ib, cudaMemcpyHostToDevice, s_in));
+    uint8_t* da = static_cast<uint8_t*>(sa.p);
+    uint8_t* dc = static_cast<uint8_t*>(sc.p);
+    const uint8_t* ha = static_cast<const uint8_t*>(a);
+    uint8_t* hc = static_cast<uint8_t*>(c);
+    for (long long i = 0; i < panels; ++i) {
+        const size_t r0 = static_cast<size_t>(i * rows);
+        const size_t mi = std::min<size_t>(m - r0, static_cast<size_t>(rows));
+        const size_t oa = r0 * k * ein, na = mi * k * ein, oc = r0 * n * eout, nc = mi * n * eout;
+        if (na) FG_CUDA(cudaMemcpyAsync(da + oa, ha + oa, na, cudaMemcpyHostToDevice, s_in));
+        if (reads_c) FG_CUDA(cudaMemcpyAsync(dc + oc, hc + oc, nc, cudaMemcpyHostToDevice, s_in));
+        cudaEvent_t in_ready, out_ready;
+        FG_CUDA(cudaEventCreateWithFlags(&in_ready, cudaEventDisableTiming));
+        cudaEventRecord(in_ready, s_in);  // after B and this panel's copies
+        cudaStreamWaitEvent(s_cmp, in_ready, 0);
+        cudaEventDestroy(in_ready);
+        FG_TRY(fg_gemm(ctx, dtype, mode, slices, mi, n, k, alpha, da + oa, k, sb.p, n, beta,
+                       dc + oc, n, accumulate, s_cmp));
+        FG_CUDA(cudaEventCreateWithFlags(&out_ready, cudaEventDisableTiming));
+        cudaEventRecord(out_ready, s_cmp);
+        cudaStreamWaitEvent(s_out, out_ready, 0);
+        cudaEventDestroy(out_ready);
+        FG_CUDA(cudaMemcpyAsync(hc + oc, dc + oc, nc, cudaMemcpyDeviceToHost, s_out));
+    }
+    FG_CUDA(cudaStreamSynchronize(s_out));
+    FG_CUDA(cudaStreamSynchronize(s_cmp));
+    return fg_sync(ctx, s_in);
 }
 
 fg_status fg_gemm_f64_host(fg_ctx* ctx, fg_mode mode, int slices, size_t m, size_t n, size_t k,

@@ -14,12 +14,17 @@
 #include "ozaki_kernels.cuh"
 #include "runtime.h"
 #include "tc_gemm.cuh"
+#include "tc_gemm2.cuh"
+#include "tune.h"
 
 namespace fgrt {
 
 using namespace fg;
 
 using CfgOzaki = TcCfg<KIND_I8, 256, 4, 1, 1, 1, 1, EPI_OZAKI>;
+// CTA-pair form (256 x 256 tiles), used where the tuned i8 table picks the
+// pair kernel for the group's (M, N, K).
+using CfgOzakiPair = Tc2Cfg<KIND_I8, 256, 6, 1, 1, 1, 1, EPI_OZAKI>;
 
 static int grid_for(long long total) {
     return static_cast<int>(std::min<long long>(std::max<long long>((total + 255) / 256, 1), 8192));
@@ -27,20 +32,43 @@ static int grid_for(long long total) {
 
 static long long round_up(long long x, long long a) { return (x + a - 1) / a * a; }
 
+template <class Cfg>
 static fg_status launch_group(fg_ctx* ctx, const TcMaps& maps, TcArgs& args, cudaStream_t st) {
+    constexpr bool pair = Cfg::BM == 256;
     static std::once_flag once;
     static cudaError_t attr_err = cudaSuccess;
-    std::call_once(once, [] {
-        attr_err = cudaFuncSetAttribute(tc_gemm_kernel<CfgOzaki>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(tc_smem_bytes<CfgOzaki>()));
+    static int max_units = 0;
+    std::call_once(once, [ctx] {
+        if constexpr (pair) {
+            attr_err = cudaFuncSetAttribute(tc_gemm2_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            static_cast<int>(tc2_smem_bytes<Cfg>()));
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(static_cast<unsigned>(ctx->sm_count & ~1), 1, 1);
+            cfg.blockDim = dim3(Cfg::THREADS, 1, 1);
+            cfg.dynamicSmemBytes = tc2_smem_bytes<Cfg>();
+            int n = 0;
+            if (attr_err == cudaSuccess &&
+                cudaOccupancyMaxActiveClusters(&n, tc_gemm2_kernel<Cfg>, &cfg) == cudaSuccess && n > 0)
+                max_units = n;
+            else
+                cudaGetLastError();
+            if (max_units <= 0) max_units = ctx->sm_count / 2;
+        } else {
+            attr_err = cudaFuncSetAttribute(tc_gemm_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            static_cast<int>(tc_smem_bytes<Cfg>()));
+            max_units = ctx->sm_count;
+        }
     });
     FG_CUDA(attr_err);
     args.status = ctx->d_status;
     args.timeout_ns = 4000000000ull;
     const long long tiles = (long long)args.tiles_m * args.tiles_n;
-    const int grid = static_cast<int>(std::min<long long>(tiles, ctx->sm_count));
-    ProfScope prof("tc_gemm_ozaki_i8", st);
-    tc_gemm_kernel<CfgOzaki><<<grid, CfgOzaki::THREADS, tc_smem_bytes<CfgOzaki>(), st>>>(maps, args);
+    const int units = static_cast<int>(std::min<long long>(tiles, max_units));
+    ProfScope prof(pair ? "tc_gemm2_ozaki_i8" : "tc_gemm_ozaki_i8", st);
+    if constexpr (pair)
+        tc_gemm2_kernel<Cfg><<<2 * units, Cfg::THREADS, tc2_smem_bytes<Cfg>(), st>>>(maps, args);
+    else
+        tc_gemm_kernel<Cfg><<<units, Cfg::THREADS, tc_smem_bytes<Cfg>(), st>>>(maps, args);
     prof.stop();
     count_launch();
     FG_CUDA(cudaGetLastError());
@@ -169,10 +197,11 @@ fg_status launch_ozaki(fg_ctx* ctx, const Gemm& g0, cudaStream_t st) {
                 FG_TRY(encode_map(&maps.b[0], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2,
                                   bc + (S - d + 1) * Kc * Np, dims, strides, box));
             }
+            const bool pair = tune_lookup(TUNE_I8, M, Nw, Kd).variant == 2;
             args.M = static_cast<int>(M);
             args.N = static_cast<int>(Nw);
             args.K = static_cast<int>(Kd);
-            args.tiles_m = static_cast<int>((M + 127) / 128);
+            args.tiles_m = static_cast<int>((M + (pair ? 255 : 127)) / (pair ? 256 : 128));
             args.tiles_n = static_cast<int>((Nw + CfgOzaki::BN - 1) / CfgOzaki::BN);
             args.k_blocks = static_cast<int>((Kd + CfgOzaki::BK - 1) / CfgOzaki::BK);
             args.batch = 1;
@@ -187,7 +216,10 @@ fg_status launch_ozaki(fg_ctx* ctx, const Gemm& g0, cudaStream_t st) {
             args.oz_beta = g.beta_re;
             args.oz_first = first ? 1 : 0;
             args.ops[0] = TcOp{0, 0, 0, 1, 1};
-            FG_TRY(launch_group(ctx, maps, args, st));
+            if (pair)
+                FG_TRY(launch_group<CfgOzakiPair>(ctx, maps, args, st));
+            else
+                FG_TRY(launch_group<CfgOzaki>(ctx, maps, args, st));
             first = false;
         }
     }

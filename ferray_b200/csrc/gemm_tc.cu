@@ -418,12 +418,12 @@ fg_status launch_split_bf16(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
         }
     } else {
         if (M * K > 0) {
-            split_bf16_kernel<<<dim3(grid_for(M * (K + 3) / 4), static_cast<unsigned>(g.a_count)), 256, 0, st>>>(
+            split_bf16_kernel<<<dim3(static_cast<unsigned>(std::min<long long>(M, 4096)), static_cast<unsigned>(g.a_count)), 256, 0, st>>>(
                 static_cast<const float*>(g.A), M, K, g.lda, ap, pa, ns, g.a_mstride, pa * M);
             count_launch();
         }
         if (K * N > 0) {
-            split_bf16_kernel<<<dim3(grid_for(K * (N + 3) / 4), static_cast<unsigned>(g.b_count)), 256, 0, st>>>(
+            split_bf16_kernel<<<dim3(static_cast<unsigned>(std::min<long long>(K, 4096)), static_cast<unsigned>(g.b_count)), 256, 0, st>>>(
                 static_cast<const float*>(g.B), K, N, g.ldb, bp, pb, ns, g.b_mstride, pb * K);
             count_launch();
         }

@@ -39,35 +39,47 @@ __device__ __forceinline__ void split_n(float x, int ns, __nv_bfloat16 (&o)[3]) 
 }
 
 // Real operand: X (rows x cols, pitch ldx) -> ns planes (pitch ldo, a
-// multiple of 4).  Four consecutive elements per thread, 8-byte stores.
+// multiple of 4).  Blocks stride over rows, threads over 4-element groups
+// of a row (no per-element division); two groups per thread per step keep
+// two 16-byte loads in flight; 8-byte stores per plane.
 static __global__ void split_bf16_kernel(const float* __restrict__ X, long long rows, long long cols,
                                          long long ldx, BfPlanes out, long long ldo, int ns,
                                          long long x_bstride, long long o_bstride) {
     const float* Xb = X + blockIdx.y * x_bstride;
     const long long cq = (cols + 3) / 4;
-    const long long total = rows * cq;
     const bool vec_in = (ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(Xb) & 15) == 0);
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-         e += (long long)gridDim.x * blockDim.x) {
-        const long long r = e / cq, c = (e - r * cq) * 4;
-        float v[4];
-        if (vec_in && c + 3 < cols) {
-            const float4 q = *reinterpret_cast<const float4*>(Xb + r * ldx + c);
-            v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
-        } else {
+    for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+        const float* xr = Xb + r * ldx;
+        for (long long q0 = threadIdx.x; q0 < cq; q0 += 2 * blockDim.x) {
+            float v[2][4];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) v[j] = (c + j < cols) ? Xb[r * ldx + c + j] : 0.f;
-        }
-        __nv_bfloat16 o[4][3];
+            for (int u = 0; u < 2; ++u) {
+                const long long c = (q0 + u * blockDim.x) * 4;
+                if (vec_in && c + 3 < cols) {
+                    const float4 w = *reinterpret_cast<const float4*>(xr + c);
+                    v[u][0] = w.x; v[u][1] = w.y; v[u][2] = w.z; v[u][3] = w.w;
+                } else {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) split_n(v[j], ns, o[j]);
-        for (int s = 0; s < ns; ++s) {
-            __nv_bfloat16* dst = out.p[s] + blockIdx.y * o_bstride + r * ldo + c;
-            if (c + 3 < ldo) {
-                __align__(8) __nv_bfloat16 w[4] = {o[0][s], o[1][s], o[2][s], o[3][s]};
-                *reinterpret_cast<uint2*>(dst) = *reinterpret_cast<const uint2*>(w);
-            } else {
-                for (int j = 0; j < 4 && c + j < ldo; ++j) dst[j] = o[j][s];
+                    for (int j = 0; j < 4; ++j) v[u][j] = (c + j < cols) ? xr[c + j] : 0.f;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const long long q = q0 + u * blockDim.x;
+                if (q >= cq) break;
+                const long long c = q * 4;
+                __nv_bfloat16 o[4][3];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) split_n(v[u][j], ns, o[j]);
+                for (int s = 0; s < ns; ++s) {
+                    __nv_bfloat16* dst = out.p[s] + blockIdx.y * o_bstride + r * ldo + c;
+                    if (c + 3 < ldo) {
+                        __align__(8) __nv_bfloat16 w[4] = {o[0][s], o[1][s], o[2][s], o[3][s]};
+                        *reinterpret_cast<uint2*>(dst) = *reinterpret_cast<const uint2*>(w);
+                    } else {
+                        for (int j = 0; j < 4 && c + j < ldo; ++j) dst[j] = o[j][s];
+                    }
+                }
             }
         }
     }

@@ -19,8 +19,12 @@ struct fg_ctx {
     int cc_major = 0, cc_minor = 0;
     size_t hbm_bytes = 0;
     cudaStream_t stream = nullptr;
+    // host-pointer calls: GEMMs and copy-out run on their own streams so the
+    // copies of one row panel overlap the GEMM of another
+    cudaStream_t pipe_comp = nullptr, pipe_out = nullptr;
     fg::DevStatus* d_status = nullptr;  // kernel error word (device)
     std::mutex mu;
+    std::mutex host_mu;  // one pipelined host-pointer call at a time
 };
 
 namespace fgrt {

@@ -318,3 +318,41 @@ def test_batched_strided_broadcast(fg):
     fg.gemm_batched_strided(np.int8, bsz, m, n, k, da, m * k, db, 0, dc, m * n)
     want = np.matmul(a.astype(np.int64), b.astype(np.int64)).astype(np.int32)
     np.testing.assert_array_equal(dc.to_numpy(), want)
+
+
+# --------------------------------------------------- pipelined host path
+def test_host_path_row_panels_i8_exact(fg):
+    # 90 MB of operands + result: the host-pointer call streams 2 row panels
+    m, n, k = 6000, 3000, 2000
+    r = rng(21)
+    a = r.integers(-128, 128, (m, k), dtype=np.int8)
+    b = r.integers(-128, 128, (k, n), dtype=np.int8)
+    c = np.zeros((m, n), np.int32)
+    assert fg.gemm_i8_signed(m, n, k, a, b, c)
+    want = (a.astype(np.float64) @ b.astype(np.float64)).astype(np.int32)  # exact: |C| < 2^53
+    np.testing.assert_array_equal(c, want)
+    # accumulate reads C through the panels too
+    c0 = r.integers(-2 ** 20, 2 ** 20, (m, n), dtype=np.int32)
+    c = c0.copy()
+    assert fg.gemm_i8_signed(m, n, k, a, b, c, accumulate=True)
+    np.testing.assert_array_equal(c, want + c0)
+
+
+@pytest.mark.parametrize("mode", ["plain", "split"])
+def test_host_path_row_panels_f32_beta(fg, oracle, mode):
+    m, n, k = 5000, 3000, 1500
+    r = rng(22)
+    a = r.standard_normal((m, k), dtype=np.float32)
+    b = r.standard_normal((k, n), dtype=np.float32)
+    c0 = r.standard_normal((m, n), dtype=np.float32)
+    c = c0.copy()
+    assert fg.gemm_f32(m, n, k, 1.5, a, b, -0.5, c, mode=mode)
+    rows, cols = oracle.sample_indices(m, n, 64, 64, seed=3)
+    ref = 1.5 * oracle.dd_sampled(a, b, rows, cols) - 0.5 * c0[np.ix_(rows, cols)].astype(np.float64)
+    got = c[np.ix_(rows, cols)]
+    scale = np.linalg.norm(a.astype(np.float64)) * np.linalg.norm(b.astype(np.float64))
+    blow = np.sqrt(m * n / got.size)  # sampled block -> whole-matrix Frobenius norms
+    err = np.linalg.norm(got - ref) * blow / scale
+    # GEMM bound plus the rounding of the f32 output (|C| ~ |beta C0| here)
+    tol = (2.0 ** -15 if mode == "split" else 0.0) + (k + 4) * U32
+    assert err <= tol + 2 * U32 * np.linalg.norm(ref) * blow / scale

@@ -125,3 +125,32 @@ def test_default_table_choices_are_valid_on_device(fg):
     with fg.tune_forced("i8", 0, 1):
         assert fg.gemm_i8_signed(m, n, k, a, b, c2)
     np.testing.assert_array_equal(c1, c2)
+
+
+@pytest.mark.parametrize("m,n,k", [(70, 33, 300), (300, 520, 700), (513, 257, 1100)])
+@pytest.mark.parametrize("dt", [np.float64, np.complex128])
+def test_ozaki_groups_pair_kernel_bitwise_equal(fg, oracle, m, n, k, dt):
+    """The Ozaki slice groups are exact int32 GEMMs with the same FP64
+    epilogue in the same group order on either kernel, so the single-CTA and
+    the CTA-pair group kernels must give bit-identical results."""
+    r = rng(m + k)
+    a = r.standard_normal((m, k))
+    b = r.standard_normal((k, n))
+    c0 = r.standard_normal((m, n))
+    if dt == np.complex128:
+        a = a + 1j * r.standard_normal((m, k))
+        b = b + 1j * r.standard_normal((k, n))
+        c0 = c0 + 1j * r.standard_normal((m, n))
+    outs = []
+    for v in (0, 2):
+        with fg.tune_forced("i8", v, 1):
+            c = c0.copy()
+            if dt == np.float64:
+                assert fg.gemm_f64(m, n, k, 0.75, a, b, 0.5, c, mode="split")
+            else:
+                assert fg.gemm_c64(m, n, k, 0.75, 0.0, a, b, 0.5, 0.0, c, mode="split")
+            outs.append(c)
+    np.testing.assert_array_equal(outs[0], outs[1])
+    ref = 0.75 * oracle.dd_full(a, b) + 0.5 * c0
+    scale = np.linalg.norm(a) * np.linalg.norm(b)
+    assert np.linalg.norm(outs[1] - ref) / scale <= 4 * k * U64
