@@ -195,15 +195,21 @@ __device__ __forceinline__ void epilogue_store(const TcArgs& p, int bz, int grow
         }
         const bool vec = ncols == 32 && (reinterpret_cast<uintptr_t>(crow) & 15) == 0;
         if (vec) {
+            if (p.accumulate) {
+                // all loads before the first store: they overlap instead of
+                // waiting behind stores that might alias them
+                uint4 o[8];
 #pragma unroll
-            for (int j = 0; j < 32; j += 4) {
-                uint4 w = make_uint4(out[j], out[j + 1], out[j + 2], out[j + 3]);
-                if (p.accumulate) {
-                    uint4 o = *reinterpret_cast<const uint4*>(crow + j);
-                    w.x += o.x; w.y += o.y; w.z += o.z; w.w += o.w;
+                for (int q = 0; q < 8; ++q) o[q] = *reinterpret_cast<const uint4*>(crow + 4 * q);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    out[4 * q] += o[q].x; out[4 * q + 1] += o[q].y;
+                    out[4 * q + 2] += o[q].z; out[4 * q + 3] += o[q].w;
                 }
-                *reinterpret_cast<uint4*>(crow + j) = w;
             }
+#pragma unroll
+            for (int j = 0; j < 32; j += 4)
+                *reinterpret_cast<uint4*>(crow + j) = make_uint4(out[j], out[j + 1], out[j + 2], out[j + 3]);
         } else {
             // fully unrolled with a predicate: a runtime trip count would
             // index `out` dynamically and move it to local memory
@@ -221,35 +227,90 @@ __device__ __forceinline__ void epilogue_store(const TcArgs& p, int bz, int grow
         const uint32_t rs = static_cast<uint32_t>(p.row_sum[grow]);
         const uint32_t azp = static_cast<uint32_t>(p.a_zp), bzp = static_cast<uint32_t>(p.b_zp);
         const uint32_t kab = static_cast<uint32_t>(p.K) * azp * bzp;
+        // every load of the chunk is issued before the first store (stores
+        // to C could alias the sums, which would serialise load -> store)
+        uint32_t cs[32];
+        float old[32];
 #pragma unroll
         for (int j = 0; j < 32; ++j) {
-            if (j >= ncols) break;
-            uint32_t cs = static_cast<uint32_t>(p.col_sum[gcol0 + j]);
-            uint32_t corr = v[0][j] - azp * cs - bzp * rs + kab;
-            // Separate roundings, as gemm/mod.rs:566-571 computes them (no FMA).
-            float o = __fmul_rn(p.scale, static_cast<float>(static_cast<int32_t>(corr)));
-            if (p.accumulate) o = __fadd_rn(crow[j], o);
-            crow[j] = o;
+            cs[j] = j < ncols ? static_cast<uint32_t>(p.col_sum[gcol0 + j]) : 0u;
+            old[j] = (p.accumulate && j < ncols) ? crow[j] : 0.f;
+        }
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            if (j < ncols) {
+                const uint32_t corr = v[0][j] - azp * cs[j] - bzp * rs + kab;
+                // Separate roundings, as gemm/mod.rs:566-571 computes them (no FMA).
+                float o = __fmul_rn(p.scale, static_cast<float>(static_cast<int32_t>(corr)));
+                if (p.accumulate) o = __fadd_rn(old[j], o);
+                crow[j] = o;
+            }
         }
     } else if constexpr (Cfg::EPI == EPI_OZAKI) {
         double* cbase = static_cast<double*>(p.C) + bz * p.strideC;
         const double rs = p.row_scale[grow] * p.oz_w;
         const int h = p.cplx_half;
+        const bool need_old = !p.oz_first || p.oz_beta != 0.0;
+        double* crow = cbase + (long long)grow * p.ldc;
+        const bool vec = h == 0 && ncols == 32 && ((reinterpret_cast<uintptr_t>(crow + gcol0) & 15) == 0);
+        // Two halves of 16 columns; in each, all loads (scales, old C) are
+        // issued before the stores so they overlap instead of serialising.
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-            if (j >= ncols) break;
-            const int col = gcol0 + j;
-            const int cc = (h > 0 && col >= h) ? col - h : col;
-            double* dst = h > 0 ? cbase + (long long)grow * p.ldc + 2 * cc + (col < h ? 0 : 1)
-                                : cbase + (long long)grow * p.ldc + col;
-            // exact int32 -> f64, then power-of-two scalings (exact) and alpha
-            double v = static_cast<double>(static_cast<int32_t>(v_[0][j])) * p.col_scale[cc] * rs;
-            if (p.oz_first) {
-                if (p.oz_beta != 0.0) v = fma(p.oz_beta, *dst, v);
-            } else {
-                v = *dst + v;
+        for (int half = 0; half < 2; ++half) {
+            const int j0 = half * 16;
+            double cs[16], old[16];
+#pragma unroll
+            for (int u = 0; u < 16; ++u) {
+                const int j = j0 + u;
+                const int col = gcol0 + j;
+                const int cc = (h > 0 && col >= h) ? col - h : col;
+                cs[u] = j < ncols ? p.col_scale[cc] : 0.0;
             }
-            *dst = v;
+            if (vec) {
+                if (need_old) {
+#pragma unroll
+                    for (int u = 0; u < 16; u += 2) {
+                        const double2 w = *reinterpret_cast<const double2*>(crow + gcol0 + j0 + u);
+                        old[u] = w.x;
+                        old[u + 1] = w.y;
+                    }
+                } else {
+#pragma unroll
+                    for (int u = 0; u < 16; ++u) old[u] = 0.0;
+                }
+            } else {
+#pragma unroll
+                for (int u = 0; u < 16; ++u) {
+                    const int j = j0 + u;
+                    const int col = gcol0 + j;
+                    const int cc = (h > 0 && col >= h) ? col - h : col;
+                    const double* src = h > 0 ? crow + 2 * cc + (col < h ? 0 : 1) : crow + col;
+                    old[u] = (need_old && j < ncols) ? *src : 0.0;
+                }
+            }
+            double out[16];
+#pragma unroll
+            for (int u = 0; u < 16; ++u) {
+                // exact int32 -> f64, then power-of-two scalings (exact) and alpha
+                const double t = static_cast<double>(static_cast<int32_t>(v_[0][j0 + u])) * cs[u] * rs;
+                out[u] = p.oz_first ? (p.oz_beta != 0.0 ? fma(p.oz_beta, old[u], t) : t) : old[u] + t;
+            }
+            if (vec) {
+#pragma unroll
+                for (int u = 0; u < 16; u += 2)
+                    *reinterpret_cast<double2*>(crow + gcol0 + j0 + u) = make_double2(out[u], out[u + 1]);
+            } else {
+#pragma unroll
+                for (int u = 0; u < 16; ++u) {
+                    const int j = j0 + u;
+                    if (j < ncols) {
+                        const int col = gcol0 + j;
+                        const int cc = (h > 0 && col >= h) ? col - h : col;
+                        double* dst = h > 0 ? crow + 2 * cc + (col < h ? 0 : 1) : crow + col;
+                        *dst = out[u];
+                    }
+                }
+            }
         }
     } else {  // EPI_F32
         float* cbase = static_cast<float*>(p.C) + bz * p.strideC;
@@ -257,15 +318,23 @@ __device__ __forceinline__ void epilogue_store(const TcArgs& p, int bz, int grow
             // Column j of the real-embedded product is Re (j < h) or Im (j >= h)
             // of complex column j mod h; C is interleaved (re, im).
             const int h = p.cplx_half;
+            float* crow = cbase + (long long)grow * p.ldc;
+            float old[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {  // loads first, then stores
+                const int col = gcol0 + j;
+                const int cc = col < h ? col : col - h;
+                old[j] = (p.beta != 0.f && j < ncols) ? crow[2 * cc + (col < h ? 0 : 1)] : 0.f;
+            }
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
-                if (j >= ncols) break;
-                int col = gcol0 + j;
-                int cc = col < h ? col : col - h;
-                float* dst = cbase + (long long)grow * p.ldc + 2 * cc + (col < h ? 0 : 1);
-                float o = p.alpha * __uint_as_float(v[0][j]);
-                if (p.beta != 0.f) o = fmaf(p.beta, *dst, o);
-                *dst = o;
+                if (j < ncols) {
+                    const int col = gcol0 + j;
+                    const int cc = col < h ? col : col - h;
+                    float o = p.alpha * __uint_as_float(v[0][j]);
+                    if (p.beta != 0.f) o = fmaf(p.beta, old[j], o);
+                    crow[2 * cc + (col < h ? 0 : 1)] = o;
+                }
             }
             return;
         }
@@ -275,16 +344,21 @@ __device__ __forceinline__ void epilogue_store(const TcArgs& p, int bz, int grow
         for (int j = 0; j < 32; ++j) out[j] = p.alpha * __uint_as_float(v[0][j]);
         const bool vec = ncols == 32 && (reinterpret_cast<uintptr_t>(crow) & 15) == 0;
         if (vec) {
+            if (p.beta != 0.f) {
+                float4 o[8];
 #pragma unroll
-            for (int j = 0; j < 32; j += 4) {
-                float4 w = make_float4(out[j], out[j + 1], out[j + 2], out[j + 3]);
-                if (p.beta != 0.f) {
-                    float4 o = *reinterpret_cast<const float4*>(crow + j);
-                    w.x = fmaf(p.beta, o.x, w.x); w.y = fmaf(p.beta, o.y, w.y);
-                    w.z = fmaf(p.beta, o.z, w.z); w.w = fmaf(p.beta, o.w, w.w);
+                for (int q = 0; q < 8; ++q) o[q] = *reinterpret_cast<const float4*>(crow + 4 * q);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    out[4 * q] = fmaf(p.beta, o[q].x, out[4 * q]);
+                    out[4 * q + 1] = fmaf(p.beta, o[q].y, out[4 * q + 1]);
+                    out[4 * q + 2] = fmaf(p.beta, o[q].z, out[4 * q + 2]);
+                    out[4 * q + 3] = fmaf(p.beta, o[q].w, out[4 * q + 3]);
                 }
-                *reinterpret_cast<float4*>(crow + j) = w;
             }
+#pragma unroll
+            for (int j = 0; j < 32; j += 4)
+                *reinterpret_cast<float4*>(crow + j) = make_float4(out[j], out[j + 1], out[j + 2], out[j + 3]);
         } else {
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
