@@ -300,6 +300,38 @@ def side_measurements(fg, L, lib, ctx, stream, n, only=""):
             del bufs
         res["ragged_4096"] = {"gflop": round(gflop, 2), **g}
         torch.cuda.empty_cache()
+    if only == "skinny":
+        # --- skinny shapes on the HBM roof: algorithmic bytes / device time
+        _, hbm, _ = peaks()
+        sk = {}
+        for (name, dt, mode, m, nn, k) in (("i8_m32", L.FG_I8, 0, 32, n, n), ("i8_n32", L.FG_I8, 0, n, 32, n),
+                                           ("f64_m32", L.FG_F64, 0, 32, n, n), ("f32_m32", L.FG_F32, 0, 32, n, n),
+                                           ("f32_split_m32", L.FG_F32, 1, 32, n, n),
+                                           ("f64_gemv", L.FG_F64, 0, n, 1, n)):
+            es = {L.FG_I8: 1, L.FG_F32: 4, L.FG_F64: 8}[dt]
+            eo = 4 if dt == L.FG_I8 else es
+            ta = torch.zeros(m * k * es, dtype=torch.int8, device="cuda")
+            tb = torch.zeros(k * nn * es, dtype=torch.int8, device="cuda")
+            if dt == L.FG_I8:
+                ta.random_(-128, 127)
+                tb.random_(-128, 127)
+            else:
+                fdt = torch.float32 if dt == L.FG_F32 else torch.float64
+                ta = torch.randn(m * k, dtype=fdt, device="cuda")
+                tb = torch.randn(k * nn, dtype=fdt, device="cuda")
+            tc = torch.zeros(m * nn * eo, dtype=torch.int8, device="cuda")
+            st_t = C.c_double if dt == L.FG_F64 else C.c_float
+            al, be = (st_t * 1)(1.0), (st_t * 1)(0.0)
+            ms = _time_calls(torch, stream, lambda: lib.fg_gemm(ctx.handle, dt, mode, 0, m, nn, k, al, ta.data_ptr(), k,
+                                                                 tb.data_ptr(), nn, be, tc.data_ptr(), nn, 0, sh), 10, 3)
+            byts = (m * k + k * nn) * es + m * nn * eo
+            v, spl = fg.tune_lookup({L.FG_I8: "i8", L.FG_F64: "f64"}.get(dt, "split_f32" if mode else "f32"), m, nn, k)
+            sk[name] = {"m": m, "n": nn, "k": k, "ms": round(ms, 4), "alg_bytes": byts,
+                        "gbs": round(byts / ms / 1e6, 1), "frac_of_measured_hbm": round(byts / ms / 1e6 / hbm, 3),
+                        "variant": v, "splits": spl}
+            del ta, tb, tc
+        res["skinny_%d" % n] = sk
+        torch.cuda.empty_cache()
     if not only or only == "serving":
         # --- served stream, one rate
         res["serving_10k_req_s"] = bench_serving.sweep(fg, L, lib, ctx, [10000.0], 1500)[0]

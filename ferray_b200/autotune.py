@@ -2,7 +2,7 @@
 
 Every tuned family ("op") has kernel variants (tile shape / pipeline depth)
 and a split-K count.  For each bucket triple of (M, N, K) -- buckets
-<=128, <=256, ..., <=4096, >4096 -- the tuner times every candidate on the
+<=16, <=32, ..., <=4096, >4096 -- the tuner times every candidate on the
 bucket's representative shape (its upper bound; 8192 for the last bucket)
 and keeps the fastest one whose result agrees with the untuned kernel
 (integers bit-exact, floats to a normwise 1e-5 / 1e-13).
@@ -31,13 +31,14 @@ import time
 import numpy as np
 
 OPS = ["i8", "split_f32", "f64", "f32"]
-BUCKETS = 7
-REPR = [128, 256, 512, 1024, 2048, 4096, 8192]
+BUCKETS = 10
+REPR = [16, 32, 64, 128, 256, 512, 1024, 2048, 4096, 8192]
 SPLITS = [1, 2, 4, 8, 16]
 MARGIN = 1.03  # a candidate must beat the untuned kernel by 3%
 # tile edge per variant (output tiles per block row / column)
 TILES = {"i8": [(128, 256), (128, 128), (256, 256)], "split_f32": [(128, 128), (128, 64), (256, 128)],
-         "f64": [(128, 128), (64, 64)], "f32": [(128, 128), (64, 64)]}
+         "f64": [(128, 128), (64, 64), (32, 128), (128, 32)],
+         "f32": [(128, 128), (64, 64), (32, 128), (128, 32)]}
 # K per split unit: one tcgen05 K block, or the SIMT split granularity
 KUNIT = {"i8": 128, "split_f32": 64, "f64": 64, "f32": 64}
 
@@ -47,8 +48,8 @@ def write_inc(choice, path, meta):
     lines = ["// tune_table.inc -- generated by ferray_b200/autotune.py; do not edit.",
              "// " + meta,
              "// kTuneTable[op][M bucket][N bucket][K bucket] = {variant, splits};",
-             "// ops: " + ", ".join(OPS) + "; buckets <=128, <=256, <=512, <=1024, <=2048,"
-             " <=4096, >4096.",
+             "// ops: " + ", ".join(OPS) + "; buckets <=16, <=32, <=64, <=128, <=256, <=512,"
+             " <=1024, <=2048, <=4096, >4096.",
              "constexpr TuneEntry kTuneTable[TUNE_OPS][TUNE_BUCKETS][TUNE_BUCKETS][TUNE_BUCKETS] = {"]
     for op in OPS:
         lines.append("    {  // " + op)

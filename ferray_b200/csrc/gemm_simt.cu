@@ -30,20 +30,20 @@ static int grid_for(long long total) {
 // Plain real GEMM with the tuned tile variant and split-K count.  Split-K
 // writes `splits` partial products into a workspace and a combine pass
 // applies alpha / beta (the partial sums are added in split order).
-template <typename T, int TM>
+template <typename T, int TMM, int TNN>
 static fg_status launch_simt_real(const Gemm& g, BatchMap bm, int splits_want, cudaStream_t st) {
-    constexpr int BT = 16 * TM;
+    constexpr int BTM = 16 * TMM, BTN = 16 * TNN;
     constexpr long long KUNIT = 64;  // split granularity in K
     const long long kunits = (g.K + KUNIT - 1) / KUNIT;
     int kps = static_cast<int>(kunits);
     const int splits = plan_splits(splits_want, static_cast<int>(kunits), g.M * g.N * g.batch,
                                    sizeof(T), &kps);
     if ((long long)splits * g.batch > 65535) return set_error(FG_ERR_UNSUPPORTED, "batch above 65535");
-    dim3 grid((g.N + BT - 1) / BT, (g.M + BT - 1) / BT, g.batch * splits);
+    dim3 grid((g.N + BTN - 1) / BTN, (g.M + BTM - 1) / BTM, g.batch * splits);
     const T* A = static_cast<const T*>(g.A);
     const T* B = static_cast<const T*>(g.B);
     if (splits <= 1) {
-        simt_gemm_real<T, 8, TM><<<grid, 256, 0, st>>>((int)g.M, (int)g.N, (int)g.K, (T)g.alpha_re, A,
+        simt_gemm_real<T, 8, TMM, TNN><<<grid, 256, 0, st>>>((int)g.M, (int)g.N, (int)g.K, (T)g.alpha_re, A,
                                                        g.lda, B, g.ldb, (T)g.beta_re,
                                                        static_cast<T*>(g.C), g.ldc, bm, g.batch, (int)g.K);
         count_launch();
@@ -55,7 +55,7 @@ static fg_status launch_simt_real(const Gemm& g, BatchMap bm, int splits_want, c
     FG_TRY(ws.alloc(static_cast<size_t>(splits * out_elems) * sizeof(T), st));
     BatchMap wbm = bm;
     wbm.c_bstride = g.M * g.N;
-    simt_gemm_real<T, 8, TM><<<grid, 256, 0, st>>>((int)g.M, (int)g.N, (int)g.K, T(1), A, g.lda, B,
+    simt_gemm_real<T, 8, TMM, TNN><<<grid, 256, 0, st>>>((int)g.M, (int)g.N, (int)g.K, T(1), A, g.lda, B,
                                                    g.ldb, T(0), static_cast<T*>(ws.p), g.N, wbm,
                                                    g.batch, (int)(kps * KUNIT));
     splitk_reduce_kernel<T><<<grid_for(out_elems), 256, 0, st>>>(
@@ -66,8 +66,53 @@ static fg_status launch_simt_real(const Gemm& g, BatchMap bm, int splits_want, c
     return FG_OK;
 }
 
+// Matrix-vector shapes (one operand is a vector; ferray's matmul of a 1-D
+// operand, products/mod.rs:362-437) go to the GEMV kernels.
+template <typename T>
+static fg_status launch_gemv(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
+    const T* A = static_cast<const T*>(g.A);
+    const T* B = static_cast<const T*>(g.B);
+    T* C = static_cast<T*>(g.C);
+    if (g.N == 1) {
+        const long long blocks = (g.M * 32 + 255) / 256;
+        gemv_rows_kernel<T><<<static_cast<unsigned>(blocks), 256, 0, st>>>(
+            (int)g.M, (int)g.K, (T)g.alpha_re, A, g.lda, B, g.ldb, (T)g.beta_re, C, g.ldc);
+        count_launch();
+        FG_CUDA(cudaGetLastError());
+        return FG_OK;
+    }
+    constexpr int CW = 32 * (16 / sizeof(T));
+    const long long cblocks = (g.N + CW - 1) / CW;
+    // split K across blocks until there are about 4 blocks per SM
+    int splits = static_cast<int>(std::min<long long>(
+        std::max<long long>(1, (4LL * ctx->sm_count) / cblocks), std::max<long long>(1, g.K / 256)));
+    splits = std::min(splits, 64);
+    const int ksplit = static_cast<int>((g.K + splits - 1) / splits);
+    splits = static_cast<int>((g.K + ksplit - 1) / ksplit);
+    dim3 grid(static_cast<unsigned>(cblocks), static_cast<unsigned>(splits));
+    if (splits == 1) {
+        gemv_cols_kernel<T><<<grid, 256, 0, st>>>((int)g.N, (int)g.K, ksplit, (T)g.alpha_re, A, 1, B,
+                                                  g.ldb, (T)g.beta_re, C, 0);
+        count_launch();
+        FG_CUDA(cudaGetLastError());
+        return FG_OK;
+    }
+    Scratch ws;
+    FG_TRY(ws.alloc(static_cast<size_t>(splits * g.N) * sizeof(T), st));
+    gemv_cols_kernel<T><<<grid, 256, 0, st>>>((int)g.N, (int)g.K, ksplit, (T)g.alpha_re, A, 1, B, g.ldb,
+                                              (T)g.beta_re, static_cast<T*>(ws.p), g.N);
+    splitk_reduce_kernel<T><<<grid_for(g.N), 256, 0, st>>>(static_cast<const T*>(ws.p), splits, 1, g.N, 1,
+                                                           C, g.ldc, 0, (T)g.alpha_re, (T)g.beta_re, 0);
+    count_launch(2);
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
 fg_status launch_simt(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
-    (void)ctx;
+    if (g.batch == 1 && (g.N == 1 || g.M == 1) && (g.dtype == FG_F64 || g.dtype == FG_F32)) {
+        ProfScope prof(g.dtype == FG_F64 ? "gemv_f64" : "gemv_f32", st);
+        return g.dtype == FG_F64 ? launch_gemv<double>(ctx, g, st) : launch_gemv<float>(ctx, g, st);
+    }
     const BatchMap bm = batch_map(g);
     if (g.batch > 65535) return set_error(FG_ERR_UNSUPPORTED, "batch above 65535");
     static const char* names[] = {"simt_dgemm", "simt_sgemm", "simt_zgemm", "simt_cgemm"};
@@ -75,13 +120,21 @@ fg_status launch_simt(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
     switch (g.dtype) {
         case FG_F64: {
             const TuneChoice c = tune_lookup(TUNE_F64, g.M, g.N, g.K);
-            return c.variant == 1 ? launch_simt_real<double, 4>(g, bm, c.splits, st)
-                                  : launch_simt_real<double, 8>(g, bm, c.splits, st);
+            switch (c.variant) {
+                case 1: return launch_simt_real<double, 4, 4>(g, bm, c.splits, st);
+                case 2: return launch_simt_real<double, 2, 8>(g, bm, c.splits, st);
+                case 3: return launch_simt_real<double, 8, 2>(g, bm, c.splits, st);
+                default: return launch_simt_real<double, 8, 8>(g, bm, c.splits, st);
+            }
         }
         case FG_F32: {
             const TuneChoice c = tune_lookup(TUNE_F32, g.M, g.N, g.K);
-            return c.variant == 1 ? launch_simt_real<float, 4>(g, bm, c.splits, st)
-                                  : launch_simt_real<float, 8>(g, bm, c.splits, st);
+            switch (c.variant) {
+                case 1: return launch_simt_real<float, 4, 4>(g, bm, c.splits, st);
+                case 2: return launch_simt_real<float, 2, 8>(g, bm, c.splits, st);
+                case 3: return launch_simt_real<float, 8, 2>(g, bm, c.splits, st);
+                default: return launch_simt_real<float, 8, 8>(g, bm, c.splits, st);
+            }
         }
         case FG_C64: {
             dim3 grid((g.N + 63) / 64, (g.M + 63) / 64, g.batch);

@@ -45,18 +45,23 @@ __device__ __forceinline__ void batch_offsets(const BatchMap& bm, int bz, long l
 }
 
 // ----------------------------------------------------------------- real
-// Tile BM = BN = 16 * TM (TM = 8: 128 x 128, TM = 4: 64 x 64 for small
-// problems).  Split-K: blockIdx.z = split * nbatch + batch index; split s
+// Tile BM = 16 * TMM rows x BN = 16 * TNN columns on a 16 x 16 thread grid,
+// TMM x TNN outputs per thread: 128 x 128 (8 x 8), 64 x 64 (4 x 4), and the
+// skinny 32 x 128 (2 x 8) / 128 x 32 (8 x 2) for small M / small N.  Split-K: blockIdx.z = split * nbatch + batch index; split s
 // covers K columns [s * ksplit, (s + 1) * ksplit) and writes output matrix
 // blockIdx.z (the host points C at a partial-sum workspace then).
-// Two resident blocks per SM for the f32 128 x 128 tile (at most 128
-// registers a thread); the f64 one needs more registers than that.
-template <typename T, int BK, int TM>
-__global__ void __launch_bounds__(256, (sizeof(T) == 4 && TM == 8) ? 2 : 1)
+// Two resident blocks per SM except for the f64 128 x 128 tile, which needs
+// more than 128 registers a thread.
+template <typename T, int BK, int TMM, int TNN>
+__global__ void __launch_bounds__(256, (sizeof(T) == 8 && TMM == 8 && TNN == 8) ? 1 : 2)
     simt_gemm_real(int M, int N, int K, T alpha, const T* __restrict__ A, long long lda,
                    const T* __restrict__ B, long long ldb, T beta, T* __restrict__ C,
                    long long ldc, BatchMap bm, int nbatch, int ksplit) {
-    constexpr int BM = 16 * TM, BN = 16 * TM, PAD = 4, H = TM / 2;
+    constexpr int BM = 16 * TMM, BN = 16 * TNN, PAD = 4, H = TMM / 2;
+    // Columns of a thread: QN groups of GN contiguous elements (16 bytes),
+    // group q at q * 16 * GN + tx * GN, so each 16-byte fragment load of a
+    // half-warp reads 256 contiguous bytes (no bank conflicts for f64).
+    constexpr int GN = 16 / sizeof(T) < TNN ? 16 / sizeof(T) : TNN, QN = TNN / GN;
     constexpr int A_PER = BM * BK / 256;  // A elements each thread loads per K block
     constexpr int B_PER = BK * BN / 256;
     __shared__ __align__(16) T As[2][BK][BM + PAD];
@@ -104,11 +109,11 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && TM == 8) ? 2 : 1)
         for (int j = 0; j < B_PER; ++j) Bs[buf][b_r][b_c + j] = rb[j];
     };
 
-    T acc[TM][TM];
+    T acc[TMM][TNN];
 #pragma unroll
-    for (int i = 0; i < TM; ++i)
+    for (int i = 0; i < TMM; ++i)
 #pragma unroll
-        for (int j = 0; j < TM; ++j) acc[i][j] = T(0);
+        for (int j = 0; j < TNN; ++j) acc[i][j] = T(0);
 
     const int kblocks = (K + BK - 1) / BK;
     load_global(0);
@@ -119,35 +124,152 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && TM == 8) ? 2 : 1)
         if (kb + 1 < kblocks) load_global((kb + 1) * BK);
 #pragma unroll
         for (int kk = 0; kk < BK; ++kk) {
-            T af[TM], bf[TM];
+            T af[TMM], bf[TNN];
 #pragma unroll
             for (int i = 0; i < H; ++i) {
                 af[i] = As[cur][kk][ty * H + i];
                 af[H + i] = As[cur][kk][BM / 2 + ty * H + i];
-                bf[i] = Bs[cur][kk][tx * H + i];
-                bf[H + i] = Bs[cur][kk][BN / 2 + tx * H + i];
             }
 #pragma unroll
-            for (int i = 0; i < TM; ++i)
+            for (int q = 0; q < QN; ++q)
 #pragma unroll
-                for (int j = 0; j < TM; ++j) acc[i][j] = fma(af[i], bf[j], acc[i][j]);
+                for (int g = 0; g < GN; ++g) bf[q * GN + g] = Bs[cur][kk][q * 16 * GN + tx * GN + g];
+#pragma unroll
+            for (int i = 0; i < TMM; ++i)
+#pragma unroll
+                for (int j = 0; j < TNN; ++j) acc[i][j] = fma(af[i], bf[j], acc[i][j]);
         }
         if (kb + 1 < kblocks) store_shared(cur ^ 1);
         __syncthreads();
     }
 
 #pragma unroll
-    for (int i = 0; i < TM; ++i) {
+    for (int i = 0; i < TMM; ++i) {
         const int r = m0 + (i < H ? ty * H + i : BM / 2 + ty * H + (i - H));
         if (r >= M) continue;
 #pragma unroll
-        for (int j = 0; j < TM; ++j) {
-            const int c = n0 + (j < H ? tx * H + j : BN / 2 + tx * H + (j - H));
+        for (int j = 0; j < TNN; ++j) {
+            const int c = n0 + (j / GN) * 16 * GN + tx * GN + (j % GN);
             if (c >= N) continue;
             T* p = C + (long long)r * ldc + c;
             T v = alpha * acc[i][j];
             if (beta != T(0)) v = fma(beta, *p, v);
             *p = v;
+        }
+    }
+}
+
+// ----------------------------------------------------------------- GEMV
+// Matrix-vector forms of the plain real GEMM (HBM-bound: the matrix is read
+// once).  matvec: N == 1, y = C[:, 0] = alpha * A x + beta * y with x = B[:, 0]
+// (stride ldb); one warp per row, lanes stride over K with 16-byte loads when
+// the row and x are contiguous and aligned, partial sums combined by a fixed
+// butterfly.  vecmat: M == 1, y = C[0, :] = alpha * x B + beta * y with
+// x = A[0, :]; a block owns 32 x G columns (16-byte loads along N), its 8
+// warps take interleaved K rows and are summed in shared memory in warp
+// order; blockIdx.y splits K (partials to a workspace, combined by
+// splitk_reduce_kernel) when the columns alone do not fill the GPU.
+template <typename T>
+__global__ void __launch_bounds__(256)
+    gemv_rows_kernel(int M, int K, T alpha, const T* __restrict__ A, long long lda,
+                     const T* __restrict__ x, long long incx, T beta, T* __restrict__ y,
+                     long long incy) {
+    constexpr int G = 16 / sizeof(T);
+    const int lane = threadIdx.x % 32;
+    const long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32;
+    if (row >= M) return;
+    const T* a = A + row * lda;
+    const bool vec = incx == 1 && (reinterpret_cast<uintptr_t>(a) % 16 == 0) &&
+                     (reinterpret_cast<uintptr_t>(x) % 16 == 0);
+    T acc[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) acc[g] = T(0);
+    int k0 = 0;
+    if (vec) {
+        const int kv = K / G * G;
+        for (int k = lane * G; k < kv; k += 32 * G) {
+            T av[G], xv[G];
+            if constexpr (sizeof(T) == 8) {
+                const double2 p = *reinterpret_cast<const double2*>(a + k);
+                const double2 q = *reinterpret_cast<const double2*>(x + k);
+                av[0] = p.x; av[1] = p.y; xv[0] = q.x; xv[1] = q.y;
+            } else {
+                const float4 p = *reinterpret_cast<const float4*>(a + k);
+                const float4 q = *reinterpret_cast<const float4*>(x + k);
+                av[0] = p.x; av[1] = p.y; av[2] = p.z; av[3] = p.w;
+                xv[0] = q.x; xv[1] = q.y; xv[2] = q.z; xv[3] = q.w;
+            }
+#pragma unroll
+            for (int g = 0; g < G; ++g) acc[g] = fma(av[g], xv[g], acc[g]);
+        }
+        k0 = kv;
+    }
+    for (int k = k0 + lane; k < K; k += 32) acc[0] = fma(a[k], x[k * incx], acc[0]);
+    T sum = acc[0];
+#pragma unroll
+    for (int g = 1; g < G; ++g) sum += acc[g];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xFFFFFFFFu, sum, o);
+    if (lane == 0) {
+        T* dst = y + row * incy;
+        T v = alpha * sum;
+        if (beta != T(0)) v = fma(beta, *dst, v);
+        *dst = v;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+    gemv_cols_kernel(int N, int K, int ksplit, T alpha, const T* __restrict__ x, long long incx,
+                     const T* __restrict__ B, long long ldb, T beta, T* __restrict__ y,
+                     long long split_stride) {
+    constexpr int G = 16 / sizeof(T);
+    __shared__ T part[8][32 * G];
+    const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+    const int c0 = blockIdx.x * 32 * G + lane * G;
+    const int kb = blockIdx.y * ksplit, ke = min(K, kb + ksplit);
+    const bool vec = c0 + G <= N && (ldb % G == 0) && (reinterpret_cast<uintptr_t>(B) % 16 == 0);
+    T acc[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) acc[g] = T(0);
+    for (int k = kb + warp; k < ke; k += 8) {
+        const T xv = x[k * incx];
+        const T* br = B + (long long)k * ldb + c0;
+        if (vec) {
+            if constexpr (sizeof(T) == 8) {
+                const double2 p = *reinterpret_cast<const double2*>(br);
+                acc[0] = fma(xv, p.x, acc[0]);
+                acc[1] = fma(xv, p.y, acc[1]);
+            } else {
+                const float4 p = *reinterpret_cast<const float4*>(br);
+                acc[0] = fma(xv, p.x, acc[0]); acc[1] = fma(xv, p.y, acc[1]);
+                acc[2] = fma(xv, p.z, acc[2]); acc[3] = fma(xv, p.w, acc[3]);
+            }
+        } else {
+#pragma unroll
+            for (int g = 0; g < G; ++g)
+                if (c0 + g < N) acc[g] = fma(xv, br[g], acc[g]);
+        }
+    }
+#pragma unroll
+    for (int g = 0; g < G; ++g) part[warp][lane * G + g] = acc[g];
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            const int c = c0 + g;
+            T sum = part[0][lane * G + g];
+#pragma unroll
+            for (int w = 1; w < 8; ++w) sum += part[w][lane * G + g];
+            if (c < N) {
+                if (gridDim.y > 1) {
+                    y[blockIdx.y * split_stride + c] = sum;  // partial (alpha/beta in the combine)
+                } else {
+                    T v = alpha * sum;
+                    if (beta != T(0)) v = fma(beta, y[c], v);
+                    y[c] = v;
+                }
+            }
         }
     }
 }

@@ -18,8 +18,8 @@ enum TuneOp : int {
     TUNE_OPS = 4
 };
 
-// Bucket b covers (2^(b+6), 2^(b+7)]: <=128, <=256, ..., <=4096, >4096.
-constexpr int TUNE_BUCKETS = 7;
+// Bucket b covers (2^(b+3), 2^(b+4)]: <=16, <=32, ..., <=4096, >4096.
+constexpr int TUNE_BUCKETS = 10;
 constexpr int TUNE_MAX_SPLITS = 16;
 
 struct TuneChoice {

@@ -111,7 +111,7 @@ fg_status fg_selftest_wait_timeout(fg_ctx *ctx, uint32_t timeout_us, fg_stream s
 
 /* ------------------------------------------------------------ autotune */
 /* Tile variant and split-K count per GEMM family come from a table indexed
- * by the size buckets of m, n, k (<=128, <=256, ..., <=4096, >4096), written
+ * by the size buckets of m, n, k (<=16, <=32, ..., <=4096, >4096), written
  * by ferray_b200/autotune.py from timings on a B200 and compiled in.  The
  * reference's blocking is fixed constants (MC 64, KC 256, NC 512,
  * gemm/outer.rs:66-68); this table is what replaces them. */

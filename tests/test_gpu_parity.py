@@ -356,3 +356,36 @@ def test_host_path_row_panels_f32_beta(fg, oracle, mode):
     # GEMM bound plus the rounding of the f32 output (|C| ~ |beta C0| here)
     tol = (2.0 ** -15 if mode == "split" else 0.0) + (k + 4) * U32
     assert err <= tol + 2 * U32 * np.linalg.norm(ref) * blow / scale
+
+
+# ------------------------------------------------------------------ GEMV
+@pytest.mark.parametrize("dt,u", [(np.float64, U64), (np.float32, U32)])
+@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (300, 1, 1001), (8192, 1, 4096), (1, 300, 1001),
+                                   (1, 4097, 3000), (1, 200, 100000), (5, 1, 77)])
+def test_gemv_shapes(fg, oracle, dt, u, m, n, k):
+    r = rng(m + 3 * n + k)
+    a = r.uniform(-1, 1, (m, k)).astype(dt)
+    b = r.uniform(-1, 1, (k, n)).astype(dt)
+    c0 = r.uniform(-1, 1, (m, n)).astype(dt)
+    gemm = fg.gemm_f64 if dt == np.float64 else fg.gemm_f32
+    c = np.zeros((m, n), dt)
+    assert gemm(m, n, k, 1.0, a, b, 0.0, c)
+    exact = oracle.dd_full(a, b)
+    scale = np.linalg.norm(a.astype(np.float64)) * np.linalg.norm(b.astype(np.float64))
+    assert np.linalg.norm(c - exact) / scale <= k * u
+    c = c0.copy()
+    assert gemm(m, n, k, -0.5, a, b, 1.5, c)
+    ref = -0.5 * exact + 1.5 * c0.astype(np.float64)
+    assert np.linalg.norm(c - ref) <= (k + 4) * u * scale + 2 * u * np.linalg.norm(ref)
+
+
+def test_matmul_vector_operands_use_gemv(fg):
+    r = rng(8)
+    a = r.standard_normal((513, 700))
+    v = r.standard_normal(700)
+    w = r.standard_normal(513)
+    da, dv, dw = (fg.DeviceArray.from_numpy(x) for x in (a, v, w))
+    got = fg.matmul(da, dv).to_numpy()
+    np.testing.assert_allclose(got, a @ v, rtol=0, atol=700 * U64 * 30)
+    got = fg.matmul(dw, da).to_numpy()
+    np.testing.assert_allclose(got, w @ a, rtol=0, atol=513 * U64 * 30)

@@ -81,7 +81,7 @@ def test_split_f32_variants(fg, oracle, variant, splits, m, n, k):
 
 
 @pytest.mark.parametrize("op,dt,u", [("f64", np.float64, U64), ("f32", np.float32, U32)])
-@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
 @pytest.mark.parametrize("splits", SPLITS)
 @pytest.mark.parametrize("m,n,k", SHAPES)
 def test_plain_variants(fg, oracle, op, dt, u, variant, splits, m, n, k):
