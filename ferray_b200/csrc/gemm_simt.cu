@@ -3,9 +3,11 @@
 #include "prep_kernels.cuh"
 #include "runtime.h"
 #include "simt_gemm.cuh"
+#include "dmma_gemm.cuh"
 #include "tune.h"
 
 #include <algorithm>
+#include <mutex>
 
 namespace fgrt {
 
@@ -61,6 +63,49 @@ static fg_status launch_simt_real(const Gemm& g, BatchMap bm, int splits_want, c
     splitk_reduce_kernel<T><<<grid_for(out_elems), 256, 0, st>>>(
         static_cast<const T*>(ws.p), splits, g.M, g.N, g.batch, static_cast<T*>(g.C), g.ldc,
         g.c_stride, (T)g.alpha_re, (T)g.beta_re, 0);
+    count_launch(2);
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+// Plain DGEMM on the FP64 tensor path (DMMA), same split-K scheme.
+static fg_status launch_dmma(fg_ctx* ctx, const Gemm& g, BatchMap bm, int splits_want, cudaStream_t st) {
+    (void)ctx;
+    static std::once_flag once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(once, [] {
+        attr_err = cudaFuncSetAttribute(dmma_gemm_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(DmmaCfg::SMEM));
+    });
+    FG_CUDA(attr_err);
+    constexpr long long KUNIT = 64;
+    const long long kunits = (g.K + KUNIT - 1) / KUNIT;
+    int kps = static_cast<int>(kunits);
+    const int splits = plan_splits(splits_want, static_cast<int>(kunits), g.M * g.N * g.batch,
+                                   sizeof(double), &kps);
+    if ((long long)splits * g.batch > 65535) return set_error(FG_ERR_UNSUPPORTED, "batch above 65535");
+    dim3 grid((g.N + DmmaCfg::BN - 1) / DmmaCfg::BN, (g.M + DmmaCfg::BM - 1) / DmmaCfg::BM, g.batch * splits);
+    const double* A = static_cast<const double*>(g.A);
+    const double* B = static_cast<const double*>(g.B);
+    if (splits <= 1) {
+        dmma_gemm_f64_kernel<<<grid, DmmaCfg::THREADS, DmmaCfg::SMEM, st>>>(
+            (int)g.M, (int)g.N, (int)g.K, g.alpha_re, A, g.lda, B, g.ldb, g.beta_re,
+            static_cast<double*>(g.C), g.ldc, bm, g.batch, (int)g.K);
+        count_launch();
+        FG_CUDA(cudaGetLastError());
+        return FG_OK;
+    }
+    Scratch ws;
+    const long long out_elems = g.M * g.N * g.batch;
+    FG_TRY(ws.alloc(static_cast<size_t>(splits * out_elems) * sizeof(double), st));
+    BatchMap wbm = bm;
+    wbm.c_bstride = g.M * g.N;
+    dmma_gemm_f64_kernel<<<grid, DmmaCfg::THREADS, DmmaCfg::SMEM, st>>>(
+        (int)g.M, (int)g.N, (int)g.K, 1.0, A, g.lda, B, g.ldb, 0.0, static_cast<double*>(ws.p), g.N, wbm,
+        g.batch, (int)(kps * KUNIT));
+    splitk_reduce_kernel<double><<<grid_for(out_elems), 256, 0, st>>>(
+        static_cast<const double*>(ws.p), splits, g.M, g.N, g.batch, static_cast<double*>(g.C), g.ldc,
+        g.c_stride, g.alpha_re, g.beta_re, 0);
     count_launch(2);
     FG_CUDA(cudaGetLastError());
     return FG_OK;
@@ -124,6 +169,7 @@ fg_status launch_simt(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
                 case 1: return launch_simt_real<double, 4, 4>(g, bm, c.splits, st);
                 case 2: return launch_simt_real<double, 2, 8>(g, bm, c.splits, st);
                 case 3: return launch_simt_real<double, 8, 2>(g, bm, c.splits, st);
+                case 4: return launch_dmma(ctx, g, bm, c.splits, st);
                 default: return launch_simt_real<double, 8, 8>(g, bm, c.splits, st);
             }
         }
@@ -137,6 +183,27 @@ fg_status launch_simt(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
             }
         }
         case FG_C64: {
+            // Real scalars and one output matrix: the real-embedded GEMM on
+            // the DMMA kernel (same 8MNK flops, FP64 FMA per product).
+            if (g.batch == 1 && g.alpha_im == 0.0 && g.beta_im == 0.0 && g.K > 0 &&
+                (reinterpret_cast<uintptr_t>(g.B) & 15) == 0) {  // 16-byte complex loads of B
+                Scratch bx;
+                FG_TRY(bx.alloc(static_cast<size_t>(4 * g.K * g.N) * sizeof(double), st));
+                zgemm_expand_b_kernel<<<grid_for(g.K * g.N), 256, 0, st>>>(
+                    static_cast<const double2*>(g.B), g.K, g.N, g.ldb, static_cast<double*>(bx.p));
+                count_launch();
+                Gemm r = g;
+                r.dtype = FG_F64;
+                r.M = g.M;
+                r.N = 2 * g.N;
+                r.K = 2 * g.K;
+                r.lda = 2 * g.lda;
+                r.B = bx.p;
+                r.ldb = 2 * g.N;
+                r.ldc = 2 * g.ldc;
+                const TuneChoice c = tune_lookup(TUNE_F64, r.M, r.N, r.K);
+                return launch_dmma(ctx, r, batch_map(r), c.variant == 4 ? c.splits : 1, st);
+            }
             dim3 grid((g.N + 63) / 64, (g.M + 63) / 64, g.batch);
             simt_gemm_cplx<double, 8><<<grid, 256, 0, st>>>(
                 (int)g.M, (int)g.N, (int)g.K, g.alpha_re, g.alpha_im,

@@ -72,14 +72,14 @@ def test_tune_table_lookup_and_force_without_device():
     from ferray_b200 import _lib, autotune
     lib = _lib.load()
     n = C.c_int()
-    for op, want in zip(range(4), (3, 3, 4, 4)):
+    for op, want in zip(range(4), (3, 3, 5, 4)):
         assert lib.fg_tune_variants(op, C.byref(n)) == 0 and n.value == want
     assert lib.fg_tune_variants(9, C.byref(n)) == _lib.FG_ERR_INVALID
     # every shape maps to a valid choice
     for op in fg.TUNE_OPS:
         for m, nn, k in [(1, 1, 1), (128, 129, 8192), (5000, 70, 100000)]:
             v, s = fg.tune_lookup(op, m, nn, k)
-            assert 0 <= v < 4 and 1 <= s <= 16
+            assert 0 <= v < 5 and 1 <= s <= 16
     # forced choices win everywhere, then the table comes back
     before = fg.tune_lookup("i8", 300, 300, 5000)
     with fg.tune_forced("i8", 1, 8):
@@ -88,7 +88,8 @@ def test_tune_table_lookup_and_force_without_device():
     assert fg.tune_lookup("i8", 300, 300, 5000) == before
     assert lib.fg_tune_force(0, 3, 1) == _lib.FG_ERR_INVALID
     assert lib.fg_tune_force(1, 3, 1) == _lib.FG_ERR_INVALID
-    assert lib.fg_tune_force(2, 4, 1) == _lib.FG_ERR_INVALID
+    assert lib.fg_tune_force(2, 5, 1) == _lib.FG_ERR_INVALID
+    assert lib.fg_tune_force(3, 4, 1) == _lib.FG_ERR_INVALID
     assert lib.fg_tune_force(0, 0, 17) == _lib.FG_ERR_INVALID
     # the compiled-in table is the committed include: check one entry per op
     inc = open(os.path.join(ROOT, "ferray_b200", "csrc", "tune_table.inc")).read()

@@ -228,6 +228,18 @@ def test_c64_plain(fg, oracle, m, n, k):
     assert err <= 2 * ref_err + 2.0 ** -50, (err, ref_err)
 
 
+@pytest.mark.parametrize("m,n,k", [(33, 47, 59), (300, 260, 700)])
+def test_c64_real_scalars_dmma_path(fg, m, n, k):
+    # real alpha / beta: the real-embedded DMMA path (beta reads C)
+    r = rng(m)
+    a, b = _cplx(r, (m, k), np.complex128), _cplx(r, (k, n), np.complex128)
+    c0 = _cplx(r, (m, n), np.complex128)
+    c = c0.copy()
+    assert fg.gemm_c64(m, n, k, -0.75, 0.0, a, b, 1.5, 0.0, c)
+    want = -0.75 * (a @ b) + 1.5 * c0
+    assert np.max(np.abs(c - want)) < 4 * k * U64 * 10
+
+
 def test_c64_alpha_beta(fg):
     r = rng(4)
     m, n, k = 33, 47, 59

@@ -80,10 +80,10 @@ def test_split_f32_variants(fg, oracle, variant, splits, m, n, k):
                                            + 2 * U32 * np.linalg.norm(ref))
 
 
-@pytest.mark.parametrize("op,dt,u", [("f64", np.float64, U64), ("f32", np.float32, U32)])
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("op,dt,u,variant", [("f64", np.float64, U64, v) for v in range(5)] +
+                         [("f32", np.float32, U32, v) for v in range(4)])
 @pytest.mark.parametrize("splits", SPLITS)
-@pytest.mark.parametrize("m,n,k", SHAPES)
+@pytest.mark.parametrize("m,n,k", SHAPES + [(257, 300, 501)])
 def test_plain_variants(fg, oracle, op, dt, u, variant, splits, m, n, k):
     r = rng(m + 5 * n)
     a = r.uniform(-1, 1, (m, k)).astype(dt)
@@ -102,7 +102,7 @@ def test_plain_variants(fg, oracle, op, dt, u, variant, splits, m, n, k):
         assert np.linalg.norm(c - ref) <= (k + 4) * u * scale + 2 * u * np.linalg.norm(ref)
 
 
-@pytest.mark.parametrize("variant,splits", [(0, 2), (1, 4)])
+@pytest.mark.parametrize("variant,splits", [(0, 2), (1, 4), (4, 1), (4, 3)])
 def test_plain_split_broadcast_batch(fg, oracle, variant, splits):
     r = rng(4)
     a = r.uniform(-1, 1, (2, 3, 33, 700))
