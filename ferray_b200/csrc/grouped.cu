@@ -71,14 +71,14 @@ struct fgrt::GroupedJob {
     long long total_tiles = 0;
     long long arena = 0;
     int nseg = 0;
-    size_t sz_probs = 0, sz_maps = 0, sz_ptrs = 0, sz_segs = 0;
+    size_t sz_probs = 0, sz_maps = 0, sz_ptrs = 0, sz_segs = 0, sz_tiles = 0;
     // bound state
     void* dev = nullptr;
     const void* host = nullptr;
     GroupedArgs targs{};
     SimtGroupedArgs sargs{};
     PrepSeg* d_segs = nullptr;
-    size_t host_bytes() const { return sz_probs + sz_maps + sz_ptrs + sz_segs; }
+    size_t host_bytes() const { return sz_probs + sz_maps + sz_ptrs + sz_segs + sz_tiles; }
     size_t dev_bytes() const { return host_bytes() + static_cast<size_t>(arena); }
 };
 
@@ -195,6 +195,7 @@ fg_status grouped_job_build(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, const fg_
     j->sz_maps = j->kind == 0 ? 0 : rup(sizeof(CUtensorMap) * nmaps * npp, 256);
     j->sz_ptrs = j->kind == 0 ? rup((2 * sizeof(void*) + 2 * sizeof(long long)) * npp, 256) : 0;
     j->sz_segs = rup(sizeof(PrepSeg) * std::max(nseg, 1), 256);
+    j->sz_tiles = rup(sizeof(TileRec) * static_cast<size_t>(std::max<long long>(j->total_tiles, 1)), 256);
     return FG_OK;
 }
 
@@ -204,8 +205,17 @@ fg_status grouped_job_bind(GroupedJob* j, void* dev_base, void* host_stage) {
     char* dbase = static_cast<char*>(dev_base);
     char* hbase = static_cast<char*>(host_stage);
     const size_t o_maps = j->sz_probs, o_ptrs = o_maps + j->sz_maps, o_segs = o_ptrs + j->sz_ptrs;
+    const size_t o_tiles = o_segs + j->sz_segs;
     char* d_arena = dbase + j->host_bytes();
     std::memcpy(hbase, j->probs.data(), sizeof(GroupedProblem) * np);
+    TileRec* htiles = reinterpret_cast<TileRec*>(hbase + o_tiles);
+    for (int x = 0; x < np; ++x) {
+        const GroupedProblem& g = j->probs[x];
+        long long t = g.tile_start;
+        for (int tm = 0; tm < g.tiles_m; ++tm)
+            for (int tn = 0; tn < g.tiles_n; ++tn) htiles[t++] = TileRec{x, tm, tn, 0};
+    }
+    const TileRec* dtiles = reinterpret_cast<const TileRec*>(dbase + o_tiles);
     CUtensorMap* hmaps = reinterpret_cast<CUtensorMap*>(hbase + o_maps);
     PrepSeg* hsegs = reinterpret_cast<PrepSeg*>(hbase + o_segs);
     int si = 0;
@@ -258,6 +268,7 @@ fg_status grouped_job_bind(GroupedJob* j, void* dev_base, void* host_stage) {
         }
         const void** dpa = reinterpret_cast<const void**>(dbase + o_ptrs);
         j->sargs.problems = reinterpret_cast<const GroupedProblem*>(dbase);
+        j->sargs.tiles = dtiles;
         j->sargs.a = dpa;
         j->sargs.b = dpa + npp;
         j->sargs.lda = reinterpret_cast<const long long*>(dpa + 2 * npp);
@@ -270,6 +281,7 @@ fg_status grouped_job_bind(GroupedJob* j, void* dev_base, void* host_stage) {
     j->d_segs = reinterpret_cast<PrepSeg*>(dbase + o_segs);
     j->targs = GroupedArgs{};
     j->targs.problems = reinterpret_cast<const GroupedProblem*>(dbase);
+    j->targs.tiles = dtiles;
     j->targs.maps = reinterpret_cast<const CUtensorMap*>(dbase + o_maps);
     j->targs.count = np;
     j->targs.total_tiles = j->total_tiles;

@@ -5,9 +5,10 @@
 // a global tile numbering (prefix sums), its output and the TMA descriptors
 // of its operands (written to global memory before the launch).  Every CTA
 // walks the global tile list with a static stride; the three warp roles of
-// tc_gemm.cuh (TMA producer, MMA issuer, epilogue) each map a tile to its
-// problem by binary search over the prefix sums, so they agree on the
-// sequence without talking to each other.  The host orders problems by
+// tc_gemm.cuh (TMA producer, MMA issuer, epilogue) each read a tile's record
+// (problem, tile row, tile column) from a host-built table, so they agree on
+// the sequence without talking to each other.  The producer prefetches the
+// tensor maps of its next tile's problem while the current one loads.  The host orders problems by
 // decreasing K so the strided walk hands every SM a similar amount of work.
 #pragma once
 #include "tc_gemm.cuh"
@@ -22,8 +23,15 @@ struct GroupedProblem {
     long long ldc;         // elements
 };
 
+// Per global tile: problem index, tile row, tile column (written by the host
+// with the problem table, so a tile costs one load instead of a search).
+struct TileRec {
+    int problem, tm, tn, pad;
+};
+
 struct GroupedArgs {
     const GroupedProblem* problems;
+    const TileRec* tiles;     // [total_tiles]
     const CUtensorMap* maps;  // per problem: NA A maps then NB B maps
     int count;
     long long total_tiles;
@@ -35,15 +43,6 @@ struct GroupedArgs {
     unsigned long long timeout_ns;
 };
 
-__device__ __forceinline__ int find_problem(const GroupedArgs& g, long long t) {
-    int lo = 0, hi = g.count - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (g.problems[mid].tile_start <= t) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
 
 // Stores one warp's 32 rows x 32 columns: lane l holds row row0 + l.  The
 // block goes through a padded shared-memory tile so that the global stores
@@ -118,11 +117,15 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
             for (int i = 0; i < Cfg::STAGES; ++i) issued_parity[i] = -1;
             bool ok = true;
             for (long long t = blockIdx.x; t < g.total_tiles && ok; t += gridDim.x) {
-                const int pi = find_problem(g, t);
+                const TileRec tr = g.tiles[t];
+                const int pi = tr.problem, tm = tr.tm, tn = tr.tn;
                 const GroupedProblem pr = g.problems[pi];
-                const int r = static_cast<int>(t - pr.tile_start);
-                const int tm = r / pr.tiles_n, tn = r - (r / pr.tiles_n) * pr.tiles_n;
                 const CUtensorMap* mp = g.maps + (long long)pi * NMAPS;
+                if (t + gridDim.x < g.total_tiles) {
+                    const int pn = g.tiles[t + gridDim.x].problem;
+                    if (pn != pi)
+                        for (int i = 0; i < NMAPS; ++i) tma_prefetch_desc(g.maps + (long long)pn * NMAPS + i);
+                }
                 for (int kb = 0; kb < pr.k_blocks; ++kb) {
                     if (!mbar_wait(&s.empty[stage], phase ^ 1u, g.timeout_ns, g.status, 0x31, abort)) {
                         ok = false;
@@ -160,7 +163,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
             int it = 0;
             bool ok = true;
             for (long long t = blockIdx.x; t < g.total_tiles && ok; t += gridDim.x) {
-                const int pi = find_problem(g, t);
+                const int pi = g.tiles[t].problem;
                 const int kblocks = g.problems[pi].k_blocks;
                 const int kchunk = (Cfg::CHUNKED && g.kchunk > 0) ? g.kchunk : max(kblocks, 1);
                 for (int kc0 = 0; kc0 < max(kblocks, 1) && ok; kc0 += kchunk, ++it) {
@@ -223,10 +226,9 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
         int it = 0;
         bool ok = true;
         for (long long t = blockIdx.x; t < g.total_tiles && ok; t += gridDim.x) {
-            const int pi = find_problem(g, t);
-            const GroupedProblem pr = g.problems[pi];
-            const int r = static_cast<int>(t - pr.tile_start);
-            const int tm = r / pr.tiles_n, tn = r - (r / pr.tiles_n) * pr.tiles_n;
+            const TileRec tr = g.tiles[t];
+            const int tm = tr.tm, tn = tr.tn;
+            const GroupedProblem pr = g.problems[tr.problem];
             const int kblocks = max(pr.k_blocks, 1);
             const int kchunk = (Cfg::CHUNKED && g.kchunk > 0) ? g.kchunk : kblocks;
             float run[Cfg::CHUNKED ? Cfg::BN : 1];
@@ -304,37 +306,50 @@ struct PrepSeg {
 
 static __global__ void grouped_prep_kernel(const PrepSeg* __restrict__ segs, int nseg,
                                            long long total_rows) {
-    // One block per segment (grid-stride over segments).  Each thread owns
-    // groups of 4 destination elements (ld_dst is a multiple of 4): it issues
-    // the 4 source loads independently and writes one 4- or 8-byte word, so
-    // many loads are in flight per thread.
+    // One block per segment (grid-stride over segments); its warps take rows,
+    // lanes take 16-byte destination chunks of a row (the destination pitch
+    // is a multiple of 16 bytes), so there is no per-element division and a
+    // warp moves 512 contiguous destination bytes per step.  Source loads of
+    // a chunk are independent (many in flight); out-of-row bytes become 0.
     (void)total_rows;
+    const int lane = threadIdx.x % 32, warp = threadIdx.x / 32, nwarps = blockDim.x / 32;
     for (int si = blockIdx.x; si < nseg; si += gridDim.x) {
         const PrepSeg sg = segs[si];
-        const long long q = sg.ld_dst / 4;  // groups per row
-        const long long groups = sg.rows * q;
-        for (long long e = threadIdx.x; e < groups; e += blockDim.x) {
-            const long long r = e / q, c = (e - r * q) * 4;
-            if (sg.op == 0) {
+        if (sg.op == 0) {
+            for (long long r = warp; r < sg.rows; r += nwarps) {
                 const uint8_t* src = static_cast<const uint8_t*>(sg.src) + r * sg.ld_src;
-                uint32_t w = 0;
+                uint8_t* dst = static_cast<uint8_t*>(sg.dst0) + r * sg.ld_dst;
+                for (long long c = lane * 16; c < sg.ld_dst; c += 32 * 16) {
+                    uint32_t w[4];
 #pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    if (c + j < sg.cols) w |= static_cast<uint32_t>(src[c + j]) << (8 * j);
-                *reinterpret_cast<uint32_t*>(static_cast<uint8_t*>(sg.dst0) + r * sg.ld_dst + c) = w;
-            } else {
-                const float* src = static_cast<const float*>(sg.src) + r * sg.ld_src;
-                __align__(8) __nv_bfloat16 h[4], l[4];
+                    for (int q = 0; q < 4; ++q) {
+                        uint32_t v = 0;
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const float x = c + j < sg.cols ? src[c + j] : 0.f;
-                    h[j] = __float2bfloat16_rn(x);
-                    l[j] = __float2bfloat16_rn(x - __bfloat162float(h[j]));
+                        for (int j = 0; j < 4; ++j) {
+                            const long long cc = c + 4 * q + j;
+                            if (cc < sg.cols) v |= static_cast<uint32_t>(src[cc]) << (8 * j);
+                        }
+                        w[q] = v;
+                    }
+                    *reinterpret_cast<uint4*>(dst + c) = make_uint4(w[0], w[1], w[2], w[3]);
                 }
-                *reinterpret_cast<uint2*>(static_cast<__nv_bfloat16*>(sg.dst0) + r * sg.ld_dst + c) =
-                    *reinterpret_cast<const uint2*>(h);
-                *reinterpret_cast<uint2*>(static_cast<__nv_bfloat16*>(sg.dst1) + r * sg.ld_dst + c) =
-                    *reinterpret_cast<const uint2*>(l);
+            }
+        } else {
+            for (long long r = warp; r < sg.rows; r += nwarps) {
+                const float* src = static_cast<const float*>(sg.src) + r * sg.ld_src;
+                __nv_bfloat16* dh = static_cast<__nv_bfloat16*>(sg.dst0) + r * sg.ld_dst;
+                __nv_bfloat16* dl = static_cast<__nv_bfloat16*>(sg.dst1) + r * sg.ld_dst;
+                for (long long c = lane * 8; c < sg.ld_dst; c += 32 * 8) {
+                    __align__(16) __nv_bfloat16 h[8], l[8];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const float x = c + j < sg.cols ? src[c + j] : 0.f;
+                        h[j] = __float2bfloat16_rn(x);
+                        l[j] = __float2bfloat16_rn(x - __bfloat162float(h[j]));
+                    }
+                    *reinterpret_cast<uint4*>(dh + c) = *reinterpret_cast<const uint4*>(h);
+                    *reinterpret_cast<uint4*>(dl + c) = *reinterpret_cast<const uint4*>(l);
+                }
             }
         }
     }
@@ -345,6 +360,7 @@ static __global__ void grouped_prep_kernel(const PrepSeg* __restrict__ segs, int
 // thread, persistent over the global tile list.
 struct SimtGroupedArgs {
     const GroupedProblem* problems;
+    const TileRec* tiles;  // [total_tiles]
     const void* const* a;  // per problem operand pointers and leading dims
     const void* const* b;
     const long long* lda;
@@ -354,29 +370,19 @@ struct SimtGroupedArgs {
     float alpha, beta;
 };
 
-static __device__ __forceinline__ int find_problem_simt(const SimtGroupedArgs& g, long long t) {
-    int lo = 0, hi = g.count - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (g.problems[mid].tile_start <= t) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
-
 static __global__ void __launch_bounds__(256) simt_grouped_sgemm(const SimtGroupedArgs g) {
     constexpr int BM = 64, BN = 64, BK = 16;
     __shared__ float As[BK][BM + 4];
     __shared__ float Bs[BK][BN + 4];
     const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
     for (long long t = blockIdx.x; t < g.total_tiles; t += gridDim.x) {
-        const int pi = find_problem_simt(g, t);
+        const TileRec tr = g.tiles[t];
+        const int pi = tr.problem;
         const GroupedProblem pr = g.problems[pi];
         const float* A = static_cast<const float*>(g.a[pi]);
         const float* B = static_cast<const float*>(g.b[pi]);
         const long long lda = g.lda[pi], ldb = g.ldb[pi];
-        const int r = static_cast<int>(t - pr.tile_start);
-        const int m0 = (r / pr.tiles_n) * BM, n0 = (r % pr.tiles_n) * BN;
+        const int m0 = tr.tm * BM, n0 = tr.tn * BN;
         float acc[4][4] = {};
         for (int k0 = 0; k0 < pr.K; k0 += BK) {
             // A tile 64x16: 1024 elements, 4 per thread (row-major reads along k)
