@@ -27,7 +27,7 @@ using namespace fg;
 
 namespace {
 
-using CfgGroupedI8 = TcCfg<KIND_I8, 128, 4, 1, 1, 1, 1, EPI_I32>;
+using CfgGroupedI8 = TcCfg<KIND_I8, 128, 6, 1, 1, 1, 1, EPI_I32>;
 using CfgGroupedBf16 = TcCfg<KIND_BF16, 128, 3, 2, 2, 1, 3, EPI_F32, 1>;
 
 long long rup(long long x, long long a) { return (x + a - 1) / a * a; }

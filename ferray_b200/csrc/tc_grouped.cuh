@@ -256,8 +256,10 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
                         for (int j = 0; j < 32; ++j) run[c * 32 + j] = __fadd_rn(run[c * 32 + j], __uint_as_float(v[j]));
                     }
                 } else {
+                    // chunks past the problem's last row / column hold nothing
+                    const int nch = row0 < pr.M ? min(Cfg::BN / 32, (pr.N - tn * Cfg::BN + 31) / 32) : 0;
 #pragma unroll 1
-                    for (int c = 0; c < Cfg::BN / 32; ++c) {
+                    for (int c = 0; c < nch; ++c) {
                         uint32_t v[32];
                         tmem_ld_32x32b_x32(row_addr + c * 32, v);
                         tmem_wait_ld();
@@ -304,52 +306,62 @@ struct PrepSeg {
     int op;
 };
 
+// One 16-byte destination chunk of segment row r at byte / element offset c.
+__device__ __forceinline__ void prep_chunk(const PrepSeg& sg, long long r, long long c) {
+    if (sg.op == 0) {
+        const uint8_t* src = static_cast<const uint8_t*>(sg.src) + r * sg.ld_src;
+        uint32_t w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            uint32_t v = 0;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const long long cc = c + 4 * q + j;
+                if (cc < sg.cols) v |= static_cast<uint32_t>(__ldg(src + cc)) << (8 * j);
+            }
+            w[q] = v;
+        }
+        *reinterpret_cast<uint4*>(static_cast<uint8_t*>(sg.dst0) + r * sg.ld_dst + c) =
+            make_uint4(w[0], w[1], w[2], w[3]);
+    } else {
+        const float* src = static_cast<const float*>(sg.src) + r * sg.ld_src;
+        __align__(16) __nv_bfloat16 h[8], l[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const float x = c + j < sg.cols ? __ldg(src + c + j) : 0.f;
+            h[j] = __float2bfloat16_rn(x);
+            l[j] = __float2bfloat16_rn(x - __bfloat162float(h[j]));
+        }
+        *reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(sg.dst0) + r * sg.ld_dst + c) =
+            *reinterpret_cast<const uint4*>(h);
+        *reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(sg.dst1) + r * sg.ld_dst + c) =
+            *reinterpret_cast<const uint4*>(l);
+    }
+}
+
 static __global__ void grouped_prep_kernel(const PrepSeg* __restrict__ segs, int nseg,
                                            long long total_rows) {
-    // One block per segment (grid-stride over segments); its warps take rows,
-    // lanes take 16-byte destination chunks of a row (the destination pitch
-    // is a multiple of 16 bytes), so there is no per-element division and a
-    // warp moves 512 contiguous destination bytes per step.  Source loads of
-    // a chunk are independent (many in flight); out-of-row bytes become 0.
+    // One block per segment (grid-stride over segments).  The block's threads
+    // take the segment's 16-byte destination chunks (destination pitch is a
+    // multiple of 16 bytes) in row-major order, so rows shorter than a warp's
+    // reach still keep every lane busy; consecutive lanes write consecutive
+    // chunks.  Out-of-row bytes become 0.
     (void)total_rows;
-    const int lane = threadIdx.x % 32, warp = threadIdx.x / 32, nwarps = blockDim.x / 32;
     for (int si = blockIdx.x; si < nseg; si += gridDim.x) {
         const PrepSeg sg = segs[si];
-        if (sg.op == 0) {
-            for (long long r = warp; r < sg.rows; r += nwarps) {
-                const uint8_t* src = static_cast<const uint8_t*>(sg.src) + r * sg.ld_src;
-                uint8_t* dst = static_cast<uint8_t*>(sg.dst0) + r * sg.ld_dst;
-                for (long long c = lane * 16; c < sg.ld_dst; c += 32 * 16) {
-                    uint32_t w[4];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        uint32_t v = 0;
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            const long long cc = c + 4 * q + j;
-                            if (cc < sg.cols) v |= static_cast<uint32_t>(src[cc]) << (8 * j);
-                        }
-                        w[q] = v;
-                    }
-                    *reinterpret_cast<uint4*>(dst + c) = make_uint4(w[0], w[1], w[2], w[3]);
-                }
+        const long long per = sg.op == 0 ? 16 : 8;  // elements per chunk
+        const long long cpr = sg.ld_dst / per;      // chunks per row
+        const long long total = sg.rows * cpr;
+        if (total < (1LL << 31)) {
+            const unsigned ucpr = static_cast<unsigned>(cpr);
+            for (unsigned idx = threadIdx.x; idx < static_cast<unsigned>(total); idx += blockDim.x) {
+                const unsigned r = idx / ucpr;
+                prep_chunk(sg, r, static_cast<long long>(idx - r * ucpr) * per);
             }
         } else {
-            for (long long r = warp; r < sg.rows; r += nwarps) {
-                const float* src = static_cast<const float*>(sg.src) + r * sg.ld_src;
-                __nv_bfloat16* dh = static_cast<__nv_bfloat16*>(sg.dst0) + r * sg.ld_dst;
-                __nv_bfloat16* dl = static_cast<__nv_bfloat16*>(sg.dst1) + r * sg.ld_dst;
-                for (long long c = lane * 8; c < sg.ld_dst; c += 32 * 8) {
-                    __align__(16) __nv_bfloat16 h[8], l[8];
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        const float x = c + j < sg.cols ? src[c + j] : 0.f;
-                        h[j] = __float2bfloat16_rn(x);
-                        l[j] = __float2bfloat16_rn(x - __bfloat162float(h[j]));
-                    }
-                    *reinterpret_cast<uint4*>(dh + c) = *reinterpret_cast<const uint4*>(h);
-                    *reinterpret_cast<uint4*>(dl + c) = *reinterpret_cast<const uint4*>(l);
-                }
+            for (long long idx = threadIdx.x; idx < total; idx += blockDim.x) {
+                const long long r = idx / cpr;
+                prep_chunk(sg, r, (idx - r * cpr) * per);
             }
         }
     }
