@@ -35,6 +35,9 @@ using CfgBf16x3 = TcCfg<KIND_BF16, 128, 3, 2, 2, 1, 3, EPI_F32, 1>;
 using CfgBf16x3n64 = TcCfg<KIND_BF16, 64, 4, 2, 2, 1, 3, EPI_F32, 1>;
 // 256 x 128 tiles on CTA pairs, 4 stages of 48 KB per CTA.
 using CfgBf16x3Pair = Tc2Cfg<KIND_BF16, 128, 4, 2, 2, 1, 3, EPI_F32, 1>;
+// 6 products (3 slices) on CTA pairs: 256 x 128 tiles, 3 stages of 72 KB per
+// CTA, hi*hi and the corrections in two TMEM accumulators.
+using CfgBf16x6Pair = Tc2Cfg<KIND_BF16, 128, 3, 3, 3, 2, 6, EPI_F32, 1>;
 using CfgBf16x6 = TcCfg<KIND_BF16, 128, 2, 3, 3, 2, 6, EPI_F32, 1>;
 
 // K blocks (64 bf16 each) per TMEM accumulation chunk of the split SGEMM.
@@ -50,7 +53,8 @@ static unsigned long long kTimeoutNs = 4000000000ull;  // 4 s per wait
 
 template <class Cfg>
 static const char* cfg_name() {
-    if (Cfg::BM == 256) return Cfg::KIND == KIND_BF16 ? "tc_gemm2_3xbf16" : "tc_gemm2_i8";
+    if (Cfg::BM == 256)
+        return Cfg::KIND == KIND_BF16 ? (Cfg::NOPS == 6 ? "tc_gemm2_6xbf16" : "tc_gemm2_3xbf16") : "tc_gemm2_i8";
     if (Cfg::KIND == KIND_BF16) return Cfg::NOPS == 6 ? "tc_gemm_6xbf16" : "tc_gemm_3xbf16";
     if (Cfg::EPI == EPI_I16) return "tc_gemm_i16";
     if (Cfg::EPI == EPI_QMM) return "tc_gemm_qmm";
@@ -462,6 +466,12 @@ fg_status launch_split_bf16(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
         args.ops[3] = TcOp{1, 0, 1, 1, 1};
         args.ops[4] = TcOp{0, 1, 1, 1, 1};
         args.ops[5] = TcOp{0, 0, 0, 1, 1};
+        // the pair kernel where the tuned 3-product table picks a pair tile
+        if (!cplx && tune_lookup(TUNE_SPLIT_F32, M, N, K).variant == 2) {
+            args.tiles_m = static_cast<int>((M + CfgBf16x6Pair::BM - 1) / CfgBf16x6Pair::BM);
+            args.tiles_n = static_cast<int>((N + CfgBf16x6Pair::BN - 1) / CfgBf16x6Pair::BN);
+            return launch_pair<CfgBf16x6Pair>(ctx, maps, args, st);
+        }
         return launch_cfg<CfgBf16x6>(ctx, maps, args, st);
     }
     args.ops[0] = TcOp{1, 0, 0, 1, 1};  // lo * hi

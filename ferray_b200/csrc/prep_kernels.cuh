@@ -39,45 +39,49 @@ __device__ __forceinline__ void split_n(float x, int ns, __nv_bfloat16 (&o)[3]) 
 }
 
 // Real operand: X (rows x cols, pitch ldx) -> ns planes (pitch ldo, a
-// multiple of 4).  Blocks stride over rows, threads over 4-element groups
-// of a row (no per-element division); two groups per thread per step keep
-// two 16-byte loads in flight; 8-byte stores per plane.
+// multiple of 8).  Blocks stride over rows, threads over 8-element groups of
+// a row (no per-element division); two groups per thread per step keep four
+// 16-byte loads in flight; 16-byte stores per plane.
 static __global__ void split_bf16_kernel(const float* __restrict__ X, long long rows, long long cols,
                                          long long ldx, BfPlanes out, long long ldo, int ns,
                                          long long x_bstride, long long o_bstride) {
     const float* Xb = X + blockIdx.y * x_bstride;
-    const long long cq = (cols + 3) / 4;
+    const long long cq = (cols + 7) / 8;
     const bool vec_in = (ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(Xb) & 15) == 0);
     for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
         const float* xr = Xb + r * ldx;
         for (long long q0 = threadIdx.x; q0 < cq; q0 += 2 * blockDim.x) {
-            float v[2][4];
+            float v[2][8];
 #pragma unroll
             for (int u = 0; u < 2; ++u) {
-                const long long c = (q0 + u * blockDim.x) * 4;
-                if (vec_in && c + 3 < cols) {
-                    const float4 w = *reinterpret_cast<const float4*>(xr + c);
-                    v[u][0] = w.x; v[u][1] = w.y; v[u][2] = w.z; v[u][3] = w.w;
+                const long long c = (q0 + u * blockDim.x) * 8;
+                if (vec_in && c + 7 < cols) {
+                    const float4 w0 = *reinterpret_cast<const float4*>(xr + c);
+                    const float4 w1 = *reinterpret_cast<const float4*>(xr + c + 4);
+                    v[u][0] = w0.x; v[u][1] = w0.y; v[u][2] = w0.z; v[u][3] = w0.w;
+                    v[u][4] = w1.x; v[u][5] = w1.y; v[u][6] = w1.z; v[u][7] = w1.w;
                 } else {
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) v[u][j] = (c + j < cols) ? xr[c + j] : 0.f;
+                    for (int j = 0; j < 8; ++j) v[u][j] = (c + j < cols) ? xr[c + j] : 0.f;
                 }
             }
 #pragma unroll
             for (int u = 0; u < 2; ++u) {
                 const long long q = q0 + u * blockDim.x;
                 if (q >= cq) break;
-                const long long c = q * 4;
-                __nv_bfloat16 o[4][3];
+                const long long c = q * 8;
+                __nv_bfloat16 o[8][3];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) split_n(v[u][j], ns, o[j]);
+                for (int j = 0; j < 8; ++j) split_n(v[u][j], ns, o[j]);
                 for (int s = 0; s < ns; ++s) {
                     __nv_bfloat16* dst = out.p[s] + blockIdx.y * o_bstride + r * ldo + c;
-                    if (c + 3 < ldo) {
-                        __align__(8) __nv_bfloat16 w[4] = {o[0][s], o[1][s], o[2][s], o[3][s]};
-                        *reinterpret_cast<uint2*>(dst) = *reinterpret_cast<const uint2*>(w);
+                    if (c + 7 < ldo) {
+                        __align__(16) __nv_bfloat16 w[8];
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) w[j] = o[j][s];
+                        *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(w);
                     } else {
-                        for (int j = 0; j < 4 && c + j < ldo; ++j) dst[j] = o[j][s];
+                        for (int j = 0; j < 8 && c + j < ldo; ++j) dst[j] = o[j][s];
                     }
                 }
             }
