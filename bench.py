@@ -300,6 +300,54 @@ def side_measurements(fg, L, lib, ctx, stream, n, only=""):
             del bufs
         res["ragged_4096"] = {"gflop": round(gflop, 2), **g}
         torch.cuda.empty_cache()
+    if only == "ozaki":
+        # --- DGEMM / ZGEMM plain vs Ozaki INT8 per exponent spread and slice
+        # count: A = diag(10^(s u)) G diag(10^(s v)), B built the same way
+        # independently, G ~ N(0, 1), u, v ~ U[-1, 1]; error vs the DD oracle
+        # on a sampled 64 x 64 block (normwise estimate).
+        oz = {}
+        for nn in (2048, 4096, 8192):
+            if nn > n:
+                continue
+            for cplx in (False, True):
+                for spread in (0, 4, 8):
+                    r2 = np.random.default_rng(SEED + spread + nn)
+
+                    def spread_mat():
+                        g = r2.standard_normal((nn, nn))
+                        if cplx:
+                            g = g + 1j * r2.standard_normal((nn, nn))
+                        du = 10.0 ** (spread * r2.uniform(-1, 1, nn))
+                        dv = 10.0 ** (spread * r2.uniform(-1, 1, nn))
+                        return (du[:, None] * g) * dv[None, :]
+                    a, b = spread_mat(), spread_mat()
+                    dt = np.complex128 if cplx else np.float64
+                    da, db = fg.DeviceArray.from_numpy(a, ctx), fg.DeviceArray.from_numpy(b, ctx)
+                    dc = fg.DeviceArray((nn, nn), dt, ctx)
+                    rows, cols = oracle.sample_indices(nn, nn, 64, 64, seed=13)
+                    ref = oracle.dd_sampled(a, b, rows, cols)
+                    na, nb = oracle.fro(a), oracle.fro(b)
+                    flops = (8.0 if cplx else 2.0) * nn ** 3
+                    entry = {}
+                    for name, mode, sl in (("plain", L.FG_MODE_PLAIN, 0), ("ozaki6", L.FG_MODE_SPLIT, 6),
+                                           ("ozaki7", L.FG_MODE_SPLIT, 7), ("ozaki8", L.FG_MODE_SPLIT, 8),
+                                           ("ozaki9", L.FG_MODE_SPLIT, 9)):
+                        if cplx:
+                            call = lambda: lib.fg_gemm_c64(ctx.handle, mode, sl, nn, nn, nn, 1.0, 0.0, da.ptr,
+                                                           db.ptr, 0.0, 0.0, dc.ptr, sh)
+                        else:
+                            call = lambda: lib.fg_gemm_f64(ctx.handle, mode, sl, nn, nn, nn, 1.0, da.ptr,
+                                                           db.ptr, 0.0, dc.ptr, sh)
+                        ms = _time_calls(torch, stream, call, 2, 1)
+                        err = oracle.normwise_error(dc.to_numpy()[np.ix_(rows, cols)], ref, nn, nn, na, nb)
+                        entry[name] = {"tflops": round(flops / ms / 1e9, 2), "ms": round(ms, 3), "err": err}
+                    for name in ("ozaki6", "ozaki7", "ozaki8", "ozaki9"):
+                        entry[name]["speed_over_plain"] = round(entry[name]["tflops"] / entry["plain"]["tflops"], 2)
+                        entry[name]["err_over_plain"] = round(entry[name]["err"] / entry["plain"]["err"], 3)
+                    oz["%s_%d_spread%d" % ("zgemm" if cplx else "dgemm", nn, spread)] = entry
+                    del da, db, dc, a, b
+                    torch.cuda.empty_cache()
+        res["ozaki_sweep"] = oz
     if only == "skinny":
         # --- skinny shapes on the HBM roof: algorithmic bytes / device time
         _, hbm, _ = peaks()

@@ -142,11 +142,14 @@ fg_status launch_ozaki(fg_ctx* ctx, const Gemm& g0, cudaStream_t st) {
     if (g.alpha_im != 0.0 || g.beta_im != 0.0)
         return set_error(FG_ERR_UNSUPPORTED, "split ZGEMM: complex alpha/beta must be real");
     const long long M = g.M, Kw = cplx ? 2 * g.K : g.K, Nw = cplx ? 2 * g.N : g.N;
-    // int32 exactness: S products of Kc * 127^2 per group sum.
-    const long long kmax = ((2147483647ll / (16129ll * S)) / 128) * 128;
-    const long long Kp = round_up(Kw, 16);
-    const long long nchunks = (Kp + kmax - 1) / kmax;
-    const long long Kc = nchunks == 1 ? Kp : kmax;
+    // The operands are sliced once over the whole (padded) K; int32
+    // exactness is kept per launch instead: a launch accumulates at most
+    // kpiece digit products (each |.| <= 127^2) in one int32, so a group
+    // whose concatenated K ((d-1) Kp) is longer runs as several launches.
+    const long long kpiece = ((2147483647ll / 16129ll) / 128) * 128;
+    const long long Kp = round_up(Kw, 128);
+    const long long nchunks = 1;
+    const long long Kc = Kp;
     const long long Np = round_up(Nw, 16);
     const size_t a_bytes = static_cast<size_t>(nchunks * M * S * Kc);
     const size_t b_bytes = static_cast<size_t>(nchunks * S * Kc * Np);
@@ -177,25 +180,24 @@ fg_status launch_ozaki(fg_ctx* ctx, const Gemm& g0, cudaStream_t st) {
     FG_TRY(sst);
 
     bool first = true;
-    for (long long c = 0; c < nchunks; ++c) {
-        const int8_t* ac = a_all + c * M * S * Kc;
-        const int8_t* bc = b_all + c * S * Kc * Np;
-        for (int d = S + 1; d >= 2; --d) {
-            const long long Kd = (d - 1) * Kc;
+    for (int d = S + 1; d >= 2; --d) {
+        const long long Kd_all = (d - 1) * Kc;
+        for (long long k0 = 0; k0 < Kd_all; k0 += kpiece) {
+            const long long Kd = std::min(kpiece, Kd_all - k0);
             TcMaps maps;
             TcArgs args{};
             {
                 uint64_t dims[2] = {static_cast<uint64_t>(Kd), static_cast<uint64_t>(M)};
                 uint64_t strides[1] = {static_cast<uint64_t>(S * Kc)};
                 uint32_t box[2] = {128, 128};
-                FG_TRY(encode_map(&maps.a[0], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, ac, dims, strides, box));
+                FG_TRY(encode_map(&maps.a[0], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, a_all + k0, dims, strides, box));
             }
             {
                 uint64_t dims[2] = {static_cast<uint64_t>(Nw), static_cast<uint64_t>(Kd)};
                 uint64_t strides[1] = {static_cast<uint64_t>(Np)};
                 uint32_t box[2] = {128, 128};
                 FG_TRY(encode_map(&maps.b[0], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2,
-                                  bc + (S - d + 1) * Kc * Np, dims, strides, box));
+                                  b_all + ((S - d + 1) * Kc + k0) * Np, dims, strides, box));
             }
             const bool pair = tune_lookup(TUNE_I8, M, Nw, Kd).variant == 2;
             args.M = static_cast<int>(M);

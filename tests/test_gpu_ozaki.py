@@ -113,3 +113,23 @@ def test_split_matmul_batched_f64(fg):
     got = fg.matmul(a, b, mode="split")
     want = np.matmul(a, b)
     assert np.max(np.abs(got - want)) < 1e-12
+
+
+@pytest.mark.parametrize("m,n,k,cplx", [(64, 48, 15000, False), (40, 24, 7600, True)])
+def test_split_long_k_group_pieces(fg, oracle, m, n, k, cplx):
+    # 9 slices: the top slice group's concatenated K (9 x K, x2 embedded for
+    # complex) exceeds what one int32 accumulator holds exactly, so that group
+    # runs as several launches; the result keeps the default-slice bound.
+    rng = np.random.default_rng(k)
+    a = rng.uniform(-1, 1, (m, k))
+    b = rng.uniform(-1, 1, (k, n))
+    if cplx:
+        a = a + 1j * rng.uniform(-1, 1, (m, k))
+        b = b + 1j * rng.uniform(-1, 1, (k, n))
+        c = np.zeros((m, n), np.complex128)
+        assert fg.gemm_c64(m, n, k, 1.0, 0.0, a, b, 0.0, 0.0, c, mode="split")
+    else:
+        c = np.zeros((m, n))
+        assert fg.gemm_f64(m, n, k, 1.0, a, b, 0.0, c, mode="split")
+    err = oracle.error_vs_dd(a, b, c)
+    assert err <= (2 if cplx else 1) * k * U64 + 11 * 2.0 ** (2 - 63), err
