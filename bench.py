@@ -300,6 +300,29 @@ def side_measurements(fg, L, lib, ctx, stream, n, only=""):
             del bufs
         res["ragged_4096"] = {"gflop": round(gflop, 2), **g}
         torch.cuda.empty_cache()
+    if only == "int":
+        # --- i16 x i16 -> i32 (4 byte-slice products) and the quantized
+        # u8 x i8 -> f32 GEMM (zero points, fused epilogue) at N = n
+        a16 = torch.randint(-32768, 32767, (n * n,), dtype=torch.int16, device="cuda")
+        b16 = torch.randint(-32768, 32767, (n * n,), dtype=torch.int16, device="cuda")
+        c32 = torch.zeros(n * n, dtype=torch.int32, device="cuda")
+        ms = _time_calls(torch, stream, lambda: lib.fg_gemm_i16(ctx.handle, n, n, n, a16.data_ptr(), b16.data_ptr(),
+                                                                 c32.data_ptr(), 0, sh), 5, 2)
+        r8, c8 = oracle.sample_indices(n, n, 16, 16, seed=3)
+        ah, bh = a16.cpu().numpy().reshape(n, n), b16.cpu().numpy().reshape(n, n)
+        want = (ah[r8].astype(np.int64) @ bh[:, c8].astype(np.int64))
+        want = ((want + 2 ** 31) % 2 ** 32 - 2 ** 31).astype(np.int32)
+        got = c32.cpu().numpy().reshape(n, n)[np.ix_(r8, c8)]
+        res["i16_square_%d" % n] = {"tops": round(2.0 * n ** 3 / ms / 1e9, 1), "ms": round(ms, 4),
+                                    "bit_exact_sampled": bool(np.array_equal(got, want))}
+        au = torch.randint(0, 255, (n * n,), dtype=torch.uint8, device="cuda")
+        bq = torch.randint(-128, 127, (n * n,), dtype=torch.int8, device="cuda")
+        cf = torch.zeros(n * n, dtype=torch.float32, device="cuda")
+        ms = _time_calls(torch, stream, lambda: lib.fg_quantized_matmul(ctx.handle, n, n, n, au.data_ptr(), 3, 0.02,
+                                                                         bq.data_ptr(), -5, 0.01, cf.data_ptr(), 0, sh), 5, 2)
+        res["quantized_u8i8_%d" % n] = {"tops": round(2.0 * n ** 3 / ms / 1e9, 1), "ms": round(ms, 4)}
+        del a16, b16, c32, au, bq, cf
+        torch.cuda.empty_cache()
     if only == "ozaki":
         # --- DGEMM / ZGEMM plain vs Ozaki INT8 per exponent spread and slice
         # count: A = diag(10^(s u)) G diag(10^(s v)), B built the same way

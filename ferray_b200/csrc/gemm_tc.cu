@@ -27,6 +27,7 @@ using CfgI8n128 = TcCfg<KIND_I8, 128, 6, 1, 1, 1, 1, EPI_I32>;
 // 256 x 256 tiles on CTA pairs (cta_group::2), 6 stages of 32 KB per CTA.
 using CfgI8Pair = Tc2Cfg<KIND_I8, 256, 6, 1, 1, 1, 1, EPI_I32>;
 using CfgQmm = TcCfg<KIND_I8, 256, 4, 1, 1, 1, 1, EPI_QMM>;
+using CfgQmmPair = Tc2Cfg<KIND_I8, 256, 6, 1, 1, 1, 1, EPI_QMM>;
 using CfgI16 = TcCfg<KIND_I8, 128, 3, 2, 2, 3, 4, EPI_I16>;
 // 3 products: one accumulator (the 2-slice representation error, about
 // 2^-18 |a||b| per product, dominates whatever the accumulation does).
@@ -341,7 +342,9 @@ fg_status launch_qmm(fg_ctx* ctx, long long M, long long N, long long K, const u
     int* row_sum = static_cast<int*>(sums.p);
     int* col_sum = row_sum + M;
     row_sum_u8_kernel<<<grid_for(M * 32), 256, 0, st>>>(a, M, K, K, row_sum);
-    col_sum_i8_kernel<<<grid_for(N), 256, 0, st>>>(b, K, N, N, col_sum);
+    FG_CUDA(cudaMemsetAsync(col_sum, 0, N * sizeof(int), st));
+    col_sum_i8_kernel<<<dim3(static_cast<unsigned>((N + 255) / 256), static_cast<unsigned>((K + 255) / 256)),
+                        256, 0, st>>>(b, K, N, N, 256, col_sum);
     count_launch(2);
     FG_CUDA(cudaGetLastError());
     Scratch sa, sb;
@@ -369,6 +372,11 @@ fg_status launch_qmm(fg_ctx* ctx, long long M, long long N, long long K, const u
     args.ops[0] = TcOp{0, 0, 0, 0, 1};
     FG_TRY(operand_map(&maps.a[0], CU_TENSOR_MAP_DATA_TYPE_UINT8, pa, K, M, lda, 1, 0, 128, 128, &args.a_rank3));
     FG_TRY(operand_map(&maps.b[0], CU_TENSOR_MAP_DATA_TYPE_UINT8, pb, N, K, ldb, 1, 0, 128, 128, &args.b_rank3));
+    // CTA pairs where the tuned i8 table picks them for this shape
+    if (tune_lookup(TUNE_I8, M, N, K).variant == 2) {
+        args.tiles_m = static_cast<int>((M + CfgQmmPair::BM - 1) / CfgQmmPair::BM);
+        return launch_pair<CfgQmmPair>(ctx, maps, args, st);
+    }
     return launch_cfg<CfgQmm>(ctx, maps, args, st);
 }
 

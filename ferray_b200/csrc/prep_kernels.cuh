@@ -169,14 +169,19 @@ static __global__ void row_sum_u8_kernel(const uint8_t* __restrict__ A, long lon
     if (lane == 0) out[warp] = static_cast<int>(s);
 }
 
-// col_sum[j] = sum_k b[k, j] (i8), one thread per column, wrapping i32.
+// col_sum[j] += sum over rows [y * rows_per, (y + 1) * rows_per) of b[k, j]
+// (i8), y = blockIdx.y: one thread per column and row block, the partial
+// sums added with atomicAdd into an array the caller zeroed.  Integer
+// addition mod 2^32 is associative, so the result is exact and independent
+// of the order the blocks arrive in.
 static __global__ void col_sum_i8_kernel(const int8_t* __restrict__ B, long long K, long long N,
-                                  long long ldb, int* __restrict__ out) {
+                                  long long ldb, long long rows_per, int* __restrict__ out) {
     const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (j >= N) return;
+    const long long k0 = blockIdx.y * rows_per, k1 = min(K, k0 + rows_per);
     uint32_t s = 0;
-    for (long long k = 0; k < K; ++k) s += static_cast<uint32_t>(static_cast<int32_t>(B[k * ldb + j]));
-    out[j] = static_cast<int>(s);
+    for (long long k = k0; k < k1; ++k) s += static_cast<uint32_t>(static_cast<int32_t>(B[k * ldb + j]));
+    atomicAdd(reinterpret_cast<unsigned int*>(out + j), s);
 }
 
 // C = beta * C for k == 0 (real / complex), and fill.

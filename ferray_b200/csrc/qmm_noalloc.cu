@@ -108,7 +108,9 @@ extern "C" fg_status fg_quantized_matmul_noalloc(fg_ctx* ctx, size_t m, size_t n
     int* col_sum = sums + kQmmNoAllocMaxM;
     const long long M = (long long)m, N = (long long)n, K = (long long)k;
     fg::row_sum_u8_kernel<<<grid_for(M * 32), 256, 0, st>>>(a, M, K, K, row_sum);
-    fg::col_sum_i8_kernel<<<grid_for(N), 256, 0, st>>>(b, K, N, N, col_sum);
+    FG_CUDA(cudaMemsetAsync(col_sum, 0, N * sizeof(int), st));
+    fg::col_sum_i8_kernel<<<dim3(static_cast<unsigned>((N + 255) / 256), static_cast<unsigned>((K + 255) / 256)),
+                            256, 0, st>>>(b, K, N, N, 256, col_sum);
     count_launch(2);
     FG_CUDA(cudaGetLastError());
 

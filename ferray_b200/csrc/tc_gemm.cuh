@@ -236,15 +236,23 @@ __device__ __forceinline__ void epilogue_store(const TcArgs& p, int bz, int grow
             cs[j] = j < ncols ? static_cast<uint32_t>(p.col_sum[gcol0 + j]) : 0u;
             old[j] = (p.accumulate && j < ncols) ? crow[j] : 0.f;
         }
+        float out[32];
 #pragma unroll
         for (int j = 0; j < 32; ++j) {
-            if (j < ncols) {
-                const uint32_t corr = v[0][j] - azp * cs[j] - bzp * rs + kab;
-                // Separate roundings, as gemm/mod.rs:566-571 computes them (no FMA).
-                float o = __fmul_rn(p.scale, static_cast<float>(static_cast<int32_t>(corr)));
-                if (p.accumulate) o = __fadd_rn(old[j], o);
-                crow[j] = o;
-            }
+            const uint32_t corr = v[0][j] - azp * cs[j] - bzp * rs + kab;
+            // Separate roundings, as gemm/mod.rs:566-571 computes them (no FMA).
+            float o = __fmul_rn(p.scale, static_cast<float>(static_cast<int32_t>(corr)));
+            if (p.accumulate) o = __fadd_rn(old[j], o);
+            out[j] = o;
+        }
+        if (ncols == 32 && (reinterpret_cast<uintptr_t>(crow) & 15) == 0) {
+#pragma unroll
+            for (int j = 0; j < 32; j += 4)
+                *reinterpret_cast<float4*>(crow + j) = make_float4(out[j], out[j + 1], out[j + 2], out[j + 3]);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+                if (j < ncols) crow[j] = out[j];
         }
     } else if constexpr (Cfg::EPI == EPI_OZAKI) {
         double* cbase = static_cast<double*>(p.C) + bz * p.strideC;
