@@ -223,9 +223,11 @@ def _time_calls(torch, stream, fn, steps, warmup):
 def side_measurements(fg, L, lib, ctx, stream, n, only=""):
     """The other configs, one short measurement each (device-timed):
     DGEMM plain vs Ozaki split at N=n with their DD-oracle errors; square i8
-    at N=n (bit-exact on a sampled block); the 4096-problem ragged batch as one
+    at N=n (bit-exact on a sampled block); i16 and quantized u8 x i8; skinny
+    shapes against the HBM roof; the 4096-problem ragged batch as one
     grouped graph replay vs a loop of per-problem launches; the served stream
-    at 10k req/s, server vs plain one-call-at-a-time."""
+    at 10k req/s, server vs plain one-call-at-a-time.  `only="ozaki"` runs
+    the per-spread / per-slice-count DGEMM and ZGEMM sweep (N = 2048..8192)."""
     import torch
     import oracle
     import bench_serving
@@ -300,7 +302,7 @@ def side_measurements(fg, L, lib, ctx, stream, n, only=""):
             del bufs
         res["ragged_4096"] = {"gflop": round(gflop, 2), **g}
         torch.cuda.empty_cache()
-    if only == "int":
+    if not only or only == "int":
         # --- i16 x i16 -> i32 (4 byte-slice products) and the quantized
         # u8 x i8 -> f32 GEMM (zero points, fused epilogue) at N = n
         a16 = torch.randint(-32768, 32767, (n * n,), dtype=torch.int16, device="cuda")
@@ -371,7 +373,7 @@ def side_measurements(fg, L, lib, ctx, stream, n, only=""):
                     del da, db, dc, a, b
                     torch.cuda.empty_cache()
         res["ozaki_sweep"] = oz
-    if only == "skinny":
+    if not only or only == "skinny":
         # --- skinny shapes on the HBM roof: algorithmic bytes / device time
         _, hbm, _ = peaks()
         sk = {}
