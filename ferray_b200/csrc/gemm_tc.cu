@@ -419,26 +419,42 @@ fg_status launch_split_bf16(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
     for (int i = 0; i < ns; ++i) bp.p[i] = base + ns * a_elems + i * b_elems;
     if (cplx) {
         if (g.M * g.K > 0) {
-            split_bf16_cplx_a_kernel<<<grid_for(g.M * g.K), 256, 0, st>>>(
-                static_cast<const float2*>(g.A), g.M, g.K, g.lda, ap, pa, ns);
+            if (ns == 3)
+                split_bf16_cplx_a_kernel<3><<<grid_for(g.M * g.K), 256, 0, st>>>(
+                    static_cast<const float2*>(g.A), g.M, g.K, g.lda, ap, pa);
+            else
+                split_bf16_cplx_a_kernel<2><<<grid_for(g.M * g.K), 256, 0, st>>>(
+                    static_cast<const float2*>(g.A), g.M, g.K, g.lda, ap, pa);
             count_launch();
         }
         if (g.K * g.N > 0) {
-            split_bf16_cplx_b_kernel<<<grid_for(g.K * g.N), 256, 0, st>>>(
-                static_cast<const float2*>(g.B), g.K, g.N, g.ldb, bp, pb, ns);
+            if (ns == 3)
+                split_bf16_cplx_b_kernel<3><<<grid_for(g.K * g.N), 256, 0, st>>>(
+                    static_cast<const float2*>(g.B), g.K, g.N, g.ldb, bp, pb);
+            else
+                split_bf16_cplx_b_kernel<2><<<grid_for(g.K * g.N), 256, 0, st>>>(
+                    static_cast<const float2*>(g.B), g.K, g.N, g.ldb, bp, pb);
             count_launch();
         }
     } else {
+        ProfScope prof("split_bf16", st);
         if (M * K > 0) {
-            split_bf16_kernel<<<dim3(static_cast<unsigned>(std::min<long long>(M, 4096)), static_cast<unsigned>(g.a_count)), 256, 0, st>>>(
-                static_cast<const float*>(g.A), M, K, g.lda, ap, pa, ns, g.a_mstride, pa * M);
+            const dim3 grid(static_cast<unsigned>(std::min<long long>(M, 8LL * ctx->sm_count)), static_cast<unsigned>(g.a_count));
+            if (ns == 3)
+                split_bf16_kernel_t<3><<<grid, 256, 0, st>>>(static_cast<const float*>(g.A), M, K, g.lda, ap, pa, g.a_mstride, pa * M);
+            else
+                split_bf16_kernel_t<2><<<grid, 256, 0, st>>>(static_cast<const float*>(g.A), M, K, g.lda, ap, pa, g.a_mstride, pa * M);
             count_launch();
         }
         if (K * N > 0) {
-            split_bf16_kernel<<<dim3(static_cast<unsigned>(std::min<long long>(K, 4096)), static_cast<unsigned>(g.b_count)), 256, 0, st>>>(
-                static_cast<const float*>(g.B), K, N, g.ldb, bp, pb, ns, g.b_mstride, pb * K);
+            const dim3 grid(static_cast<unsigned>(std::min<long long>(K, 8LL * ctx->sm_count)), static_cast<unsigned>(g.b_count));
+            if (ns == 3)
+                split_bf16_kernel_t<3><<<grid, 256, 0, st>>>(static_cast<const float*>(g.B), K, N, g.ldb, bp, pb, g.b_mstride, pb * K);
+            else
+                split_bf16_kernel_t<2><<<grid, 256, 0, st>>>(static_cast<const float*>(g.B), K, N, g.ldb, bp, pb, g.b_mstride, pb * K);
             count_launch();
         }
+        prof.stop();
     }
     FG_CUDA(cudaGetLastError());
     TcMaps maps;

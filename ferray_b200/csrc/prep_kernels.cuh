@@ -38,26 +38,43 @@ __device__ __forceinline__ void split_n(float x, int ns, __nv_bfloat16 (&o)[3]) 
     }
 }
 
-// Real operand: X (rows x cols, pitch ldx) -> ns planes (pitch ldo, a
-// multiple of 8).  Blocks stride over rows, threads over 8-element groups of
-// a row (no per-element division); two groups per thread per step keep four
-// 16-byte loads in flight; 16-byte stores per plane.
-static __global__ void split_bf16_kernel(const float* __restrict__ X, long long rows, long long cols,
-                                         long long ldx, BfPlanes out, long long ldo, int ns,
-                                         long long x_bstride, long long o_bstride) {
+__device__ __forceinline__ uint32_t pack_bf16x2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+    return static_cast<uint32_t>(__bfloat16_as_ushort(lo)) |
+           (static_cast<uint32_t>(__bfloat16_as_ushort(hi)) << 16);
+}
+
+// Real operand: X (rows x cols, pitch ldx) -> NS planes (pitch ldo, a
+// multiple of 8).  The (row, 8-element group) pairs are flattened and
+// walked grid-stride, four groups per thread per step (eight 16-byte loads in
+// flight), each group written as one 16-byte store per plane.  NS is a
+// template parameter and the slices are packed with integer ops, so nothing
+// is indexed dynamically (no local memory).
+template <int NS>
+static __global__ void split_bf16_kernel_t(const float* __restrict__ X, long long rows, long long cols,
+                                           long long ldx, BfPlanes out, long long ldo,
+                                           long long x_bstride, long long o_bstride) {
+    constexpr int U = 4;
     const float* Xb = X + blockIdx.y * x_bstride;
     const long long cq = (cols + 7) / 8;
+    const long long total = rows * cq;
     const bool vec_in = (ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(Xb) & 15) == 0);
-    for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
-        const float* xr = Xb + r * ldx;
-        for (long long q0 = threadIdx.x; q0 < cq; q0 += 2 * blockDim.x) {
-            float v[2][8];
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long e0 = blockIdx.x * (long long)blockDim.x + threadIdx.x; e0 < total; e0 += U * stride) {
+        float v[U][8];
+        long long rr[U], cc[U];
 #pragma unroll
-            for (int u = 0; u < 2; ++u) {
-                const long long c = (q0 + u * blockDim.x) * 8;
+        for (int u = 0; u < U; ++u) {
+            const long long e = e0 + u * stride;
+            rr[u] = -1;
+            cc[u] = 0;
+            if (e < total) {
+                const long long r = e / cq, c = (e - r * cq) * 8;
+                rr[u] = r;
+                cc[u] = c;
+                const float* xr = Xb + r * ldx;
                 if (vec_in && c + 7 < cols) {
-                    const float4 w0 = *reinterpret_cast<const float4*>(xr + c);
-                    const float4 w1 = *reinterpret_cast<const float4*>(xr + c + 4);
+                    const float4 w0 = __ldg(reinterpret_cast<const float4*>(xr + c));
+                    const float4 w1 = __ldg(reinterpret_cast<const float4*>(xr + c + 4));
                     v[u][0] = w0.x; v[u][1] = w0.y; v[u][2] = w0.z; v[u][3] = w0.w;
                     v[u][4] = w1.x; v[u][5] = w1.y; v[u][6] = w1.z; v[u][7] = w1.w;
                 } else {
@@ -65,42 +82,41 @@ static __global__ void split_bf16_kernel(const float* __restrict__ X, long long 
                     for (int j = 0; j < 8; ++j) v[u][j] = (c + j < cols) ? xr[c + j] : 0.f;
                 }
             }
+        }
 #pragma unroll
-            for (int u = 0; u < 2; ++u) {
-                const long long q = q0 + u * blockDim.x;
-                if (q >= cq) break;
-                const long long c = q * 8;
-                __nv_bfloat16 o[8][3];
+        for (int u = 0; u < U; ++u) {
+            if (rr[u] < 0) break;
+            uint32_t pk[NS][4];
 #pragma unroll
-                for (int j = 0; j < 8; ++j) split_n(v[u][j], ns, o[j]);
-                for (int s = 0; s < ns; ++s) {
-                    __nv_bfloat16* dst = out.p[s] + blockIdx.y * o_bstride + r * ldo + c;
-                    if (c + 7 < ldo) {
-                        __align__(16) __nv_bfloat16 w[8];
+            for (int j = 0; j < 8; j += 2) {
+                __nv_bfloat16 a[3], b[3];
+                split_n(v[u][j], NS, a);
+                split_n(v[u][j + 1], NS, b);
 #pragma unroll
-                        for (int j = 0; j < 8; ++j) w[j] = o[j][s];
-                        *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(w);
-                    } else {
-                        for (int j = 0; j < 8 && c + j < ldo; ++j) dst[j] = o[j][s];
-                    }
-                }
+                for (int s = 0; s < NS; ++s) pk[s][j / 2] = pack_bf16x2(a[s], b[s]);
             }
+            const long long off = blockIdx.y * o_bstride + rr[u] * ldo + cc[u];
+#pragma unroll
+            for (int s = 0; s < NS; ++s)
+                *reinterpret_cast<uint4*>(out.p[s] + off) = make_uint4(pk[s][0], pk[s][1], pk[s][2], pk[s][3]);
         }
     }
 }
 
 // Complex A (M x K, interleaved) -> real-embedded A' = [Ar | Ai] (M x 2K).
+template <int NS>
 static __global__ void split_bf16_cplx_a_kernel(const float2* __restrict__ A, long long M, long long K,
-                                                long long lda, BfPlanes out, long long ldo, int ns) {
+                                                long long lda, BfPlanes out, long long ldo) {
     const long long total = M * K;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
          e += (long long)gridDim.x * blockDim.x) {
         long long r = e / K, c = e - r * K;
         float2 v = A[r * lda + c];
         __nv_bfloat16 ore[3], oim[3];
-        split_n(v.x, ns, ore);
-        split_n(v.y, ns, oim);
-        for (int s = 0; s < ns; ++s) {
+        split_n(v.x, NS, ore);
+        split_n(v.y, NS, oim);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
             out.p[s][r * ldo + c] = ore[s];
             out.p[s][r * ldo + K + c] = oim[s];
         }
@@ -108,17 +124,19 @@ static __global__ void split_bf16_cplx_a_kernel(const float2* __restrict__ A, lo
 }
 
 // Complex B (K x N) -> B' = [[Br, Bi], [-Bi, Br]] (2K x 2N).
+template <int NS>
 static __global__ void split_bf16_cplx_b_kernel(const float2* __restrict__ B, long long K, long long N,
-                                                long long ldb, BfPlanes out, long long ldo, int ns) {
+                                                long long ldb, BfPlanes out, long long ldo) {
     const long long total = K * N;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
          e += (long long)gridDim.x * blockDim.x) {
         long long r = e / N, c = e - r * N;
         float2 v = B[r * ldb + c];
         __nv_bfloat16 ore[3], oim[3];
-        split_n(v.x, ns, ore);
-        split_n(v.y, ns, oim);
-        for (int s = 0; s < ns; ++s) {
+        split_n(v.x, NS, ore);
+        split_n(v.y, NS, oim);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
             __nv_bfloat16* P = out.p[s];
             P[r * ldo + c] = ore[s];             // top-left      Br
             P[r * ldo + N + c] = oim[s];         // top-right     Bi
