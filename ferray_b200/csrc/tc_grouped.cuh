@@ -113,8 +113,9 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
         if (elect_one()) {
             int stage = 0;
             uint32_t phase = 0;
-            int issued_parity[Cfg::STAGES];
-            for (int i = 0; i < Cfg::STAGES; ++i) issued_parity[i] = -1;
+            // per stage: a load was issued (bit) and its phase parity (bit),
+            // kept in registers
+            uint32_t issued_mask = 0, issued_par = 0;
             bool ok = true;
             for (long long t = blockIdx.x; t < g.total_tiles && ok; t += gridDim.x) {
                 const TileRec tr = g.tiles[t];
@@ -141,7 +142,8 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
                             tma_load_2d(s.b[stage][i] + c * Cfg::B_CHUNK_BYTES, mp + Cfg::NA + i,
                                         tn * Cfg::BN + c * Cfg::B_CHUNK_ELEMS, kx, &s.full[stage]);
                     }
-                    issued_parity[stage] = static_cast<int>(phase);
+                    issued_mask |= 1u << stage;
+                    issued_par = (issued_par & ~(1u << stage)) | (phase << stage);
                     if (++stage == Cfg::STAGES) {
                         stage = 0;
                         phase ^= 1u;
@@ -150,9 +152,9 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
             }
             if (!ok) {
                 for (int i = 0; i < Cfg::STAGES; ++i) {
-                    if (issued_parity[i] < 0) continue;
+                    if (!((issued_mask >> i) & 1u)) continue;
                     volatile int never = 0;
-                    mbar_wait(&s.full[i], static_cast<uint32_t>(issued_parity[i]), g.timeout_ns, nullptr, 0, &never);
+                    mbar_wait(&s.full[i], (issued_par >> i) & 1u, g.timeout_ns, nullptr, 0, &never);
                 }
             }
         }
