@@ -325,6 +325,34 @@ def side_measurements(fg, L, lib, ctx, stream, n, only=""):
         res["quantized_u8i8_%d" % n] = {"tops": round(2.0 * n ** 3 / ms / 1e9, 1), "ms": round(ms, 4)}
         del a16, b16, c32, au, bq, cf
         torch.cuda.empty_cache()
+    if not only or only == "half":
+        # --- bf16 x bf16 / f16 x f16 -> f32 straight on tcgen05 (gemm_bf16_f32 /
+        # gemm_f16_f32), against the measured BF16 peak; error vs DD of the
+        # widened operands on a sampled block
+        bf16_peak, _, _ = peaks()
+        r2 = np.random.default_rng(SEED + 1)
+        af = r2.standard_normal((n, n), dtype=np.float32)
+        bf_ = r2.standard_normal((n, n), dtype=np.float32)
+        hv = {}
+        for name, fn in (("bf16", lib.fg_gemm_bf16_f32), ("f16", lib.fg_gemm_f16_f32)):
+            if name == "bf16":
+                ah = ((af.view(np.uint32) + 0x7FFF + ((af.view(np.uint32) >> 16) & 1)) >> 16).astype(np.uint16)
+                bh = ((bf_.view(np.uint32) + 0x7FFF + ((bf_.view(np.uint32) >> 16) & 1)) >> 16).astype(np.uint16)
+                aw, bw = oracle.bf16_to_f32(ah), oracle.bf16_to_f32(bh)
+            else:
+                ah, bh = af.astype(np.float16).view(np.uint16), bf_.astype(np.float16).view(np.uint16)
+                aw, bw = ah.view(np.float16).astype(np.float32), bh.view(np.float16).astype(np.float32)
+            da, db = fg.DeviceArray.from_numpy(ah, ctx), fg.DeviceArray.from_numpy(bh, ctx)
+            dc = fg.DeviceArray((n, n), np.float32, ctx)
+            ms = _time_calls(torch, stream, lambda: fn(ctx.handle, n, n, n, da.ptr, db.ptr, dc.ptr, 0, sh), 10, 3)
+            rows, cols = oracle.sample_indices(n, n, 48, 48, seed=17)
+            err = oracle.normwise_error(dc.to_numpy()[np.ix_(rows, cols)], oracle.dd_sampled(aw, bw, rows, cols),
+                                        n, n, oracle.fro(aw), oracle.fro(bw))
+            tf = 2.0 * n ** 3 / ms / 1e9
+            hv[name] = {"tflops": round(tf, 1), "ms": round(ms, 4), "frac_of_measured_bf16": round(tf / bf16_peak, 3),
+                        "normwise_err_vs_widened": err}
+            del da, db, dc
+        res["half_f32_%d" % n] = hv
     if only == "ozaki":
         # --- DGEMM / ZGEMM plain vs Ozaki INT8 per exponent spread and slice
         # count: A = diag(10^(s u)) G diag(10^(s v)), B built the same way

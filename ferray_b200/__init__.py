@@ -28,7 +28,7 @@ __all__ = [
     "FerrayError", "ShapeMismatch", "BroadcastFailure", "InvalidDtype", "InvalidValue",
     "OutOfMemory", "BudgetExceeded", "DeviceTimeout", "DeviceError", "Context", "DeviceArray",
     "default_context", "gemm_f64", "gemm_f32", "gemm_c64", "gemm_c32", "gemm_i8",
-    "gemm_i8_signed", "gemm_i16", "quantized_matmul", "matmul", "matmul_complex",
+    "gemm_i8_signed", "gemm_i16", "gemm_bf16_f32", "gemm_f16_f32", "quantized_matmul", "matmul", "matmul_complex",
     "gemm_batched_strided", "gemm_grouped", "GroupedPlan", "Server", "launch_count", "PLAIN",
     "SPLIT", "TUNE_OPS", "tune_lookup", "tune_forced",
 ]
@@ -142,7 +142,7 @@ _NP2FG = {np.dtype(np.float64): L.FG_F64, np.dtype(np.float32): L.FG_F32,
           np.dtype(np.int8): L.FG_I8, np.dtype(np.int16): L.FG_I16}
 _OUT_DTYPE = {L.FG_F64: np.float64, L.FG_F32: np.float32, L.FG_C64: np.complex128,
               L.FG_C32: np.complex64, L.FG_I8: np.int32, L.FG_U8I8: np.int32,
-              L.FG_I16: np.int32}
+              L.FG_I16: np.int32, L.FG_BF16: np.float32, L.FG_F16: np.float32}
 
 
 def _mode(mode):
@@ -297,6 +297,24 @@ def gemm_i16(m, n, k, a, b, c, accumulate=False):
     _need(a, m * k, np.int16, "a"); _need(b, k * n, np.int16, "b"); _need(c, m * n, np.int32, "c")
     return _run_gemm(L.FG_I16, PLAIN, 0, m, n, k, [0.0], a, b, [0.0], c, accumulate,
                      C.c_double)
+
+
+def gemm_bf16_f32(m, n, k, a, b, c, accumulate=False):
+    """bf16 x bf16 -> f32 (gemm/mod.rs:851); a, b are uint16 arrays of bf16
+    bit patterns (NumPy has no bf16 dtype), c float32."""
+    _need(a, m * k, np.uint16, "a"); _need(b, k * n, np.uint16, "b"); _need(c, m * n, np.float32, "c")
+    return _run_gemm(L.FG_BF16, PLAIN, 0, m, n, k, [0.0], a, b, [0.0], c, accumulate, C.c_double)
+
+
+def gemm_f16_f32(m, n, k, a, b, c, accumulate=False):
+    """f16 x f16 -> f32 (gemm/mod.rs:906); a, b float16 (or their uint16
+    bit patterns), c float32."""
+    a = a if _is_dev(a) else np.ascontiguousarray(a).view(np.uint16)
+    b = b if _is_dev(b) else np.ascontiguousarray(b).view(np.uint16)
+    _need(a, m * k, np.uint16 if not _is_dev(a) else a.dtype, "a")
+    _need(b, k * n, np.uint16 if not _is_dev(b) else b.dtype, "b")
+    _need(c, m * n, np.float32, "c")
+    return _run_gemm(L.FG_F16, PLAIN, 0, m, n, k, [0.0], a, b, [0.0], c, accumulate, C.c_double)
 
 
 def quantized_matmul(m, n, k, a, a_zp, scale_a, b, b_zp, scale_b, c, accumulate=False):

@@ -22,7 +22,7 @@ FG_ERR_UNSUPPORTED = 8
 FG_ERR_BROADCAST = 9
 
 # fg_dtype
-FG_F64, FG_F32, FG_C64, FG_C32, FG_I8, FG_U8I8, FG_I16 = range(7)
+FG_F64, FG_F32, FG_C64, FG_C32, FG_I8, FG_U8I8, FG_I16, FG_BF16, FG_F16 = range(9)
 # fg_mode
 FG_MODE_PLAIN, FG_MODE_SPLIT = 0, 1
 
@@ -82,6 +82,8 @@ SIGNATURES = {
     "fg_gemm_i8_signed": (_i, [_p, _sz, _sz, _sz, _p, _p, _p, _i, _p]),
     "fg_gemm_i8": (_i, [_p, _sz, _sz, _sz, _p, _p, _p, _i, _p]),
     "fg_gemm_i16": (_i, [_p, _sz, _sz, _sz, _p, _p, _p, _i, _p]),
+    "fg_gemm_bf16_f32": (_i, [_p, _sz, _sz, _sz, _p, _p, _p, _i, _p]),
+    "fg_gemm_f16_f32": (_i, [_p, _sz, _sz, _sz, _p, _p, _p, _i, _p]),
     "fg_quantized_matmul": (_i, [_p, _sz, _sz, _sz, _p, C.c_uint8, _f, _p, C.c_int8, _f, _p,
                                  _i, _p]),
     "fg_quantized_matmul_noalloc": (_i, [_p, _sz, _sz, _sz, _p, C.c_uint8, _f, _p, C.c_int8, _f,

@@ -152,11 +152,14 @@ fg_status run_gemm(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
         case FG_U8I8:
         case FG_I16:
             return launch_int_tc(ctx, g, st);
+        case FG_BF16:
+        case FG_F16:
+            return launch_half_tc(ctx, g, st);
     }
     return set_error(FG_ERR_DTYPE, "unknown dtype");
 }
 
-static bool valid_dtype(fg_dtype d) { return d >= FG_F64 && d <= FG_I16; }
+static bool valid_dtype(fg_dtype d) { return d >= FG_F64 && d <= FG_F16; }
 
 static void set_scalars(Gemm& g, const void* alpha, const void* beta) {
     switch (g.dtype) {
@@ -443,6 +446,18 @@ fg_status fg_gemm_i8(fg_ctx* ctx, size_t m, size_t n, size_t k, const uint8_t* a
 fg_status fg_gemm_i16(fg_ctx* ctx, size_t m, size_t n, size_t k, const int16_t* a,
                       const int16_t* b, int32_t* c, int accumulate, fg_stream stream) {
     return fg_gemm(ctx, FG_I16, FG_MODE_PLAIN, 0, m, n, k, nullptr, a, k, b, n, nullptr, c, n,
+                   accumulate, stream);
+}
+
+fg_status fg_gemm_bf16_f32(fg_ctx* ctx, size_t m, size_t n, size_t k, const uint16_t* a,
+                           const uint16_t* b, float* c, int accumulate, fg_stream stream) {
+    return fg_gemm(ctx, FG_BF16, FG_MODE_PLAIN, 0, m, n, k, nullptr, a, k, b, n, nullptr, c, n,
+                   accumulate, stream);
+}
+
+fg_status fg_gemm_f16_f32(fg_ctx* ctx, size_t m, size_t n, size_t k, const uint16_t* a,
+                          const uint16_t* b, float* c, int accumulate, fg_stream stream) {
+    return fg_gemm(ctx, FG_F16, FG_MODE_PLAIN, 0, m, n, k, nullptr, a, k, b, n, nullptr, c, n,
                    accumulate, stream);
 }
 

@@ -36,16 +36,31 @@ using CfgBf16x3 = TcCfg<KIND_BF16, 128, 3, 2, 2, 1, 3, EPI_F32, 1>;
 using CfgBf16x3n64 = TcCfg<KIND_BF16, 64, 4, 2, 2, 1, 3, EPI_F32, 1>;
 // 256 x 128 tiles on CTA pairs, 4 stages of 48 KB per CTA.
 using CfgBf16x3Pair = Tc2Cfg<KIND_BF16, 128, 4, 2, 2, 1, 3, EPI_F32, 1>;
+// bf16 / f16 operands as given (one product): 128 x 128 single-CTA tiles with
+// 6 stages of 32 KB, or 256 x 128 CTA-pair tiles with 8 stages of 24 KB per CTA.
+using CfgHalf = TcCfg<KIND_BF16, 128, 6, 1, 1, 1, 1, EPI_F32, 1>;
+using CfgHalfPair = Tc2Cfg<KIND_BF16, 128, 8, 1, 1, 1, 1, EPI_F32, 1>;
 // 6 products (3 slices) on CTA pairs: 256 x 128 tiles, 3 stages of 72 KB per
 // CTA, hi*hi and the corrections in two TMEM accumulators.
 using CfgBf16x6Pair = Tc2Cfg<KIND_BF16, 128, 3, 3, 3, 2, 6, EPI_F32, 1>;
 using CfgBf16x6 = TcCfg<KIND_BF16, 128, 2, 3, 3, 2, 6, EPI_F32, 1>;
 
+// K blocks per TMEM accumulation chunk of the one-product bf16 / f16 GEMM
+// (its MMAs are 3x shorter per K block than the split form's, so its chunks
+// are longer to keep the epilogue's chunk sums off the critical path).
+static int half_kchunk() {
+    static int v = [] {
+        const char* e = getenv("FG_HALF_KCHUNK");
+        return e ? atoi(e) : 8;
+    }();
+    return v;
+}
+
 // K blocks (64 bf16 each) per TMEM accumulation chunk of the split SGEMM.
 static int split_kchunk() {
     static int v = [] {
         const char* e = getenv("FG_SPLIT_KCHUNK");
-        return e ? atoi(e) : 2;
+        return e ? atoi(e) : 4;
     }();
     return v;
 }
@@ -55,8 +70,11 @@ static unsigned long long kTimeoutNs = 4000000000ull;  // 4 s per wait
 template <class Cfg>
 static const char* cfg_name() {
     if (Cfg::BM == 256)
-        return Cfg::KIND == KIND_BF16 ? (Cfg::NOPS == 6 ? "tc_gemm2_6xbf16" : "tc_gemm2_3xbf16") : "tc_gemm2_i8";
-    if (Cfg::KIND == KIND_BF16) return Cfg::NOPS == 6 ? "tc_gemm_6xbf16" : "tc_gemm_3xbf16";
+        return Cfg::KIND == KIND_BF16
+                   ? (Cfg::NOPS == 6 ? "tc_gemm2_6xbf16" : Cfg::NOPS == 3 ? "tc_gemm2_3xbf16" : "tc_gemm2_f16")
+                   : "tc_gemm2_i8";
+    if (Cfg::KIND == KIND_BF16)
+        return Cfg::NOPS == 6 ? "tc_gemm_6xbf16" : Cfg::NOPS == 3 ? "tc_gemm_3xbf16" : "tc_gemm_f16";
     if (Cfg::EPI == EPI_I16) return "tc_gemm_i16";
     if (Cfg::EPI == EPI_QMM) return "tc_gemm_qmm";
     return "tc_gemm_i8";
@@ -378,6 +396,49 @@ fg_status launch_qmm(fg_ctx* ctx, long long M, long long N, long long K, const u
         return launch_pair<CfgQmmPair>(ctx, maps, args, st);
     }
     return launch_cfg<CfgQmm>(ctx, maps, args, st);
+}
+
+// bf16 x bf16 / f16 x f16 -> f32 straight from the caller's 16-bit operands
+// (gemm/mod.rs:851-933 widen them to f32 for an SGEMM): one tcgen05 kind::f16
+// product per K block, K accumulated in TMEM chunks summed in FP32
+// registers (round to nearest) like the split SGEMM; C = A@B, or C += A@B
+// when accumulating.
+fg_status launch_half_tc(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
+    const CUtensorMapDataType tdt =
+        g.dtype == FG_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+    const int fmt = g.dtype == FG_BF16 ? 1 : 0;  // kind::f16 operand format (0 F16, 1 BF16)
+    Scratch sa, sb;
+    const void *pa, *pb;
+    long long lda, ldb, msa, msb;
+    FG_TRY(make_tma_operand(g.A, g.M, g.K, g.lda, g.a_count, g.a_mstride, 2, sa, &pa, &lda, &msa, st));
+    FG_TRY(make_tma_operand(g.B, g.K, g.N, g.ldb, g.b_count, g.b_mstride, 2, sb, &pb, &ldb, &msb, st));
+    TcMaps maps;
+    TcArgs args{};
+    FG_TRY(operand_map(&maps.a[0], tdt, pa, g.K, g.M, lda * 2, g.a_count, msa * 2, 64, 128, &args.a_rank3));
+    FG_TRY(operand_map(&maps.b[0], tdt, pb, g.N, g.K, ldb * 2, g.b_count, msb * 2, 64, 64, &args.b_rank3));
+    args.M = static_cast<int>(g.M);
+    args.N = static_cast<int>(g.N);
+    args.K = static_cast<int>(g.K);
+    args.tiles_m = static_cast<int>((g.M + 127) / 128);
+    args.k_blocks = static_cast<int>((g.K + CfgHalf::BK - 1) / CfgHalf::BK);
+    args.C = g.C;
+    args.ldc = g.ldc;
+    args.alpha = 1.f;
+    args.beta = g.accumulate ? 1.f : 0.f;
+    fill_batch(g, args);
+    args.kchunk = half_kchunk();
+    args.ops[0] = TcOp{0, 0, 0, fmt, fmt};
+    float* C = static_cast<float*>(g.C);
+    const TuneChoice c = tune_lookup(TUNE_SPLIT_F32, g.M, g.N, g.K);
+    if (c.variant == 2) {
+        args.tiles_m = static_cast<int>((g.M + CfgHalfPair::BM - 1) / CfgHalfPair::BM);
+        args.tiles_n = static_cast<int>((g.N + CfgHalfPair::BN - 1) / CfgHalfPair::BN);
+        return launch_splitk<CfgHalfPair, float>(ctx, maps, args, c.splits, C, g.ldc, g.c_stride, 1.f,
+                                                 args.beta, 0, st);
+    }
+    args.tiles_n = static_cast<int>((g.N + CfgHalf::BN - 1) / CfgHalf::BN);
+    return launch_splitk<CfgHalf, float>(ctx, maps, args, c.splits, C, g.ldc, g.c_stride, 1.f, args.beta, 0,
+                                         st);
 }
 
 // 3xBF16: C = alpha * (Alo*Bhi + Ahi*Blo + Ahi*Bhi) + beta * C, f32 accumulate.

@@ -110,17 +110,21 @@ inline size_t in_size(fg_dtype d) {
         case FG_C32: return 8;
         case FG_I8: case FG_U8I8: return 1;
         case FG_I16: return 2;
+        case FG_BF16: case FG_F16: return 2;
     }
     return 0;
 }
 inline size_t out_size(fg_dtype d) {
     switch (d) {
         case FG_I8: case FG_U8I8: case FG_I16: return 4;
+        case FG_BF16: case FG_F16: return 4;
         default: return in_size(d);
     }
 }
 inline bool is_complex(fg_dtype d) { return d == FG_C64 || d == FG_C32; }
 inline bool is_integer(fg_dtype d) { return d == FG_I8 || d == FG_U8I8 || d == FG_I16; }
+// 16-bit float operands, f32 result, accumulate-flag semantics like the integers.
+inline bool is_half(fg_dtype d) { return d == FG_BF16 || d == FG_F16; }
 
 // One (possibly batched, possibly broadcast) GEMM after argument lowering.
 struct Gemm {
@@ -153,6 +157,7 @@ fg_status run_gemm(fg_ctx* ctx, const Gemm& g, cudaStream_t st);
 // Family launchers (gemm_tc.cu, gemm_simt.cu, gemm_ozaki.cu).
 fg_status launch_simt(fg_ctx* ctx, const Gemm& g, cudaStream_t st);
 fg_status launch_int_tc(fg_ctx* ctx, const Gemm& g, cudaStream_t st);
+fg_status launch_half_tc(fg_ctx* ctx, const Gemm& g, cudaStream_t st);
 fg_status launch_split_bf16(fg_ctx* ctx, const Gemm& g, cudaStream_t st);
 fg_status launch_ozaki(fg_ctx* ctx, const Gemm& g, cudaStream_t st);
 fg_status launch_qmm(fg_ctx* ctx, long long M, long long N, long long K, const uint8_t* a,

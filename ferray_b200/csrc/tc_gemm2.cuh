@@ -18,7 +18,8 @@
 //                frees stage s in both;
 //   acc_full[b]  each CTA: leader's commit (multicast) -> both epilogues;
 //   acc_empty[b] leader only: 4 epilogue warps of each CTA arrive (the
-//                peer's remotely) before accumulator b is reused.
+//                peer's remotely) before accumulator b is reused
+//                (up to 4 accumulator buffers when they fit in TMEM).
 // Loads carry no cluster multicast: each CTA reads its own half from HBM.
 // Every wait is bounded (timeout, abort flag) like the single-CTA kernel;
 // both CTAs meet at a cluster barrier before TMEM is freed.
@@ -47,7 +48,7 @@ struct Tc2Cfg {
     static constexpr int B_CHUNK_BYTES = BK * 128;
     static constexpr int STAGE_BYTES = NA * A_TILE + NB * B_TILE;  // per CTA
     static constexpr int ACC_COLS = NACC * BN;                     // per CTA
-    static constexpr int ACC_BUFS = (2 * ACC_COLS <= 512) ? 2 : 1;
+    static constexpr int ACC_BUFS = (4 * ACC_COLS <= 512) ? 4 : (2 * ACC_COLS <= 512) ? 2 : 1;
     static constexpr int TMEM_COLS = 512;
     static constexpr int THREADS = 192;
     static_assert(ACC_COLS <= 512, "accumulators exceed TMEM");
@@ -61,8 +62,8 @@ struct Tc2Smem {
     alignas(1024) uint8_t b[Cfg::STAGES][Cfg::NB][Cfg::B_TILE];
     uint64_t full[Cfg::STAGES];
     uint64_t empty[Cfg::STAGES];
-    uint64_t acc_full[2];
-    uint64_t acc_empty[2];
+    uint64_t acc_full[4];
+    uint64_t acc_empty[4];
     uint64_t drain;
     uint32_t tmem_base;
     int abort;
@@ -103,7 +104,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Cfg::THREADS, 1)
             mbar_init(&s.full[i], 1);
             mbar_init(&s.empty[i], 1);
         }
-        for (int i = 0; i < 2; ++i) {
+        for (int i = 0; i < 4; ++i) {
             mbar_init(&s.acc_full[i], 1);
             mbar_init(&s.acc_empty[i], 8);  // 4 epilogue warps x 2 CTAs
         }

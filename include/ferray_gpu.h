@@ -59,7 +59,9 @@ typedef enum fg_dtype {
     FG_C32 = 3,  /* Complex<f32> (8 bytes)  */
     FG_I8 = 4,   /* i8 x i8 -> i32          */
     FG_U8I8 = 5, /* u8 x i8 -> i32          */
-    FG_I16 = 6   /* i16 x i16 -> i32        */
+    FG_I16 = 6,  /* i16 x i16 -> i32        */
+    FG_BF16 = 7, /* bf16 x bf16 -> f32 (raw 16-bit patterns) */
+    FG_F16 = 8   /* f16 x f16 -> f32 (IEEE binary16)         */
 } fg_dtype;
 
 typedef enum fg_mode {
@@ -172,6 +174,15 @@ fg_status fg_gemm_i8(fg_ctx *ctx, size_t m, size_t n, size_t k, const uint8_t *a
 /* i16 x i16 -> i32, wrapping.  Replaces gemm_i16 (gemm/mod.rs:348-392). */
 fg_status fg_gemm_i16(fg_ctx *ctx, size_t m, size_t n, size_t k, const int16_t *a,
                       const int16_t *b, int32_t *c, int accumulate, fg_stream stream);
+/* C = A@B (C += A@B when accumulate), bf16 x bf16 -> f32, on tcgen05
+ * kind::f16 with FP32 accumulation straight from the 16-bit operands.
+ * Replaces gemm_bf16_f32 (gemm/mod.rs:851-882; ferray widens to f32 and runs
+ * its SGEMM).  a, b hold bf16 bit patterns. */
+fg_status fg_gemm_bf16_f32(fg_ctx *ctx, size_t m, size_t n, size_t k, const uint16_t *a,
+                           const uint16_t *b, float *c, int accumulate, fg_stream stream);
+/* Same for IEEE f16 operands.  Replaces gemm_f16_f32 (gemm/mod.rs:906-933). */
+fg_status fg_gemm_f16_f32(fg_ctx *ctx, size_t m, size_t n, size_t k, const uint16_t *a,
+                          const uint16_t *b, float *c, int accumulate, fg_stream stream);
 /* scale_a*scale_b*sum((a-a_zp)*(b-b_zp)) -> f32, zero points and scale fused
  * into the i8 kernel's epilogue.  Replaces quantized_matmul
  * (gemm/mod.rs:484-575). */

@@ -94,6 +94,24 @@ def gemm_f32(a, b, alpha=1.0, beta=0.0, c=None):
     return c
 
 
+def bf16_to_f32(bits):
+    """bf16 bit patterns (uint16) -> f32, exact (the `half` crate's widening)."""
+    return (np.asarray(bits, np.uint16).astype(np.uint32) << 16).view(np.float32)
+
+
+def gemm_bf16_f32(a_bits, b_bits, c=None, accumulate=False):
+    """gemm/mod.rs:851-882: widen both bf16 operands to f32 (exact), then the
+    SGEMM with beta = 1 when accumulating, 0 otherwise."""
+    return gemm_f32(bf16_to_f32(a_bits), bf16_to_f32(b_bits), 1.0, 1.0 if accumulate else 0.0, c)
+
+
+def gemm_f16_f32(a, b, c=None, accumulate=False):
+    """gemm/mod.rs:906-933: widen f16 -> f32 (exact), then the SGEMM."""
+    a = np.asarray(a, np.float16).astype(np.float32)
+    b = np.asarray(b, np.float16).astype(np.float32)
+    return gemm_f32(a, b, 1.0, 1.0 if accumulate else 0.0, c)
+
+
 def gemm_complex(a, b, alpha=1.0 + 0j, beta=0j, c=None):
     """c64 (complex128) or c32 (complex64) according to a.dtype."""
     m, k = a.shape

@@ -401,3 +401,51 @@ def test_matmul_vector_operands_use_gemv(fg):
     np.testing.assert_allclose(got, a @ v, rtol=0, atol=700 * U64 * 30)
     got = fg.matmul(dw, da).to_numpy()
     np.testing.assert_allclose(got, w @ a, rtol=0, atol=513 * U64 * 30)
+
+
+# ------------------------------------------------------- bf16 / f16 -> f32
+def _bf16_bits(x):
+    """round-to-nearest-even f32 -> bf16 bit patterns"""
+    u = x.astype(np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) >> 16
+    return u.astype(np.uint16)
+
+
+@pytest.mark.parametrize("kind", ["bf16", "f16"])
+@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (17, 13, 9), (128, 256, 128), (300, 257, 1000),
+                                   (513, 300, 2048), (1024, 1024, 1024)])
+def test_half_gemm_f32(fg, oracle, kind, m, n, k):
+    r = rng(m + n + k)
+    af, bf = r.standard_normal((m, k)), r.standard_normal((k, n))
+    if kind == "bf16":
+        a, b = _bf16_bits(af), _bf16_bits(bf)
+        aw, bw = oracle.bf16_to_f32(a), oracle.bf16_to_f32(b)
+        gemm, ref = fg.gemm_bf16_f32, oracle.gemm_bf16_f32
+    else:
+        a, b = af.astype(np.float16), bf.astype(np.float16)
+        aw, bw = a.astype(np.float32), b.astype(np.float32)
+        gemm, ref = fg.gemm_f16_f32, oracle.gemm_f16_f32
+    c = np.zeros((m, n), np.float32)
+    assert gemm(m, n, k, a, b, c)
+    err = _err(oracle, aw, bw, c)
+    assert err <= k * U32, err
+    ref_err = _err(oracle, aw, bw, ref(a, b))
+    assert err <= 2 * ref_err + 2.0 ** -21, (err, ref_err)
+    # accumulate: C += A @ B
+    c0 = r.standard_normal((m, n)).astype(np.float32)
+    c = c0.copy()
+    assert gemm(m, n, k, a, b, c, accumulate=True)
+    want = oracle.dd_full(aw, bw) + c0.astype(np.float64)
+    scale = np.linalg.norm(aw.astype(np.float64)) * np.linalg.norm(bw.astype(np.float64))
+    assert np.linalg.norm(c - want) <= (k + 4) * U32 * scale + 2 * U32 * np.linalg.norm(want)
+
+
+@pytest.mark.parametrize("variant,splits", [(0, 1), (2, 1), (0, 4), (2, 3)])
+def test_half_gemm_tile_variants(fg, oracle, variant, splits):
+    r = rng(5)
+    m, n, k = 300, 260, 3000
+    a, b = _bf16_bits(r.standard_normal((m, k))), _bf16_bits(r.standard_normal((k, n)))
+    c = np.zeros((m, n), np.float32)
+    with fg.tune_forced("split_f32", variant, splits):
+        assert fg.gemm_bf16_f32(m, n, k, a, b, c)
+    assert _err(oracle, oracle.bf16_to_f32(a), oracle.bf16_to_f32(b), c) <= k * U32

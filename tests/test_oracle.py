@@ -180,3 +180,20 @@ def test_normwise_sampling_consistent(oracle):
     full = oracle.normwise_error(c, oracle.dd_full(a, b), m, n, oracle.fro(a), oracle.fro(b))
     sampled = oracle.error_vs_dd(a, b, c)
     assert 0.5 < sampled / full < 2.0
+
+
+def test_half_restatements_widen_exactly(oracle):
+    rng = np.random.default_rng(11)
+    x = rng.standard_normal((7, 5)).astype(np.float32)
+    bits = (x.view(np.uint32) >> 16).astype(np.uint16)      # truncate to bf16
+    w = oracle.bf16_to_f32(bits)
+    assert np.all((w.view(np.uint32) & 0xFFFF) == 0)
+    assert np.all(np.abs(w - x) <= np.abs(x) * 2.0 ** -7)
+    a16 = rng.standard_normal((6, 9)).astype(np.float16)
+    b16 = rng.standard_normal((9, 4)).astype(np.float16)
+    got = oracle.gemm_f16_f32(a16, b16)
+    np.testing.assert_array_equal(got, oracle.gemm_f32(a16.astype(np.float32), b16.astype(np.float32)))
+    c0 = rng.standard_normal((6, 4)).astype(np.float32)
+    acc = oracle.gemm_f16_f32(a16, b16, c=c0.copy(), accumulate=True)
+    np.testing.assert_array_equal(acc, oracle.gemm_f32(a16.astype(np.float32), b16.astype(np.float32),
+                                                       1.0, 1.0, c0.copy()))
