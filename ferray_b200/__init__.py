@@ -30,7 +30,7 @@ __all__ = [
     "default_context", "gemm_f64", "gemm_f32", "gemm_c64", "gemm_c32", "gemm_i8",
     "gemm_i8_signed", "gemm_i16", "gemm_bf16_f32", "gemm_f16_f32", "quantized_matmul", "matmul", "matmul_complex",
     "gemm_batched_strided", "gemm_grouped", "GroupedPlan", "Server", "launch_count", "PLAIN",
-    "SPLIT", "TUNE_OPS", "tune_lookup", "tune_forced",
+    "SPLIT", "TUNE_OPS", "tune_lookup", "tune_forced", "multi_dot", "multi_dot_order", "matrix_power",
 ]
 
 PLAIN, SPLIT = "plain", "split"
@@ -401,6 +401,82 @@ def _table(problems):
         tab[i] = L.fg_problem(m, n, k, a.ptr if _is_dev(a) else a, b.ptr if _is_dev(b) else b,
                               c.ptr if _is_dev(c) else c, k, n, n)
     return tab
+
+
+def _chain_dims(arrays):
+    """dims of products/mod.rs:789-815: a 1-D first operand is 1 x n, a 1-D
+    last operand n x 1; every other operand must be 2-D and aligned.  (The
+    reference pushes a trailing vector's length twice, so its cost model sees
+    that vector as n x n; the product is the same, here the true n x 1 is
+    used.)"""
+    n = len(arrays)
+    dims = []
+    for i, x in enumerate(arrays):
+        sh = x.shape
+        if len(sh) != 2:
+            if i == 0 and len(sh) == 1:
+                dims += [1, sh[0]]
+                continue
+            if i == n - 1 and len(sh) == 1:
+                dims.append(1)
+                continue
+            raise ShapeMismatch(f"multi_dot: matrix {i} has {len(sh)} dimensions (expected 2)")
+        if i == 0:
+            dims.append(sh[0])
+        dims.append(sh[1])
+    for i in range(1, n):
+        prev, cur = arrays[i - 1].shape, arrays[i].shape
+        if prev[-1] != cur[0]:
+            raise ShapeMismatch(f"multi_dot: shapes of matrices {i - 1} and {i} not aligned "
+                                f"({prev[-1]} != {cur[0]})")
+    return dims
+
+
+def multi_dot(arrays, mode=PLAIN):
+    """Chain product of DeviceArrays in the reference's optimal order
+    (products/mod.rs:776); intermediates stay on the device."""
+    if len(arrays) < 2:
+        raise InvalidValue("multi_dot: need at least 2 matrices")
+    if len(arrays) == 2:
+        return matmul(arrays[0], arrays[1], mode)
+    dt = arrays[0].dtype
+    if any(x.dtype != dt for x in arrays):
+        raise InvalidDtype("multi_dot: all operands need the same dtype")
+    dims = _chain_dims(arrays)
+    n = len(arrays)
+    shape = [dims[0], dims[-1]]
+    if len(arrays[0].shape) == 1:
+        shape = shape[1:]
+    if len(arrays[-1].shape) == 1:
+        shape = shape[:-1]
+    ctx = arrays[0].ctx
+    out = DeviceArray(shape, dt, ctx)
+    mats = (C.c_void_p * n)(*[x.ptr for x in arrays])
+    cd = (C.c_int64 * (n + 1))(*dims)
+    check(ctx._lib.fg_multi_dot(ctx.handle, _NP2FG[np.dtype(dt)], _mode(mode), n, mats, cd, out.ptr, None),
+          "multi_dot")
+    ctx.sync()
+    return out
+
+
+def multi_dot_order(dims):
+    """The split table fg_multi_dot uses, as a (count x count) int array."""
+    n = len(dims) - 1
+    cd = (C.c_int64 * (n + 1))(*dims)
+    sp = (C.c_size_t * (n * n))()
+    check(L.load().fg_multi_dot_order(n, cd, sp), "multi_dot_order")
+    return np.array(sp[:], dtype=np.int64).reshape(n, n)
+
+
+def matrix_power(a, exponent, mode=PLAIN):
+    """A^exponent for a square 2-D DeviceArray (solve.rs:456)."""
+    if a.ndim != 2 or a.shape[0] != a.shape[1]:
+        raise ShapeMismatch(f"matrix_power requires a square matrix, got {'x'.join(map(str, a.shape))}")
+    out = DeviceArray(a.shape, a.dtype, a.ctx)
+    check(a.ctx._lib.fg_matrix_power(a.ctx.handle, _NP2FG[a.dtype], _mode(mode), a.shape[0], a.ptr,
+                                     int(exponent), out.ptr, None), "matrix_power")
+    a.ctx.sync()
+    return out
 
 
 TUNE_OPS = {"i8": 0, "split_f32": 1, "f64": 2, "f32": 3}

@@ -111,6 +111,25 @@ fg_status fg_device_info(fg_ctx *ctx, int *sm_count, int *cc_major, int *cc_mino
  * The same bounded wait guards every pipeline barrier of the GEMM kernels. */
 fg_status fg_selftest_wait_timeout(fg_ctx *ctx, uint32_t timeout_us, fg_stream stream);
 
+/* ------------------------------------------------------------ GEMM chains */
+/* multi_dot (products/mod.rs:776-902): mats[i] is a contiguous row-major
+ * dims[i] x dims[i+1] device matrix (a 1-D first / last operand is passed as
+ * 1 x n / n x 1, as the reference forms its dims), out is dims[0] x
+ * dims[count].  The product order is the reference's optimal
+ * parenthesisation (same dynamic programme, same tie-breaking); the
+ * intermediates stay on the device.  Errors: FG_ERR_INVALID for fewer than 2
+ * matrices, FG_ERR_SHAPE for non-positive dims. */
+fg_status fg_multi_dot(fg_ctx *ctx, fg_dtype dtype, fg_mode mode, size_t count,
+                       const void *const *mats, const int64_t *dims, void *out, fg_stream stream);
+/* The parenthesisation fg_multi_dot uses (host only): split[i*count + j] is
+ * the k at which the product of matrices i..j is split. */
+fg_status fg_multi_dot_order(size_t count, const int64_t *dims, size_t *split);
+/* A^exponent for a square n x n device matrix (solve.rs:456-494): identity
+ * for 0, exponentiation by squaring in the reference's order for > 0;
+ * negative powers need inv(A) and return FG_ERR_UNSUPPORTED. */
+fg_status fg_matrix_power(fg_ctx *ctx, fg_dtype dtype, fg_mode mode, size_t n, const void *a,
+                          int64_t exponent, void *out, fg_stream stream);
+
 /* ------------------------------------------------------------ autotune */
 /* Tile variant and split-K count per GEMM family come from a table indexed
  * by the size buckets of m, n, k (<=16, <=32, ..., <=4096, >4096), written

@@ -94,6 +94,54 @@ def gemm_f32(a, b, alpha=1.0, beta=0.0, c=None):
     return c
 
 
+def chain_order(dims):
+    """products/mod.rs:839-855: optimal chain parenthesisation, u64 costs,
+    the first k reaching the minimum wins; split[i][j] = k."""
+    n = len(dims) - 1
+    cost = [[0] * n for _ in range(n)]
+    split = [[0] * n for _ in range(n)]
+    for length in range(2, n + 1):
+        for i in range(0, n - length + 1):
+            j = i + length - 1
+            cost[i][j] = 2 ** 64 - 1
+            for k in range(i, j):
+                q = cost[i][k] + cost[k + 1][j] + dims[i] * dims[k + 1] * dims[j + 1]
+                if q < cost[i][j]:
+                    cost[i][j] = q
+                    split[i][j] = k
+    return np.array(split, dtype=np.int64)
+
+
+def multi_dot(arrays):
+    """products/mod.rs:858-902: multiply along chain_order with the restated
+    GEMM (f64 / f32 by dtype)."""
+    dims = [arrays[0].shape[0]] + [x.shape[1] for x in arrays]
+    split = chain_order(dims)
+    mm = gemm_f64 if arrays[0].dtype == np.float64 else gemm_f32
+
+    def prod(i, j):
+        if i == j:
+            return arrays[i]
+        k = split[i][j]
+        return mm(prod(i, k), prod(k + 1, j))
+    return prod(0, len(arrays) - 1)
+
+
+def matrix_power(a, n):
+    """solve.rs:478-491 for n > 0: result = I; result @= base on set bits;
+    base = base @ base (the restated GEMM)."""
+    mm = gemm_f64 if a.dtype == np.float64 else gemm_f32
+    result = np.eye(a.shape[0], dtype=a.dtype)
+    base = a.copy()
+    p = n
+    while p > 0:
+        if p & 1:
+            result = mm(result, base)
+        base = mm(base, base)
+        p >>= 1
+    return result
+
+
 def bf16_to_f32(bits):
     """bf16 bit patterns (uint16) -> f32, exact (the `half` crate's widening)."""
     return (np.asarray(bits, np.uint16).astype(np.uint32) << 16).view(np.float32)

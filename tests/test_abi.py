@@ -101,3 +101,20 @@ def test_tune_table_lookup_and_force_without_device():
             idx = ((oi * autotune.BUCKETS + bm) * autotune.BUCKETS + bn) * autotune.BUCKETS + bk
             m, nn, k = (autotune.REPR[b] for b in (bm, bn, bk))
             assert fg.tune_lookup(op, m, nn, k) == entries[idx]
+
+
+def test_multi_dot_order_matches_the_reference_programme():
+    """The parenthesisation is host logic: fg_multi_dot_order against the
+    restated dynamic programme of products/mod.rs:839-855."""
+    import numpy as np
+    import oracle
+    import ferray_b200 as fg
+    rng = np.random.default_rng(3)
+    for trial in range(40):
+        n = int(rng.integers(2, 9))
+        dims = [int(x) for x in rng.integers(1, 600, n + 1)]
+        want = oracle.chain_order(dims)
+        got = fg.multi_dot_order(dims)
+        np.testing.assert_array_equal(np.triu(got, 1), np.triu(want, 1))
+    # ties keep the first split (all-equal dims)
+    assert fg.multi_dot_order([4, 4, 4, 4])[0][2] == oracle.chain_order([4, 4, 4, 4])[0][2]

@@ -1,0 +1,62 @@
+"""multi_dot and matrix_power on device-resident operands against the
+restated reference (same product order), within the chained GEMM bound."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+U64, U32 = 2.0 ** -53, 2.0 ** -24
+
+
+@pytest.mark.parametrize("dt,u", [(np.float64, U64), (np.float32, U32)])
+@pytest.mark.parametrize("dims", [[30, 400, 5, 300], [7, 200, 200, 3, 150, 60], [300, 300, 300, 300, 300]])
+def test_multi_dot(fg, oracle, dt, u, dims):
+    rng = np.random.default_rng(sum(dims))
+    mats = [rng.uniform(-1, 1, (dims[i], dims[i + 1])).astype(dt) for i in range(len(dims) - 1)]
+    got = fg.multi_dot([fg.DeviceArray.from_numpy(x) for x in mats]).to_numpy()
+    want = oracle.multi_dot(mats)
+    exact = mats[0].astype(np.float64)
+    for x in mats[1:]:
+        exact = exact @ x.astype(np.float64)
+    scale = np.prod([np.linalg.norm(x.astype(np.float64)) for x in mats])
+    kk = sum(dims)
+    assert np.linalg.norm(got - exact) / scale <= kk * u
+    assert np.linalg.norm(got - exact) <= 2 * np.linalg.norm(want - exact) + kk * u * scale
+
+
+def test_multi_dot_vector_ends_and_errors(fg):
+    rng = np.random.default_rng(1)
+    v = rng.standard_normal(50)
+    a = rng.standard_normal((50, 40))
+    b = rng.standard_normal((40, 30))
+    w = rng.standard_normal(30)
+    dv, da, db, dw = (fg.DeviceArray.from_numpy(x) for x in (v, a, b, w))
+    got = fg.multi_dot([dv, da, db, dw]).to_numpy()
+    assert got.shape == ()
+    np.testing.assert_allclose(got, v @ a @ b @ w, rtol=1e-12, atol=1e-12)
+    with pytest.raises(fg.ShapeMismatch):
+        fg.multi_dot([da, da, db])
+    with pytest.raises(fg.InvalidValue):
+        fg.multi_dot([da])
+
+
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+@pytest.mark.parametrize("p", [0, 1, 2, 3, 7, 10])
+def test_matrix_power(fg, oracle, dt, p):
+    rng = np.random.default_rng(p)
+    n = 64
+    a = (rng.uniform(-1, 1, (n, n)) / np.sqrt(n)).astype(dt)
+    got = fg.matrix_power(fg.DeviceArray.from_numpy(a), p).to_numpy()
+    want = oracle.matrix_power(a, p)
+    exact = np.linalg.matrix_power(a.astype(np.float64), p)
+    tol = (1e-12 if dt == np.float64 else 1e-4) * max(1, p)
+    assert np.max(np.abs(got - exact)) <= tol
+    assert np.max(np.abs(got - exact)) <= 2 * np.max(np.abs(want - exact)) + tol / 10
+
+
+def test_matrix_power_errors(fg):
+    a = fg.DeviceArray.from_numpy(np.eye(3))
+    with pytest.raises(fg.Unsupported):
+        fg.matrix_power(a, -1)
+    with pytest.raises(fg.ShapeMismatch):
+        fg.matrix_power(fg.DeviceArray.from_numpy(np.zeros((2, 3))), 2)
