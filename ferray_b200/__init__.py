@@ -30,7 +30,7 @@ __all__ = [
     "default_context", "gemm_f64", "gemm_f32", "gemm_c64", "gemm_c32", "gemm_i8",
     "gemm_i8_signed", "gemm_i16", "gemm_bf16_f32", "gemm_f16_f32", "quantized_matmul", "matmul", "matmul_complex",
     "gemm_batched_strided", "gemm_grouped", "GroupedPlan", "Server", "launch_count", "PLAIN",
-    "SPLIT", "TUNE_OPS", "tune_lookup", "tune_forced", "multi_dot", "multi_dot_order", "matrix_power",
+    "SPLIT", "TUNE_OPS", "tune_lookup", "tune_forced", "multi_dot", "multi_dot_order", "matrix_power", "tensordot",
 ]
 
 PLAIN, SPLIT = "plain", "split"
@@ -466,6 +466,35 @@ def multi_dot_order(dims):
     sp = (C.c_size_t * (n * n))()
     check(L.load().fg_multi_dot_order(n, cd, sp), "multi_dot_order")
     return np.array(sp[:], dtype=np.int64).reshape(n, n)
+
+
+def tensordot(a, b, axes=2, mode=PLAIN):
+    """numpy.tensordot on DeviceArrays (products/tensordot.rs:35): `axes` an
+    int N (last N of a with first N of b) or a pair of axis lists."""
+    if isinstance(axes, int):
+        if axes > a.ndim or axes > b.ndim:
+            raise ShapeMismatch(f"tensordot: cannot contract {axes} axes from shapes {a.shape} and {b.shape}")
+        ax_a, ax_b = list(range(a.ndim - axes, a.ndim)), list(range(axes))
+    else:
+        ax_a, ax_b = [list(x) for x in axes]
+        if len(ax_a) != len(ax_b):
+            raise ShapeMismatch("tensordot: axes_a and axes_b must have the same length")
+    if a.dtype != b.dtype:
+        raise InvalidDtype("tensordot: operands need the same dtype")
+    free_a = [a.shape[i] for i in range(a.ndim) if i not in ax_a]
+    free_b = [b.shape[i] for i in range(b.ndim) if i not in ax_b]
+    out = DeviceArray(free_a + free_b, a.dtype, a.ctx)
+    sa = (C.c_int64 * max(a.ndim, 1))(*a.shape)
+    sb = (C.c_int64 * max(b.ndim, 1))(*b.shape)
+    n = len(ax_a)
+    xa = (C.c_int * max(n, 1))(*ax_a)
+    xb = (C.c_int * max(n, 1))(*ax_b)
+    osh = (C.c_int64 * 16)()
+    ond = C.c_int()
+    check(a.ctx._lib.fg_tensordot(a.ctx.handle, _NP2FG[a.dtype], _mode(mode), a.ptr, a.ndim, sa, b.ptr, b.ndim,
+                                  sb, n, xa, xb, out.ptr, osh, C.byref(ond), None), "tensordot")
+    a.ctx.sync()
+    return out
 
 
 def matrix_power(a, exponent, mode=PLAIN):

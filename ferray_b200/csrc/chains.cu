@@ -101,6 +101,74 @@ fg_status write_identity(fg_dtype d, void* out, long long n, cudaStream_t st) {
     return FG_OK;
 }
 
+// N-D permutation (up to 8 dims) of a contiguous row-major array into a
+// contiguous one: out[o] = in[sum_d idx_d(o) * in_stride[perm[d]]], elements
+// of E bytes moved as 4- or 8-byte words.
+struct PermuteArgs {
+    int nd;
+    long long out_shape[8];
+    long long in_stride[8];  // elements, of the input axis that is output axis d
+};
+
+template <typename W, int WPE>
+__global__ void permute_kernel(const W* __restrict__ in, W* __restrict__ out, long long total,
+                               PermuteArgs pa) {
+    for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < total;
+         o += (long long)gridDim.x * blockDim.x) {
+        long long rem = o, src = 0;
+#pragma unroll
+        for (int d = 7; d >= 0; --d) {
+            if (d < pa.nd) {
+                const long long idx = rem % pa.out_shape[d];
+                rem /= pa.out_shape[d];
+                src += idx * pa.in_stride[d];
+            }
+        }
+#pragma unroll
+        for (int w = 0; w < WPE; ++w) out[o * WPE + w] = in[src * WPE + w];
+    }
+}
+
+// Permutes `in` (shape, nd) by perm into `out`; no-op (returns in) for the
+// identity permutation.
+fg_status permute(fg_dtype d, const void* in, int nd, const int64_t* shape, const int* perm, Scratch& sc,
+                  const void** result, cudaStream_t st) {
+    bool ident = true;
+    for (int i = 0; i < nd; ++i) ident = ident && perm[i] == i;
+    if (ident) {
+        *result = in;
+        return FG_OK;
+    }
+    PermuteArgs pa{};
+    pa.nd = nd;
+    long long stride[8], total = 1;
+    for (int i = nd - 1; i >= 0; --i) {
+        stride[i] = total;
+        total *= shape[i];
+    }
+    for (int i = 0; i < nd; ++i) {
+        pa.out_shape[i] = shape[perm[i]];
+        pa.in_stride[i] = stride[perm[i]];
+    }
+    const size_t es = out_size(d);
+    FG_TRY(sc.alloc(static_cast<size_t>(std::max<long long>(total, 1)) * es, st));
+    const int grid = static_cast<int>(std::min<long long>(std::max<long long>((total + 255) / 256, 1), 8192));
+    using U64 = unsigned long long;
+    if (es == 4)
+        permute_kernel<uint32_t, 1><<<grid, 256, 0, st>>>(static_cast<const uint32_t*>(in),
+                                                          static_cast<uint32_t*>(sc.p), total, pa);
+    else if (es == 8)
+        permute_kernel<U64, 1><<<grid, 256, 0, st>>>(static_cast<const U64*>(in), static_cast<U64*>(sc.p),
+                                                     total, pa);
+    else
+        permute_kernel<U64, 2><<<grid, 256, 0, st>>>(static_cast<const U64*>(in), static_cast<U64*>(sc.p),
+                                                     total, pa);
+    count_launch();
+    FG_CUDA(cudaGetLastError());
+    *result = sc.p;
+    return FG_OK;
+}
+
 }  // namespace
 
 }  // namespace fgrt
@@ -180,6 +248,66 @@ fg_status fg_matrix_power(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, size_t n, c
     }
     if (res_bufs[ri] != out) FG_CUDA(cudaMemcpyAsync(out, res_bufs[ri], bytes, cudaMemcpyDeviceToDevice, st));
     return FG_OK;
+}
+
+fg_status fg_tensordot(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, const void* a, int ndim_a,
+                       const int64_t* shape_a, const void* b, int ndim_b, const int64_t* shape_b, int naxes,
+                       const int* axes_a, const int* axes_b, void* out, int64_t* out_shape, int* out_ndim,
+                       fg_stream stream) {
+    if (!ctx) return set_error(FG_ERR_INVALID, "null context");
+    if (!chain_dtype_ok(dtype)) return set_error(FG_ERR_DTYPE, "tensordot: dtype must be f64, f32, c64 or c32");
+    if (ndim_a < 0 || ndim_b < 0 || ndim_a > 8 || ndim_b > 8 || naxes < 0 || !out_shape || !out_ndim)
+        return set_error(FG_ERR_INVALID, "tensordot: bad ranks or null output arguments");
+    if (naxes > 0 && (!axes_a || !axes_b)) return set_error(FG_ERR_INVALID, "tensordot: null axes");
+    // checks and free axes as products/tensordot.rs:67-97
+    for (int i = 0; i < naxes; ++i) {
+        if (axes_a[i] < 0 || axes_a[i] >= ndim_a || axes_b[i] < 0 || axes_b[i] >= ndim_b)
+            return set_error(FG_ERR_SHAPE, "tensordot: axis out of bounds");
+        if (shape_a[axes_a[i]] != shape_b[axes_b[i]])
+            return set_error(FG_ERR_SHAPE, "tensordot: contracted dimensions must match");
+        for (int j = 0; j < i; ++j)
+            if (axes_a[j] == axes_a[i] || axes_b[j] == axes_b[i])
+                return set_error(FG_ERR_SHAPE, "tensordot: repeated axis");
+    }
+    auto contains = [](const int* ax, int n, int v) {
+        for (int i = 0; i < n; ++i)
+            if (ax[i] == v) return true;
+        return false;
+    };
+    int perm_a[8], perm_b[8], nfa = 0, nfb = 0;
+    long long free_a = 1, free_b = 1, contract = 1;
+    int nout = 0;
+    for (int i = 0; i < ndim_a; ++i)
+        if (!contains(axes_a, naxes, i)) {
+            perm_a[nfa++] = i;
+            free_a *= shape_a[i];
+            out_shape[nout++] = shape_a[i];
+        }
+    for (int i = 0; i < naxes; ++i) {
+        perm_a[nfa + i] = axes_a[i];
+        contract *= shape_a[axes_a[i]];
+    }
+    for (int i = 0; i < naxes; ++i) perm_b[i] = axes_b[i];
+    for (int i = 0; i < ndim_b; ++i)
+        if (!contains(axes_b, naxes, i)) {
+            perm_b[naxes + nfb++] = i;
+            free_b *= shape_b[i];
+            out_shape[nout++] = shape_b[i];
+        }
+    *out_ndim = nout;
+    FG_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream_of(ctx, stream);
+    if (free_a == 0 || free_b == 0) return FG_OK;
+    if (!a || !b || !out) return set_error(FG_ERR_INVALID, "tensordot: null pointer");
+    Scratch sa, sb;
+    const void *pa = a, *pb = b;
+    FG_TRY(permute(dtype, a, ndim_a, shape_a, perm_a, sa, &pa, st));
+    FG_TRY(permute(dtype, b, ndim_b, shape_b, perm_b, sb, &pb, st));
+    // (free_a x contract) @ (contract x free_b); contract == 1 with no axes
+    // is the outer product
+    return fg_gemm(ctx, dtype, mode, 0, static_cast<size_t>(free_a), static_cast<size_t>(free_b),
+                   static_cast<size_t>(contract), nullptr, pa, static_cast<size_t>(contract), pb,
+                   static_cast<size_t>(free_b), nullptr, out, static_cast<size_t>(free_b), 0, st);
 }
 
 }  // extern "C"

@@ -124,6 +124,16 @@ fg_status fg_multi_dot(fg_ctx *ctx, fg_dtype dtype, fg_mode mode, size_t count,
 /* The parenthesisation fg_multi_dot uses (host only): split[i*count + j] is
  * the k at which the product of matrices i..j is split. */
 fg_status fg_multi_dot_order(size_t count, const int64_t *dims, size_t *split);
+/* numpy-style tensordot (products/tensordot.rs:35-153): contracts axes_a[i]
+ * of `a` with axes_b[i] of `b` (naxes pairs; the scalar form axes = N is
+ * the last N of a with the first N of b); out (contiguous) gets a's free
+ * axes then b's.  Operands are permuted on the device (free axes first for
+ * a, contracted first for b; skipped when already in that order) and
+ * contracted by one GEMM.  out_shape receives up to ndim_a + ndim_b dims. */
+fg_status fg_tensordot(fg_ctx *ctx, fg_dtype dtype, fg_mode mode, const void *a, int ndim_a,
+                       const int64_t *shape_a, const void *b, int ndim_b, const int64_t *shape_b,
+                       int naxes, const int *axes_a, const int *axes_b, void *out,
+                       int64_t *out_shape, int *out_ndim, fg_stream stream);
 /* A^exponent for a square n x n device matrix (solve.rs:456-494): identity
  * for 0, exponentiation by squaring in the reference's order for > 0;
  * negative powers need inv(A) and return FG_ERR_UNSUPPORTED. */

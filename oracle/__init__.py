@@ -142,6 +142,20 @@ def matrix_power(a, n):
     return result
 
 
+def tensordot(a, b, axes_a, axes_b):
+    """products/tensordot.rs:86-153: permute a (free axes, then contracted)
+    and b (contracted, then free), then the naive loop sum += x * y in k
+    order (separate multiply and add, the Rust `+=` of a product)."""
+    fa = [i for i in range(a.ndim) if i not in axes_a]
+    fb = [i for i in range(b.ndim) if i not in axes_b]
+    ap = np.transpose(a, fa + list(axes_a)).reshape(int(np.prod([a.shape[i] for i in fa])), -1)
+    bp = np.transpose(b, list(axes_b) + fb).reshape(ap.shape[1], -1)
+    out = np.zeros((ap.shape[0], bp.shape[1]), a.dtype)
+    for k in range(ap.shape[1]):
+        out = out + ap[:, k:k + 1] * bp[k:k + 1, :]
+    return out.reshape([a.shape[i] for i in fa] + [b.shape[i] for i in fb])
+
+
 def bf16_to_f32(bits):
     """bf16 bit patterns (uint16) -> f32, exact (the `half` crate's widening)."""
     return (np.asarray(bits, np.uint16).astype(np.uint32) << 16).view(np.float32)

@@ -60,3 +60,44 @@ def test_matrix_power_errors(fg):
         fg.matrix_power(a, -1)
     with pytest.raises(fg.ShapeMismatch):
         fg.matrix_power(fg.DeviceArray.from_numpy(np.zeros((2, 3))), 2)
+
+
+@pytest.mark.parametrize("dt,u", [(np.float64, U64), (np.float32, U32), (np.complex128, U64)])
+@pytest.mark.parametrize("sa,sb,axes", [
+    ((3, 4, 5), (4, 5, 6), 2),                 # identity permutations
+    ((3, 4, 5), (5, 4, 2), ([1, 2], [1, 0])),  # both permuted
+    ((6, 7, 8, 9), (9, 7, 5), ([3, 1], [0, 1])),
+    ((30, 40), (40, 50), 1),
+    ((5, 6), (7, 8), 0),                       # outer product
+    ((4, 5), (5, 4), ([0, 1], [1, 0])),        # full contraction -> shape ()
+])
+def test_tensordot(fg, oracle, dt, u, sa, sb, axes):
+    rng = np.random.default_rng(len(sa) * 10 + len(sb))
+    a = rng.standard_normal(sa)
+    b = rng.standard_normal(sb)
+    if dt == np.complex128:
+        a = a + 1j * rng.standard_normal(sa)
+        b = b + 1j * rng.standard_normal(sb)
+    a, b = a.astype(dt), b.astype(dt)
+    got = fg.tensordot(fg.DeviceArray.from_numpy(a), fg.DeviceArray.from_numpy(b), axes).to_numpy()
+    if isinstance(axes, int):
+        ax = (list(range(a.ndim - axes, a.ndim)), list(range(axes)))
+    else:
+        ax = axes
+    want = np.tensordot(a.astype(np.complex128), b.astype(np.complex128), axes=ax)
+    assert got.shape == want.shape
+    k = max(1, int(np.prod([a.shape[i] for i in ax[0]])))
+    scale = np.linalg.norm(a) * np.linalg.norm(b)
+    assert np.linalg.norm(got - want) <= 4 * k * u * scale + 1e-300
+    if dt == np.float64:
+        ref = oracle.tensordot(a, b, ax[0], ax[1])
+        assert np.linalg.norm(got - want) <= 2 * np.linalg.norm(ref - want) + 2 * k * u * scale
+
+
+def test_tensordot_errors(fg):
+    a = fg.DeviceArray.from_numpy(np.zeros((3, 4)))
+    b = fg.DeviceArray.from_numpy(np.zeros((5, 6)))
+    with pytest.raises(fg.ShapeMismatch):
+        fg.tensordot(a, b, 1)
+    with pytest.raises(fg.ShapeMismatch):
+        fg.tensordot(a, b, ([0], [0, 1]))
