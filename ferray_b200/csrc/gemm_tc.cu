@@ -67,6 +67,15 @@ static int split_kchunk() {
 
 static unsigned long long kTimeoutNs = 4000000000ull;  // 4 s per wait
 
+// Row tiles per raster group of the persistent tile walk (FG_RASTER, 8).
+static int raster_group() {
+    static int v = [] {
+        const char* e = getenv("FG_RASTER");
+        return e ? atoi(e) : 8;
+    }();
+    return v;
+}
+
 template <class Cfg>
 static const char* cfg_name() {
     if (Cfg::BM == 256)
@@ -95,6 +104,7 @@ static fg_status launch_cfg(fg_ctx* ctx, const TcMaps& maps, TcArgs& args, cudaS
     FG_CUDA(attr_err);
     args.status = ctx->d_status;
     args.timeout_ns = kTimeoutNs;
+    if (args.raster <= 0) args.raster = raster_group();
     const long long tiles =
         (long long)std::max(args.splits, 1) * args.batch * args.tiles_m * args.tiles_n;
     if (tiles == 0) return FG_OK;
@@ -132,6 +142,7 @@ static fg_status launch_pair(fg_ctx* ctx, const TcMaps& maps, TcArgs& args, cuda
     FG_CUDA(attr_err);
     args.status = ctx->d_status;
     args.timeout_ns = kTimeoutNs;
+    if (args.raster <= 0) args.raster = raster_group();
     const long long units =
         (long long)std::max(args.splits, 1) * args.batch * args.tiles_m * args.tiles_n;
     if (units == 0) return FG_OK;

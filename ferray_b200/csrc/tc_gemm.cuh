@@ -104,6 +104,7 @@ struct TcArgs {
     // of one tile, s = t / (batch*tiles); its partial result goes to output
     // matrix s*batch + bz.  splits <= 1: no split (zero-initialised args).
     int splits, kb_per_split;
+    int raster;                // row tiles per raster group (0: 8)
     // EPI_OZAKI: C (f64) (+)= oz_w * 2^(e_i + f_j) * acc; the first group of a
     // call applies C = oz_beta * C first.  cplx_half > 0 interleaves complex.
     const double* row_scale;
@@ -119,9 +120,10 @@ __device__ __forceinline__ void tile_coords(const TcArgs& p, int t, int& bz, int
     const int per_batch = p.tiles_m * p.tiles_n;
     bz = t / per_batch;
     int r = t - bz * per_batch;
-    // Grouped raster: 8 row-tiles share each sweep over the column tiles so
-    // the A rows and B columns of concurrently running tiles stay in L2.
-    const int GROUP = 8;
+    // Grouped raster: `raster` (default 8) row-tiles share each sweep over
+    // the column tiles so the A rows and B columns of concurrently running
+    // tiles stay in L2.
+    const int GROUP = p.raster > 0 ? p.raster : 8;
     int per_group = GROUP * p.tiles_n;
     int g = r / per_group;
     int first_m = g * GROUP;
