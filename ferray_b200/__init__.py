@@ -30,7 +30,7 @@ __all__ = [
     "default_context", "gemm_f64", "gemm_f32", "gemm_c64", "gemm_c32", "gemm_i8",
     "gemm_i8_signed", "gemm_i16", "gemm_bf16_f32", "gemm_f16_f32", "quantized_matmul", "matmul", "matmul_complex",
     "gemm_batched_strided", "gemm_grouped", "GroupedPlan", "Server", "launch_count", "PLAIN",
-    "SPLIT", "TUNE_OPS", "tune_lookup", "tune_forced", "multi_dot", "multi_dot_order", "matrix_power", "tensordot",
+    "SPLIT", "TUNE_OPS", "tune_lookup", "tune_forced", "multi_dot", "multi_dot_order", "matrix_power", "tensordot", "npy_parse", "npy_load",
 ]
 
 PLAIN, SPLIT = "plain", "split"
@@ -430,6 +430,37 @@ def _chain_dims(arrays):
             raise ShapeMismatch(f"multi_dot: shapes of matrices {i - 1} and {i} not aligned "
                                 f"({prev[-1]} != {cur[0]})")
     return dims
+
+
+_FG2NP = {L.FG_F64: np.float64, L.FG_F32: np.float32, L.FG_C64: np.complex128, L.FG_C32: np.complex64,
+          L.FG_I8: np.int8, L.FG_U8I8: np.uint8, L.FG_I16: np.int16, L.FG_F16: np.float16}
+
+
+def npy_parse(data):
+    """Header of an .npy byte image: (numpy dtype, shape, fortran_order,
+    payload offset); host only."""
+    buf = bytes(data)
+    dt, nd, fo, off = C.c_int(), C.c_int(), C.c_int(), C.c_size_t()
+    sh = (C.c_int64 * 8)()
+    check(L.load().fg_npy_parse(buf, len(buf), C.byref(dt), sh, C.byref(nd), C.byref(fo), C.byref(off)),
+          "npy_parse")
+    return np.dtype(_FG2NP[dt.value]), tuple(sh[:nd.value]), bool(fo.value), off.value
+
+
+def npy_load(data, ctx=None):
+    """A DeviceArray holding the payload of an .npy byte image (C order)."""
+    ctx = ctx or default_context()
+    buf = bytes(data)
+    p, dt, nd = C.c_void_p(), C.c_int(), C.c_int()
+    sh = (C.c_int64 * 8)()
+    check(ctx._lib.fg_npy_upload(ctx.handle, buf, len(buf), C.byref(p), C.byref(dt), sh, C.byref(nd), None),
+          "npy_load")
+    ctx.sync()
+    arr = DeviceArray.__new__(DeviceArray)
+    arr.ctx, arr.shape, arr.dtype = ctx, tuple(sh[:nd.value]), np.dtype(_FG2NP[dt.value])
+    arr.nbytes = int(np.prod(arr.shape, dtype=np.int64)) * arr.dtype.itemsize
+    arr.ptr = p.value
+    return arr
 
 
 def multi_dot(arrays, mode=PLAIN):

@@ -66,6 +66,9 @@ SIGNATURES = {
     "fg_profile_collect": (_i, [C.POINTER(fg_profile_entry), _i, C.POINTER(_i)]),
     "fg_device_info": (_i, [_p, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(_sz)]),
     "fg_selftest_wait_timeout": (_i, [_p, C.c_uint32, _p]),
+    "fg_npy_parse": (_i, [_p, _sz, C.POINTER(_i), C.POINTER(_i64), C.POINTER(_i), C.POINTER(_i),
+                          C.POINTER(_sz)]),
+    "fg_npy_upload": (_i, [_p, _p, _sz, C.POINTER(_p), C.POINTER(_i), C.POINTER(_i64), C.POINTER(_i), _p]),
     "fg_multi_dot": (_i, [_p, _i, _i, _sz, C.POINTER(_p), C.POINTER(_i64), _p, _p]),
     "fg_multi_dot_order": (_i, [_sz, C.POINTER(_i64), C.POINTER(_sz)]),
     "fg_matrix_power": (_i, [_p, _i, _i, _sz, _p, _i64, _p, _p]),

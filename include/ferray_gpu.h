@@ -111,6 +111,23 @@ fg_status fg_device_info(fg_ctx *ctx, int *sm_count, int *cc_major, int *cc_mino
  * The same bounded wait guards every pipeline barrier of the GEMM kernels. */
 fg_status fg_selftest_wait_timeout(fg_ctx *ctx, uint32_t timeout_us, fg_stream stream);
 
+/* ------------------------------------------------------------ .npy ingest */
+/* Parses an .npy byte image (format 1.0 / 2.0 / 3.0, the header rules of
+ * ferray-io/src/npy/header.rs:32-106; host only, no device needed): element
+ * type as the fg_dtype of a GEMM operand (<f8 F64, <f4 F32, <c16 C64, <c8 C32,
+ * |i1 I8, |u1 U8I8 (the u8 operand), <i2 I16, <f2 F16), shape (up to 8
+ * dims), Fortran order flag and the payload offset.  FG_ERR_DTYPE for other
+ * or big-endian descrs, FG_ERR_SHAPE when the payload is shorter than the
+ * shape, FG_ERR_INVALID for a malformed image. */
+fg_status fg_npy_parse(const void *bytes, size_t len, fg_dtype *dtype, int64_t *shape, int *ndim,
+                       int *fortran_order, size_t *data_offset);
+/* Parses the image and copies its payload into a new device buffer
+ * (fg_buffer_alloc; free with fg_buffer_free), asynchronously on `stream`
+ * (the host bytes must stay valid until the stream reaches the copy).
+ * Row-major (C order) only. */
+fg_status fg_npy_upload(fg_ctx *ctx, const void *bytes, size_t len, void **dptr, fg_dtype *dtype,
+                        int64_t *shape, int *ndim, fg_stream stream);
+
 /* ------------------------------------------------------------ GEMM chains */
 /* multi_dot (products/mod.rs:776-902): mats[i] is a contiguous row-major
  * dims[i] x dims[i+1] device matrix (a 1-D first / last operand is passed as

@@ -18,6 +18,10 @@ Fixtures:
   `as i8`/`as i16`/`as u8` wrapping, with the answers of the naive
   wrapping-i32 loops those tests assert equality against
   (integer_tests.rs:15-63).
+* ``npy_dtypes.json`` -- the save / load cases of fixtures/io/npy_dtypes.json
+  (NumPy 2.4.5): data, shape, dtype, descr and Fortran order per case (complex
+  values as [re, im] pairs); the tests write them with NumPy's own .npy
+  writer and parse the bytes.
 """
 import json
 import os
@@ -159,6 +163,21 @@ def integer_cases():
     return cases
 
 
+def npy_dtypes():
+    d = json.load(open(os.path.join(FERRAY_ROOT, "fixtures", "io", "npy_dtypes.json")))
+    assert d["numpy_version"] == "2.4.5"
+    out = []
+    for c in d["test_cases"]:
+        inp = c["inputs"]
+        data = inp["data"]["data"]
+        if data and isinstance(data[0], dict):
+            data = [[v["re"], v["im"]] for v in data]
+        out.append({"name": c["name"], "data": data, "shape": inp["data"]["shape"],
+                    "dtype": inp["data"]["dtype"], "descr": inp.get("numpy_dtype_str", "<f8"),
+                    "fortran_order": bool(inp.get("fortran_order", False))})
+    return out
+
+
 def main():
     with open(os.path.join(HERE, "matmul_numpy.json"), "w") as f:
         json.dump(matmul_numpy(), f, indent=1)
@@ -166,6 +185,8 @@ def main():
         json.dump(gemm_hexfloat(), f, indent=1)
     with open(os.path.join(HERE, "integer_cases.json"), "w") as f:
         json.dump(integer_cases(), f)
+    with open(os.path.join(HERE, "npy_dtypes.json"), "w") as f:
+        json.dump(npy_dtypes(), f, indent=1)
     print("wrote fixtures to", HERE)
 
 

@@ -118,3 +118,65 @@ def test_multi_dot_order_matches_the_reference_programme():
         np.testing.assert_array_equal(np.triu(got, 1), np.triu(want, 1))
     # ties keep the first split (all-equal dims)
     assert fg.multi_dot_order([4, 4, 4, 4])[0][2] == oracle.chain_order([4, 4, 4, 4])[0][2]
+
+
+def _npy_bytes(arr, version=None):
+    import io
+    import numpy as np
+    f = io.BytesIO()
+    if version is None:
+        np.save(f, arr)
+    else:
+        np.lib.format.write_array(f, arr, version=version)
+    return f.getvalue()
+
+
+def test_npy_parse_reference_fixture_cases():
+    """The dtype cases of fixtures/io/npy_dtypes.json (NumPy 2.4.5 save /
+    load), written here by NumPy's own writer: GEMM operand types parse with
+    their shape and payload offset, the others are rejected as dtypes, and a
+    Fortran-order array reports its order."""
+    import json
+    import numpy as np
+    import ferray_b200 as fg
+    cases = json.load(open(os.path.join(ROOT, "tests", "golden", "npy_dtypes.json")))
+    gemm_types = {"<f4", "<f8", "|u1", "<c8", "<c16"}
+    seen = 0
+    for cs in cases:
+        data = cs["data"]
+        if "complex" in cs["dtype"]:
+            data = [complex(re, im) for re, im in data]
+        arr = np.array(data, dtype=cs["dtype"]).reshape(cs["shape"])
+        if cs.get("fortran_order"):
+            arr = np.asfortranarray(arr)
+        blob = _npy_bytes(arr)
+        if cs["descr"] in gemm_types:
+            dt, shape, fortran, off = fg.npy_parse(blob)
+            assert dt == arr.dtype and shape == tuple(cs["shape"]), cs["name"]
+            assert fortran == bool(cs.get("fortran_order")), cs["name"]
+            payload = np.frombuffer(blob[off:], dtype=dt)
+            order = "F" if fortran else "C"
+            np.testing.assert_array_equal(payload.reshape(shape, order=order), arr)
+            seen += 1
+        else:
+            with pytest.raises(fg.InvalidDtype):
+                fg.npy_parse(blob)
+    assert seen >= 5
+
+
+def test_npy_parse_versions_and_malformed_images():
+    import numpy as np
+    import ferray_b200 as fg
+    a = np.arange(12, dtype=np.int16).reshape(3, 4)
+    for v in ((1, 0), (2, 0), (3, 0)):
+        dt, shape, fo, off = fg.npy_parse(_npy_bytes(a, v))
+        assert dt == np.int16 and shape == (3, 4) and not fo
+    blob = _npy_bytes(np.zeros((2, 3), np.float32))
+    with pytest.raises(fg.InvalidValue):
+        fg.npy_parse(b"NOTNPY" + blob[6:])
+    with pytest.raises(fg.ShapeMismatch):
+        fg.npy_parse(blob[:-4])                         # payload shorter than the shape
+    with pytest.raises(fg.InvalidDtype):
+        fg.npy_parse(_npy_bytes(np.zeros(3, ">f8")))    # big-endian
+    dt, shape, fo, off = fg.npy_parse(_npy_bytes(np.float64(2.5)))  # 0-d
+    assert shape == () and dt == np.float64
