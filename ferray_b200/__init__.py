@@ -30,7 +30,7 @@ __all__ = [
     "default_context", "gemm_f64", "gemm_f32", "gemm_c64", "gemm_c32", "gemm_i8",
     "gemm_i8_signed", "gemm_i16", "gemm_bf16_f32", "gemm_f16_f32", "quantized_matmul", "matmul", "matmul_complex",
     "gemm_batched_strided", "gemm_grouped", "GroupedPlan", "Server", "launch_count", "PLAIN",
-    "SPLIT", "TUNE_OPS", "tune_lookup", "tune_forced", "multi_dot", "multi_dot_order", "matrix_power", "tensordot", "npy_parse", "npy_load",
+    "SPLIT", "TUNE_OPS", "tune_lookup", "tune_forced", "multi_dot", "multi_dot_order", "matrix_power", "tensordot", "einsum", "npy_parse", "npy_load",
 ]
 
 PLAIN, SPLIT = "plain", "split"
@@ -524,6 +524,29 @@ def tensordot(a, b, axes=2, mode=PLAIN):
     ond = C.c_int()
     check(a.ctx._lib.fg_tensordot(a.ctx.handle, _NP2FG[a.dtype], _mode(mode), a.ptr, a.ndim, sa, b.ptr, b.ndim,
                                   sb, n, xa, xb, out.ptr, osh, C.byref(ond), None), "tensordot")
+    a.ctx.sync()
+    return out
+
+
+def einsum(subscripts, a, b, mode=PLAIN):
+    """Two-operand einsum on DeviceArrays (pairwise contractions; see
+    fg_einsum)."""
+    if a.dtype != b.dtype:
+        raise InvalidDtype("einsum: operands need the same dtype")
+    sa = (C.c_int64 * max(a.ndim, 1))(*a.shape)
+    sb = (C.c_int64 * max(b.ndim, 1))(*b.shape)
+    osh = (C.c_int64 * 8)()
+    ond = C.c_int()
+    lib = a.ctx._lib
+    # shape pass (null operands, nothing launched): the output shape
+    st = lib.fg_einsum(a.ctx.handle, _NP2FG[a.dtype], _mode(mode), subscripts.encode(), None, a.ndim, sa, None,
+                       b.ndim, sb, None, osh, C.byref(ond), None)
+    if st not in (L.FG_OK, L.FG_ERR_INVALID):
+        check(st, "einsum")
+    shape = tuple(osh[:ond.value])
+    out = DeviceArray(shape, a.dtype, a.ctx)
+    check(lib.fg_einsum(a.ctx.handle, _NP2FG[a.dtype], _mode(mode), subscripts.encode(), a.ptr, a.ndim, sa, b.ptr,
+                        b.ndim, sb, out.ptr, osh, C.byref(ond), None), "einsum")
     a.ctx.sync()
     return out
 

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "prep_kernels.cuh"
@@ -308,6 +309,119 @@ fg_status fg_tensordot(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, const void* a,
     return fg_gemm(ctx, dtype, mode, 0, static_cast<size_t>(free_a), static_cast<size_t>(free_b),
                    static_cast<size_t>(contract), nullptr, pa, static_cast<size_t>(contract), pb,
                    static_cast<size_t>(free_b), nullptr, out, static_cast<size_t>(free_b), 0, st);
+}
+
+// Two-operand einsum "ab..,cd..->xy.." (labels a-z, A-Z; implicit output =
+// the labels that appear once, sorted, as numpy does).  Labels split into
+// batch (in both operands and the output), free-a, free-b (one operand and
+// the output) and contracted (both operands, not the output; a label in one
+// operand only and not in the output is summed by contracting with ones,
+// which is not supported here).  A is permuted to [batch, free_a, contract],
+// B to [batch, contract, free_b], one batched GEMM forms
+// [batch, free_a, free_b], and a last permute puts the output in the
+// requested label order.  This covers the reference's matmul shortcut
+// (products/einsum/mod.rs:251-282) and every other pairwise contraction
+// without repeated labels inside one operand.
+fg_status fg_einsum(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, const char* subscripts, const void* a, int ndim_a,
+                    const int64_t* shape_a, const void* b, int ndim_b, const int64_t* shape_b, void* out,
+                    int64_t* out_shape, int* out_ndim, fg_stream stream) {
+    if (!ctx || !subscripts || !out_shape || !out_ndim) return set_error(FG_ERR_INVALID, "einsum: null argument");
+    if (!chain_dtype_ok(dtype)) return set_error(FG_ERR_DTYPE, "einsum: dtype must be f64, f32, c64 or c32");
+    std::string spec;
+    for (const char* c = subscripts; *c; ++c)
+        if (*c != ' ') spec.push_back(*c);
+    const size_t comma = spec.find(','), arrow = spec.find("->");
+    if (comma == std::string::npos || spec.find(',', comma + 1) != std::string::npos ||
+        (arrow != std::string::npos && arrow < comma))
+        return set_error(FG_ERR_INVALID, "einsum: expected exactly two operands 'ab,bc->ac'");
+    const std::string la = spec.substr(0, comma);
+    const std::string lb = spec.substr(comma + 1, arrow == std::string::npos ? std::string::npos : arrow - comma - 1);
+    auto is_label = [](char c) { return (c >= 'a' && c <= 'z') || (c >= 'A' && c <= 'Z'); };
+    for (char c : la + lb)
+        if (!is_label(c)) return set_error(FG_ERR_UNSUPPORTED, "einsum: only letter labels (no ellipsis)");
+    if ((int)la.size() != ndim_a || (int)lb.size() != ndim_b)
+        return set_error(FG_ERR_SHAPE, "einsum: subscripts do not match the operand ranks");
+    for (size_t i = 0; i < la.size(); ++i)
+        if (la.find(la[i]) != i) return set_error(FG_ERR_UNSUPPORTED, "einsum: repeated label within an operand");
+    for (size_t i = 0; i < lb.size(); ++i)
+        if (lb.find(lb[i]) != i) return set_error(FG_ERR_UNSUPPORTED, "einsum: repeated label within an operand");
+    std::string lo;
+    if (arrow != std::string::npos) {
+        lo = spec.substr(arrow + 2);
+        for (size_t i = 0; i < lo.size(); ++i) {
+            if (!is_label(lo[i]) || lo.find(lo[i]) != i) return set_error(FG_ERR_INVALID, "einsum: bad output labels");
+            if (la.find(lo[i]) == std::string::npos && lb.find(lo[i]) == std::string::npos)
+                return set_error(FG_ERR_INVALID, "einsum: output label not in any operand");
+        }
+    } else {
+        for (char c = 'A'; c <= 'z'; ++c) {
+            if (!is_label(c)) continue;
+            const int n = (la.find(c) != std::string::npos) + (lb.find(c) != std::string::npos);
+            if (n == 1) lo.push_back(c);
+        }
+    }
+    if (lo.size() > 8 || la.size() > 8 || lb.size() > 8) return set_error(FG_ERR_UNSUPPORTED, "einsum: more than 8 dims");
+    auto size_of = [&](char c, int64_t* v) -> bool {
+        const size_t ia = la.find(c), ib = lb.find(c);
+        if (ia != std::string::npos && ib != std::string::npos && shape_a[ia] != shape_b[ib]) return false;
+        *v = ia != std::string::npos ? shape_a[ia] : shape_b[ib];
+        return true;
+    };
+    std::string batch, fa, fb, con;
+    for (char c : la) {
+        const bool inb = lb.find(c) != std::string::npos, ino = lo.find(c) != std::string::npos;
+        if (inb && ino) batch.push_back(c);
+        else if (inb) con.push_back(c);
+        else if (ino) fa.push_back(c);
+        else return set_error(FG_ERR_UNSUPPORTED, "einsum: label summed within one operand");
+    }
+    for (char c : lb) {
+        const bool ina = la.find(c) != std::string::npos, ino = lo.find(c) != std::string::npos;
+        if (!ina && ino) fb.push_back(c);
+        else if (!ina) return set_error(FG_ERR_UNSUPPORTED, "einsum: label summed within one operand");
+    }
+    int64_t nb = 1, m = 1, n = 1, k = 1, v;
+    for (char c : batch) { if (!size_of(c, &v)) return set_error(FG_ERR_SHAPE, "einsum: dimension mismatch"); nb *= v; }
+    for (char c : fa) { size_of(c, &v); m *= v; }
+    for (char c : fb) { size_of(c, &v); n *= v; }
+    for (char c : con) { if (!size_of(c, &v)) return set_error(FG_ERR_SHAPE, "einsum: dimension mismatch"); k *= v; }
+    *out_ndim = static_cast<int>(lo.size());
+    for (size_t i = 0; i < lo.size(); ++i) size_of(lo[i], &out_shape[i]);
+    FG_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream_of(ctx, stream);
+    if (nb * m * n == 0) return FG_OK;
+    if (!a || !b || !out) return set_error(FG_ERR_INVALID, "einsum: null pointer");
+    int perm_a[8], perm_b[8], perm_o[8];
+    const std::string oa = batch + fa + con, ob = batch + con + fb, om = batch + fa + fb;
+    for (size_t i = 0; i < oa.size(); ++i) perm_a[i] = static_cast<int>(la.find(oa[i]));
+    for (size_t i = 0; i < ob.size(); ++i) perm_b[i] = static_cast<int>(lb.find(ob[i]));
+    Scratch sa, sb, sm;
+    const void *pa, *pb;
+    FG_TRY(permute(dtype, a, ndim_a, shape_a, perm_a, sa, &pa, st));
+    FG_TRY(permute(dtype, b, ndim_b, shape_b, perm_b, sb, &pb, st));
+    // [batch, free_a, free_b] -> requested order; identity writes straight to out
+    int64_t mshape[8];
+    for (size_t i = 0; i < om.size(); ++i) size_of(om[i], &mshape[i]);
+    for (size_t i = 0; i < lo.size(); ++i) perm_o[i] = static_cast<int>(om.find(lo[i]));
+    bool ident = true;
+    for (size_t i = 0; i < lo.size(); ++i) ident = ident && perm_o[i] == static_cast<int>(i);
+    void* dst = out;
+    if (!ident) {
+        FG_TRY(sm.alloc(static_cast<size_t>(nb * m * n) * out_size(dtype), st));
+        dst = sm.p;
+    }
+    FG_TRY(fg_gemm_batched_strided(ctx, dtype, mode, 0, static_cast<size_t>(nb), static_cast<size_t>(m),
+                                   static_cast<size_t>(n), static_cast<size_t>(k), nullptr, pa,
+                                   static_cast<size_t>(k), m * k, pb, static_cast<size_t>(n), k * n, nullptr, dst,
+                                   static_cast<size_t>(n), m * n, 0, st));
+    if (!ident) {
+        Scratch tmp;
+        const void* res = nullptr;
+        FG_TRY(permute(dtype, dst, static_cast<int>(om.size()), mshape, perm_o, tmp, &res, st));
+        FG_CUDA(cudaMemcpyAsync(out, res, static_cast<size_t>(nb * m * n) * out_size(dtype),
+                                cudaMemcpyDeviceToDevice, st));
+    }
+    return FG_OK;
 }
 
 }  // extern "C"

@@ -151,6 +151,17 @@ fg_status fg_tensordot(fg_ctx *ctx, fg_dtype dtype, fg_mode mode, const void *a,
                        const int64_t *shape_a, const void *b, int ndim_b, const int64_t *shape_b,
                        int naxes, const int *axes_a, const int *axes_b, void *out,
                        int64_t *out_shape, int *out_ndim, fg_stream stream);
+/* Two-operand einsum ("ij,jk->ik", "bij,bjk->bik", "ijk,kjl->il", ...;
+ * letter labels, implicit output = labels seen once in ASCII order).  Covers
+ * the reference's matmul shortcut (products/einsum/mod.rs:251-282) and every
+ * pairwise contraction without repeated labels inside one operand
+ * (FG_ERR_UNSUPPORTED otherwise, e.g. traces or ellipsis): operands permuted
+ * on the device to [batch, free, contracted], one batched GEMM, and the
+ * output permuted to the requested order.  out_shape gets up to 8 dims. */
+fg_status fg_einsum(fg_ctx *ctx, fg_dtype dtype, fg_mode mode, const char *subscripts,
+                    const void *a, int ndim_a, const int64_t *shape_a, const void *b, int ndim_b,
+                    const int64_t *shape_b, void *out, int64_t *out_shape, int *out_ndim,
+                    fg_stream stream);
 /* A^exponent for a square n x n device matrix (solve.rs:456-494): identity
  * for 0, exponentiation by squaring in the reference's order for > 0;
  * negative powers need inv(A) and return FG_ERR_UNSUPPORTED. */

@@ -101,3 +101,31 @@ def test_tensordot_errors(fg):
         fg.tensordot(a, b, 1)
     with pytest.raises(fg.ShapeMismatch):
         fg.tensordot(a, b, ([0], [0, 1]))
+
+
+@pytest.mark.parametrize("spec,sa,sb", [
+    ("ij,jk->ik", (30, 40), (40, 20)),          # the reference's matmul shortcut
+    ("ij,jk", (30, 40), (40, 20)),              # implicit output
+    ("bij,bjk->bik", (4, 30, 40), (4, 40, 20)),  # batched
+    ("ij,kj->ik", (30, 40), (20, 40)),          # B transposed
+    ("ijk,kjl->il", (5, 6, 7), (7, 6, 8)),      # two contracted labels, permuted
+    ("bij,bjk->kib", (3, 5, 6), (3, 6, 4)),     # output permuted
+    ("i,j->ij", (7,), (9,)),                    # outer product
+    ("ij,ij->", (6, 5), (6, 5)),                # full contraction
+])
+def test_einsum_pairwise(fg, spec, sa, sb):
+    rng = np.random.default_rng(len(spec))
+    a = rng.standard_normal(sa)
+    b = rng.standard_normal(sb)
+    got = fg.einsum(spec, fg.DeviceArray.from_numpy(a), fg.DeviceArray.from_numpy(b)).to_numpy()
+    want = np.einsum(spec, a, b)
+    assert got.shape == want.shape
+    np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12 * max(1.0, np.abs(want).max()))
+
+
+def test_einsum_unsupported_forms(fg):
+    a = fg.DeviceArray.from_numpy(np.zeros((3, 3)))
+    with pytest.raises(fg.Unsupported):
+        fg.einsum("ii,ij->j", a, a)   # repeated label within an operand (trace)
+    with pytest.raises(fg.ShapeMismatch):
+        fg.einsum("ij,jk->ik", a, fg.DeviceArray.from_numpy(np.zeros((4, 2))))
