@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -530,8 +531,11 @@ fg_status fg_gemm_host(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, int slices, si
         }
     } join{s_in, s_cmp, s_out};
     const size_t total = ia + ib + ic;
-    const size_t kPanelBytes = 64u << 20;
-    long long panels = total <= kPanelBytes ? 1 : std::min<long long>(8, (total + kPanelBytes - 1) / kPanelBytes);
+    static const size_t kPanelBytes = [] {
+        const char* e = getenv("FG_PANEL_MB");
+        return static_cast<size_t>(e ? std::max(1, atoi(e)) : 64) << 20;
+    }();
+    long long panels = total <= kPanelBytes ? 1 : std::min<long long>(32, (total + kPanelBytes - 1) / kPanelBytes);
     long long rows = ((long long)m + panels - 1) / panels;
     rows = (rows + 255) / 256 * 256;
     panels = ((long long)m + rows - 1) / rows;
