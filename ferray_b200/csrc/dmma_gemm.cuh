@@ -24,8 +24,11 @@
 
 namespace fg {
 
+#ifndef FG_DMMA_BK
+#define FG_DMMA_BK 16
+#endif
 struct DmmaCfg {
-    static constexpr int BM = 128, BN = 128, BK = 16, STAGES = 3, THREADS = 256;
+    static constexpr int BM = 128, BN = 128, BK = FG_DMMA_BK, STAGES = 3, THREADS = 256;
     static constexpr int APAD = 4, BPAD = 4;
     static constexpr int A_ELEMS = BM * (BK + APAD);
     static constexpr int B_ELEMS = BK * (BN + BPAD);
@@ -74,21 +77,21 @@ __global__ void __launch_bounds__(DmmaCfg::THREADS, 1)
     const int m0 = blockIdx.y * Cfg::BM, n0 = blockIdx.x * Cfg::BN;
     const int kblocks = (K + Cfg::BK - 1) / Cfg::BK;
 
-    // global -> shared: 8 A and 8 B elements per thread per stage
+    // global -> shared: BM*BK/256 A and BK*BN/256 B elements per thread per stage
     auto load_stage = [&](int stage, int kb) {
         const int k0 = kb * Cfg::BK;
         double* as = As + stage * Cfg::A_ELEMS;
         double* bs = Bs + stage * Cfg::B_ELEMS;
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
+        for (int i = 0; i < Cfg::BM * Cfg::BK / 256; ++i) {
             const int e = tid + 256 * i;
-            const int r = e / Cfg::BK, c = e % Cfg::BK;  // A: 16 k per row
+            const int r = e / Cfg::BK, c = e % Cfg::BK;  // A: BK k per row
             const int gr = m0 + r, gk = k0 + c;
             const bool ok = gr < M && gk < K;
             cp_async8(as + r * (Cfg::BK + Cfg::APAD) + c, ok ? A + (long long)gr * lda + gk : A, ok);
         }
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
+        for (int i = 0; i < Cfg::BK * Cfg::BN / 256; ++i) {
             const int e = tid + 256 * i;
             const int r = e / Cfg::BN, c = e % Cfg::BN;  // B: 128 n per row
             const int gk = k0 + r, gn = n0 + c;

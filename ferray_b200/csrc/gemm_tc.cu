@@ -26,6 +26,9 @@ using CfgI8 = TcCfg<KIND_I8, 256, 4, 1, 1, 1, 1, EPI_I32>;
 using CfgI8n128 = TcCfg<KIND_I8, 128, 6, 1, 1, 1, 1, EPI_I32>;
 // 256 x 256 tiles on CTA pairs (cta_group::2), 6 stages of 32 KB per CTA.
 using CfgI8Pair = Tc2Cfg<KIND_I8, 256, 6, 1, 1, 1, 1, EPI_I32>;
+// 256 x 512 tiles on CTA pairs: one A tile feeds two N = 256 MMAs into two
+// TMEM accumulators (all 512 columns, single-buffered); 4 stages of 48 KB.
+using CfgI8PairW = Tc2Cfg<KIND_I8, 256, 4, 1, 2, 2, 2, EPI_I32, 0, 1>;
 using CfgQmm = TcCfg<KIND_I8, 256, 4, 1, 1, 1, 1, EPI_QMM>;
 using CfgQmmPair = Tc2Cfg<KIND_I8, 256, 6, 1, 1, 1, 1, EPI_QMM>;
 using CfgI16 = TcCfg<KIND_I8, 128, 3, 2, 2, 3, 4, EPI_I16>;
@@ -313,6 +316,13 @@ fg_status launch_int_tc(fg_ctx* ctx, const Gemm& g0, cudaStream_t st) {
             args.tiles_n = static_cast<int>((g.N + CfgI8Pair::BN - 1) / CfgI8Pair::BN);
             return launch_splitk<CfgI8Pair, int32_t>(ctx, maps, args, c.splits, C, g.ldc, g.c_stride,
                                                      0, 0, g.accumulate, st);
+        }
+        if (c.variant == 3) {
+            args.tiles_m = static_cast<int>((g.M + CfgI8PairW::BM - 1) / CfgI8PairW::BM);
+            args.tiles_n = static_cast<int>((g.N + CfgI8PairW::TILE_N - 1) / CfgI8PairW::TILE_N);
+            args.ops[1] = TcOp{0, 1, 1, g.dtype == FG_I8 ? 1 : 0, 1};
+            return launch_splitk<CfgI8PairW, int32_t>(ctx, maps, args, c.splits, C, g.ldc, g.c_stride,
+                                                      0, 0, g.accumulate, st);
         }
         if (c.variant == 1) {
             args.tiles_n = static_cast<int>((g.N + CfgI8n128::BN - 1) / CfgI8n128::BN);

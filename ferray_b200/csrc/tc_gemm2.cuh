@@ -28,12 +28,18 @@
 
 namespace fg {
 
+// COLSPLIT: the tile is NB x BN columns wide; B operand i holds columns
+// [i BN, (i + 1) BN) of the tile and accumulator i receives them (product
+// i = A x B_i), so one staged A tile feeds NB MMAs of N = BN -- less shared-
+// memory traffic per MAC than NB separate tiles.  Otherwise all operands and
+// accumulators cover the same BN columns (split / byte-slice schemes).
 template <int KIND_, int BN_, int STAGES_, int NA_, int NB_, int NACC_, int NOPS_, int EPI_,
-          int CHUNKED_ = 0>
+          int CHUNKED_ = 0, int COLSPLIT_ = 0>
 struct Tc2Cfg {
     static constexpr int KIND = KIND_, BM = 256, BN = BN_, STAGES = STAGES_;
     static constexpr int NA = NA_, NB = NB_, NACC = NACC_, NOPS = NOPS_, EPI = EPI_;
-    static constexpr int CHUNKED = CHUNKED_;
+    static constexpr int CHUNKED = CHUNKED_, COLSPLIT = COLSPLIT_;
+    static constexpr int TILE_N = COLSPLIT ? NB * BN : BN;  // output columns per tile
     static constexpr int ESIZE = KIND == KIND_I8 ? 1 : 2;
     static constexpr int BK_BYTES = 128;
     static constexpr int BK = BK_BYTES / ESIZE;
@@ -54,6 +60,14 @@ struct Tc2Cfg {
     static_assert(ACC_COLS <= 512, "accumulators exceed TMEM");
     static_assert(BN % 32 == 0 && BN <= 256, "UMMA N (pair)");
     static_assert(CTA_N % B_CHUNK_ELEMS == 0, "B half must be whole 128-byte chunks");
+    static_assert(!COLSPLIT || (NACC == NB && NOPS == NB && !CHUNKED), "column split: one acc per B");
+};
+
+// Single-accumulator view of a config for epilogue_store (column-split
+// accumulators are stored one at a time).
+template <class Cfg>
+struct Tc2EpiView {
+    static constexpr int NACC = 1, EPI = Cfg::EPI;
 };
 
 template <class Cfg>
@@ -114,7 +128,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Cfg::THREADS, 1)
     }
     if (warp == 0 && lane == 0) {
         for (int i = 0; i < Cfg::NA; ++i) tma_prefetch_desc(&maps.a[i]);
-        for (int i = 0; i < Cfg::NB; ++i) tma_prefetch_desc(&maps.b[i]);
+        for (int i = 0; i < (Cfg::COLSPLIT ? 1 : Cfg::NB); ++i) tma_prefetch_desc(&maps.b[i]);
     }
     if (warp == 1) {
         tmem_alloc_pair(&s.tmem_base, Cfg::TMEM_COLS);
@@ -139,7 +153,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Cfg::THREADS, 1)
                 unit_coords(p, t, zo, bz, tm, tn, kb0, kb1);
                 batch_operands(p, bz, za, zb);
                 const int row0 = tm * Cfg::BM + static_cast<int>(rank) * Cfg::CTA_M;
-                const int col0 = tn * Cfg::BN + static_cast<int>(rank) * Cfg::CTA_N;
+                const int col0 = tn * Cfg::TILE_N + static_cast<int>(rank) * Cfg::CTA_N;
                 for (int kb = kb0; kb < kb1; ++kb) {
                     if (!mbar_wait(&s.empty[stage], phase ^ 1u, p.timeout_ns, p.status, 0x01, abort)) {
                         ok = false;
@@ -158,11 +172,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Cfg::THREADS, 1)
 #pragma unroll
                         for (int c = 0; c < Cfg::B_CHUNKS; ++c) {
                             uint8_t* dst = s.b[stage][i] + c * Cfg::B_CHUNK_BYTES;
-                            const int nx = col0 + c * Cfg::B_CHUNK_ELEMS;
+                            // column split: every B operand is a column range of map 0
+                            const int nx = col0 + (Cfg::COLSPLIT ? i * Cfg::BN : 0) + c * Cfg::B_CHUNK_ELEMS;
+                            const CUtensorMap* mb = &maps.b[Cfg::COLSPLIT ? 0 : i];
                             if (p.b_rank3)
-                                tma_load_3d_pair(dst, &maps.b[i], nx, kx, zb, fb);
+                                tma_load_3d_pair(dst, mb, nx, kx, zb, fb);
                             else
-                                tma_load_2d_pair(dst, &maps.b[i], nx, kx, fb);
+                                tma_load_2d_pair(dst, mb, nx, kx, fb);
                         }
                     }
                     if (++stage == Cfg::STAGES) {
@@ -304,13 +320,26 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Cfg::THREADS, 1)
                 tc_fence_after();
                 const uint32_t row_addr =
                     tmem + (static_cast<uint32_t>(ew * 32) << 16) + buf * Cfg::ACC_COLS;
+                if constexpr (Cfg::COLSPLIT) {
+                    // accumulator a holds tile columns [a BN, (a + 1) BN)
+                    for (int a = 0; a < Cfg::NACC; ++a) {
 #pragma unroll 1
-                for (int c = 0; c < Cfg::BN / 32; ++c) {
-                    uint32_t v[Cfg::NACC][32];
+                        for (int c = 0; c < Cfg::BN / 32; ++c) {
+                            uint32_t v[1][32];
+                            tmem_ld_32x32b_x32(row_addr + a * Cfg::BN + c * 32, v[0]);
+                            tmem_wait_ld();
+                            epilogue_store<Tc2EpiView<Cfg>>(p, zo, grow, tn * Cfg::TILE_N + a * Cfg::BN + c * 32, v);
+                        }
+                    }
+                } else {
+#pragma unroll 1
+                    for (int c = 0; c < Cfg::BN / 32; ++c) {
+                        uint32_t v[Cfg::NACC][32];
 #pragma unroll
-                    for (int a = 0; a < Cfg::NACC; ++a) tmem_ld_32x32b_x32(row_addr + a * Cfg::BN + c * 32, v[a]);
-                    tmem_wait_ld();
-                    epilogue_store<Cfg>(p, zo, grow, tn * Cfg::BN + c * 32, v);
+                        for (int a = 0; a < Cfg::NACC; ++a) tmem_ld_32x32b_x32(row_addr + a * Cfg::BN + c * 32, v[a]);
+                        tmem_wait_ld();
+                        epilogue_store<Cfg>(p, zo, grow, tn * Cfg::BN + c * 32, v);
+                    }
                 }
                 tc_fence_before();
                 __syncwarp();

@@ -25,9 +25,9 @@ def rng(seed=0):
     return np.random.default_rng(seed)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
 @pytest.mark.parametrize("splits", SPLITS)
-@pytest.mark.parametrize("m,n,k", SHAPES + [(300, 520, 700), (257, 129, 4096)])
+@pytest.mark.parametrize("m,n,k", SHAPES + [(300, 520, 700), (257, 129, 4096), (513, 1100, 384)])
 def test_i8_variants_bit_exact(fg, oracle, variant, splits, m, n, k):
     r = rng(m + n + k)
     a = r.integers(-128, 128, (m, k), dtype=np.int8)
@@ -46,7 +46,7 @@ def test_i8_variants_bit_exact(fg, oracle, variant, splits, m, n, k):
         np.testing.assert_array_equal(c, oracle.gemm_i8(au, b, variant="vnni"))
 
 
-@pytest.mark.parametrize("variant,splits", [(0, 4), (1, 3), (2, 1), (2, 2)])
+@pytest.mark.parametrize("variant,splits", [(0, 4), (1, 3), (2, 1), (2, 2), (3, 1), (3, 3)])
 def test_i8_split_broadcast_batch(fg, oracle, variant, splits):
     r = rng(9)
     a = r.integers(-128, 128, (3, 1, 40, 520), dtype=np.int8)
