@@ -57,7 +57,7 @@ def parse():
     ap.add_argument("--peaks", action="store_true",
                     help="measure library reference rates (cuBLAS via torch) for INT8, FP64, FP32")
     ap.add_argument("--side", default="",
-                    help="run one side measurement only: dgemm, i8, ragged or serving")
+                    help="run one side measurement only: dgemm, i8, ragged, int, half, skinny, trsm, serving or ozaki")
     return ap.parse_args()
 
 
@@ -225,8 +225,9 @@ def side_measurements(fg, L, lib, ctx, stream, n, only=""):
     DGEMM plain vs Ozaki split at N=n with their DD-oracle errors; square i8
     at N=n (bit-exact on a sampled block); i16 and quantized u8 x i8; skinny
     shapes against the HBM roof; the 4096-problem ragged batch as one
-    grouped graph replay vs a loop of per-problem launches; the served stream
-    at 10k req/s, server vs plain one-call-at-a-time.  `only="ozaki"` runs
+    grouped graph replay vs a loop of per-problem launches; the lower
+    triangular solve at m = n (plain and split trailing updates); the served
+    stream at 10k req/s, server vs plain one-call-at-a-time.  `only="ozaki"` runs
     the per-spread / per-slice-count DGEMM and ZGEMM sweep (N = 2048..8192)."""
     import torch
     import oracle
@@ -432,6 +433,37 @@ def side_measurements(fg, L, lib, ctx, stream, n, only=""):
                         "variant": v, "splits": spl}
             del ta, tb, tc
         res["skinny_%d" % n] = sk
+        torch.cuda.empty_cache()
+    if not only or only == "trsm":
+        # --- triangular solve L X = B (m = n), work m^2 n: plain and split
+        # trailing updates; normwise residual ||L X - B|| / (||L|| ||X||) on
+        # 16 sampled columns (float64 on the host)
+        tr = {}
+        for name, dt, fgdt, st_t, mode in (("f64_plain", np.float64, L.FG_F64, C.c_double, L.FG_MODE_PLAIN),
+                                           ("f32_plain", np.float32, L.FG_F32, C.c_float, L.FG_MODE_PLAIN),
+                                           ("f32_split", np.float32, L.FG_F32, C.c_float, L.FG_MODE_SPLIT)):
+            lo = rng.uniform(-1.0, 1.0, (n, n)) / n
+            lo[np.arange(n), np.arange(n)] = rng.uniform(1.0, 2.0, n)
+            lo = np.tril(lo).astype(dt)
+            bb = rng.standard_normal((n, n)).astype(dt)
+            dl, dx = fg.DeviceArray.from_numpy(lo, ctx), fg.DeviceArray.from_numpy(bb, ctx)
+            one = st_t(1.0)
+
+            def solve():
+                return lib.fg_trsm_left(ctx.handle, fgdt, mode, 0, 0, n, n, C.byref(one), dl.ptr, n, dx.ptr, n, sh)
+            assert solve() == 0
+            torch.cuda.synchronize()
+            cols = np.sort(rng.choice(n, 16, replace=False))
+            x = dx.to_numpy()[:, cols].astype(np.float64)
+            r = lo.astype(np.float64) @ x - bb[:, cols].astype(np.float64)
+            res_n = float(np.linalg.norm(r) / (np.linalg.norm(lo.astype(np.float64)) * np.linalg.norm(x)))
+            l0 = fg.launch_count()
+            ms = _time_calls(torch, stream, solve, 3, 1)
+            tr[name] = {"ms": round(ms, 3), "tflops_m2n": round(float(n) ** 3 / ms / 1e9, 2),
+                        "launches_per_solve": int(round((fg.launch_count() - l0) / 4.0)),
+                        "normwise_residual": res_n}
+            del dl, dx
+        res["trsm_lower_%d" % n] = tr
         torch.cuda.empty_cache()
     if not only or only == "serving":
         # --- served stream, one rate

@@ -30,7 +30,8 @@ __all__ = [
     "default_context", "gemm_f64", "gemm_f32", "gemm_c64", "gemm_c32", "gemm_i8",
     "gemm_i8_signed", "gemm_i16", "gemm_bf16_f32", "gemm_f16_f32", "quantized_matmul", "matmul", "matmul_complex",
     "gemm_batched_strided", "gemm_grouped", "GroupedPlan", "Server", "launch_count", "PLAIN",
-    "SPLIT", "TUNE_OPS", "tune_lookup", "tune_forced", "multi_dot", "multi_dot_order", "matrix_power", "tensordot", "einsum", "npy_parse", "npy_load",
+    "SPLIT", "TUNE_OPS", "tune_lookup", "tune_forced", "multi_dot", "multi_dot_order", "matrix_power", "tensordot", "einsum",
+    "trsm_left_lower_f64", "trsm_left_upper_f64", "trsm_left_lower_f32", "trsm_left_upper_f32", "npy_parse", "npy_load",
 ]
 
 PLAIN, SPLIT = "plain", "split"
@@ -560,6 +561,58 @@ def matrix_power(a, exponent, mode=PLAIN):
                                      int(exponent), out.ptr, None), "matrix_power")
     a.ctx.sync()
     return out
+
+
+def _trsm(np_t, scalar_t, upper, m, n, alpha, a, lda, b, ldb, unit_diag, mode):
+    """Shared body of the trsm_left_* mirrors (trsm.rs:46-133): B (m x n,
+    row stride ldb) is overwritten by X with op(A) X = alpha B.  Device
+    arrays are solved in place; host arrays are staged through the device."""
+    if m == 0 or n == 0:
+        return
+    if lda < m or ldb < n:
+        raise ShapeMismatch("trsm: lda must be >= m and ldb >= n")
+    _need(a, (m - 1) * lda + m, np_t, "a")
+    _need(b, (m - 1) * ldb + n, np_t, "b")
+    ctx = default_context()
+    lib = ctx._lib
+    al = scalar_t(alpha)
+    fgdt = L.FG_F64 if np_t == np.float64 else L.FG_F32
+    if _is_dev(a) != _is_dev(b):
+        raise InvalidValue("mix of device and host operands")
+    if _is_dev(a):
+        check(lib.fg_trsm_left(ctx.handle, fgdt, _mode(mode), int(upper), int(bool(unit_diag)), m, n,
+                               C.byref(al), a.ptr, lda, b.ptr, ldb, None), "trsm")
+        ctx.sync()
+        return
+    da = DeviceArray.from_numpy(a, ctx)
+    db = DeviceArray.from_numpy(b, ctx)
+    try:
+        check(lib.fg_trsm_left(ctx.handle, fgdt, _mode(mode), int(upper), int(bool(unit_diag)), m, n,
+                               C.byref(al), da.ptr, lda, db.ptr, ldb, None), "trsm")
+        b[...] = db.to_numpy().reshape(b.shape)
+    finally:
+        da.free()
+        db.free()
+
+
+def trsm_left_lower_f64(m, n, alpha, a, lda, b, ldb, unit_diag, mode=PLAIN):
+    """Solve L X = alpha B in place (trsm.rs:46); L lower triangular."""
+    _trsm(np.float64, C.c_double, False, m, n, alpha, a, lda, b, ldb, unit_diag, mode)
+
+
+def trsm_left_upper_f64(m, n, alpha, a, lda, b, ldb, unit_diag, mode=PLAIN):
+    """Solve U X = alpha B in place (trsm.rs:70); U upper triangular."""
+    _trsm(np.float64, C.c_double, True, m, n, alpha, a, lda, b, ldb, unit_diag, mode)
+
+
+def trsm_left_lower_f32(m, n, alpha, a, lda, b, ldb, unit_diag, mode=PLAIN):
+    """f32 sibling of trsm_left_lower_f64 (trsm.rs:94)."""
+    _trsm(np.float32, C.c_float, False, m, n, alpha, a, lda, b, ldb, unit_diag, mode)
+
+
+def trsm_left_upper_f32(m, n, alpha, a, lda, b, ldb, unit_diag, mode=PLAIN):
+    """f32 sibling of trsm_left_upper_f64 (trsm.rs:118)."""
+    _trsm(np.float32, C.c_float, True, m, n, alpha, a, lda, b, ldb, unit_diag, mode)
 
 
 TUNE_OPS = {"i8": 0, "split_f32": 1, "f64": 2, "f32": 3}

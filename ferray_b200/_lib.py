@@ -72,6 +72,7 @@ SIGNATURES = {
     "fg_multi_dot": (_i, [_p, _i, _i, _sz, C.POINTER(_p), C.POINTER(_i64), _p, _p]),
     "fg_multi_dot_order": (_i, [_sz, C.POINTER(_i64), C.POINTER(_sz)]),
     "fg_matrix_power": (_i, [_p, _i, _i, _sz, _p, _i64, _p, _p]),
+    "fg_trsm_left": (_i, [_p, _i, _i, _i, _i, _sz, _sz, _p, _p, _sz, _p, _sz, _p]),
     "fg_einsum": (_i, [_p, _i, _i, C.c_char_p, _p, _i, C.POINTER(_i64), _p, _i, C.POINTER(_i64), _p,
                        C.POINTER(_i64), C.POINTER(_i), _p]),
     "fg_tensordot": (_i, [_p, _i, _i, _p, _i, C.POINTER(_i64), _p, _i, C.POINTER(_i64), _i,

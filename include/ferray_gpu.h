@@ -167,6 +167,22 @@ fg_status fg_einsum(fg_ctx *ctx, fg_dtype dtype, fg_mode mode, const char *subsc
  * negative powers need inv(A) and return FG_ERR_UNSUPPORTED. */
 fg_status fg_matrix_power(fg_ctx *ctx, fg_dtype dtype, fg_mode mode, size_t n, const void *a,
                           int64_t exponent, void *out, fg_stream stream);
+/* Left-side triangular solve op(A) X = alpha B, in place on the device
+ * matrix B (m x n, row stride ldb >= n); A is m x m with row stride
+ * lda >= m, lower (upper = 0) or upper triangular, its diagonal taken as 1
+ * when unit_diag.  Replaces trsm_left_lower_f64 / trsm_left_upper_f64 /
+ * trsm_left_lower_f32 / trsm_left_upper_f32 (ferray-linalg/src/trsm.rs:
+ * 46-133): alpha is a host double / float (null = 1); the same block
+ * recursion; sub-problems of <= 128 rows are solved with the reference's own
+ * operations in its order (bit-identical results), and each trailing update
+ * above them, B2 -= L21 X1 (B1 -= U12 X2), is one tuned GEMM in `mode` (f64
+ * split: the Ozaki form for updates of at least 4096 in rows, k and n,
+ * plain FP64 below).
+ * m == 0 or n == 0 returns FG_OK with B untouched.  FG_ERR_DTYPE for dtypes
+ * other than f64 / f32. */
+fg_status fg_trsm_left(fg_ctx *ctx, fg_dtype dtype, fg_mode mode, int upper, int unit_diag,
+                       size_t m, size_t n, const void *alpha, const void *a, size_t lda, void *b,
+                       size_t ldb, fg_stream stream);
 
 /* ------------------------------------------------------------ autotune */
 /* Tile variant and split-K count per GEMM family come from a table indexed

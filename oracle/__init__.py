@@ -156,6 +156,65 @@ def tensordot(a, b, axes_a, axes_b):
     return out.reshape([a.shape[i] for i in fa] + [b.shape[i] for i in fb])
 
 
+_TRSM_NB = 32  # trsm.rs:33
+
+
+def trsm_left(a, b, alpha=1.0, upper=False, unit_diag=False):
+    """ferray-linalg/src/trsm.rs:46-133 restated: X with op(A) X = alpha B
+    (a m x m, b m x n; b is copied, its dtype kept).  The same alpha scale
+    (trsm.rs:137-153), block recursion and split rule (trsm.rs:165-200,
+    264-300), unblocked substitution (trsm.rs:227-262, 304-332) and scalar
+    trailing update (trsm.rs:205-225), vectorised over columns only: every
+    element sees the reference's operations in the reference's order (a
+    product, then a difference; 1 / a_ii, then a product; no fused
+    multiply-add)."""
+    t = a.dtype.type
+    x = np.array(b, copy=True)
+    m, n = x.shape
+    if m == 0 or n == 0:
+        return x
+    if alpha != 1.0:
+        x *= t(alpha)
+
+    def unblocked(r0, mm):
+        for i in (range(mm - 1, -1, -1) if upper else range(mm)):
+            for p in (range(i + 1, mm) if upper else range(i)):
+                x[r0 + i] -= a[r0 + i, r0 + p] * x[r0 + p]
+            if not unit_diag:
+                x[r0 + i] *= t(1) / a[r0 + i, r0 + i]
+
+    def update(d0, rows, s0, blk):  # x[d0:d0+rows] -= blk @ x[s0:...], p ascending
+        for p in range(blk.shape[1]):
+            x[d0:d0 + rows] -= blk[:, p:p + 1] * x[s0 + p][None, :]
+
+    def rec(r0, mm):
+        if mm <= _TRSM_NB:
+            unblocked(r0, mm)
+            return
+        m1 = min(-(-(mm // 2) // _TRSM_NB) * _TRSM_NB, mm - _TRSM_NB)
+        m2 = mm - m1
+        if not upper:
+            rec(r0, m1)
+            update(r0 + m1, m2, r0, a[r0 + m1:r0 + mm, r0:r0 + m1])
+            rec(r0 + m1, m2)
+        else:
+            rec(r0 + m1, m2)
+            update(r0, m1, r0 + m1, a[r0:r0 + m1, r0 + m1:r0 + mm])
+            rec(r0, m1)
+
+    rec(0, m)
+    return x
+
+
+def trsm_test_triangle(m, upper=False):
+    """The triangular test matrices of trsm.rs:492-518: diagonal
+    2 + 0.5 i, off-diagonal 0.1 (i + j + 1) on the stored triangle."""
+    i, j = np.indices((m, m))
+    a = np.where(i == j, 2.0 + 0.5 * i, 0.1 * (i + j + 1))
+    keep = (j >= i) if upper else (j <= i)
+    return np.where(keep, a, 0.0)
+
+
 def bf16_to_f32(bits):
     """bf16 bit patterns (uint16) -> f32, exact (the `half` crate's widening)."""
     return (np.asarray(bits, np.uint16).astype(np.uint32) << 16).view(np.float32)

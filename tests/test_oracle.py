@@ -197,3 +197,36 @@ def test_half_restatements_widen_exactly(oracle):
     acc = oracle.gemm_f16_f32(a16, b16, c=c0.copy(), accumulate=True)
     np.testing.assert_array_equal(acc, oracle.gemm_f32(a16.astype(np.float32), b16.astype(np.float32),
                                                        1.0, 1.0, c0.copy()))
+
+
+@pytest.mark.parametrize("case", __import__("trsm_cases").CASES, ids=lambda c: c[0])
+def test_trsm_restatement_reference_cases(oracle, case):
+    """The TRSM restatement passes the reference's own residual tests."""
+    import trsm_cases as tc
+    a, b = tc.operands(case)
+    x = oracle.trsm_left(a, b, alpha=case[6], upper=case[2], unit_diag=case[3])
+    assert x.dtype == b.dtype
+    assert tc.residual_ok(case, a, b, x)
+
+
+def test_trsm_restatement_unit_diag_and_empty(oracle):
+    import trsm_cases as tc
+    a = tc.unit_diag_triangle()
+    b = (np.arange(24) * 0.3 + 0.5).reshape(6, 4)
+    xu = oracle.trsm_left(a, b, unit_diag=True)
+    xe = oracle.trsm_left(a, b, unit_diag=False)
+    assert np.abs(xu - xe).max() < 1e-12
+    e = np.zeros((0, 3))
+    assert oracle.trsm_left(np.zeros((0, 0)), e).shape == (0, 3)
+
+
+def test_trsm_restatement_split_rule(oracle):
+    """m1 = min(round_up(m / 2, 32), m - 32): leaves for m = 100 are 64 -> (32, 32)
+    and 36 -> (4, 32); the restatement's result is the same whatever the
+    recursion (exact arithmetic), so check it against a dense solve."""
+    import trsm_cases as tc
+    for m in (33, 64, 100, 129):
+        a = tc.random_triangle(m, np.float64, False, m)
+        b = np.random.default_rng(m).standard_normal((m, 5))
+        x = oracle.trsm_left(a, b)
+        np.testing.assert_allclose(x, np.linalg.solve(a, b), rtol=1e-12, atol=1e-12)
