@@ -31,7 +31,7 @@ __all__ = [
     "gemm_i8_signed", "gemm_i16", "gemm_bf16_f32", "gemm_f16_f32", "quantized_matmul", "matmul", "matmul_complex",
     "gemm_batched_strided", "gemm_grouped", "GroupedPlan", "Server", "launch_count", "PLAIN",
     "SPLIT", "TUNE_OPS", "tune_lookup", "tune_forced", "multi_dot", "multi_dot_order", "matrix_power", "tensordot", "einsum",
-    "trsm_left_lower_f64", "trsm_left_upper_f64", "trsm_left_lower_f32", "trsm_left_upper_f32", "npy_parse", "npy_load",
+    "trsm_left_lower_f64", "trsm_left_upper_f64", "trsm_left_lower_f32", "trsm_left_upper_f32", "npy_parse", "npy_load", "npz_names", "npz_read", "npz_load",
 ]
 
 PLAIN, SPLIT = "plain", "split"
@@ -456,6 +456,52 @@ def npy_load(data, ctx=None):
     sh = (C.c_int64 * 8)()
     check(ctx._lib.fg_npy_upload(ctx.handle, buf, len(buf), C.byref(p), C.byref(dt), sh, C.byref(nd), None),
           "npy_load")
+    ctx.sync()
+    arr = DeviceArray.__new__(DeviceArray)
+    arr.ctx, arr.shape, arr.dtype = ctx, tuple(sh[:nd.value]), np.dtype(_FG2NP[dt.value])
+    arr.nbytes = int(np.prod(arr.shape, dtype=np.int64)) * arr.dtype.itemsize
+    arr.ptr = p.value
+    return arr
+
+
+def npz_names(data):
+    """Names of the arrays in an .npz byte image, in archive order
+    (NpzFile::names, ferray-io/src/npz/mod.rs:140); host only."""
+    buf = bytes(data)
+    lib = L.load()
+    cnt = C.c_size_t()
+    check(lib.fg_npz_count(buf, len(buf), C.byref(cnt)), "npz_names")
+    names = []
+    for i in range(cnt.value):
+        n = C.c_size_t()
+        check(lib.fg_npz_name(buf, len(buf), i, None, 0, C.byref(n)), "npz_names")
+        out = C.create_string_buffer(n.value + 1)
+        check(lib.fg_npz_name(buf, len(buf), i, out, n.value + 1, C.byref(n)), "npz_names")
+        names.append(out.value.decode())
+    return names
+
+
+def npz_read(data, name):
+    """The .npy bytes of one array of an .npz byte image (inflated, CRC
+    checked); host only."""
+    buf = bytes(data)
+    lib = L.load()
+    n = C.c_size_t()
+    check(lib.fg_npz_read(buf, len(buf), name.encode(), None, 0, C.byref(n)), "npz_read")
+    out = C.create_string_buffer(max(n.value, 1))
+    check(lib.fg_npz_read(buf, len(buf), name.encode(), out, n.value, C.byref(n)), "npz_read")
+    return out.raw[:n.value]
+
+
+def npz_load(data, name, ctx=None):
+    """One array of an .npz byte image as a DeviceArray (NpzFile::get,
+    ferray-io/src/npz/mod.rs:150)."""
+    ctx = ctx or default_context()
+    buf = bytes(data)
+    p, dt, nd = C.c_void_p(), C.c_int(), C.c_int()
+    sh = (C.c_int64 * 8)()
+    check(ctx._lib.fg_npz_upload(ctx.handle, buf, len(buf), name.encode(), C.byref(p), C.byref(dt), sh,
+                                 C.byref(nd), None), "npz_load")
     ctx.sync()
     arr = DeviceArray.__new__(DeviceArray)
     arr.ctx, arr.shape, arr.dtype = ctx, tuple(sh[:nd.value]), np.dtype(_FG2NP[dt.value])

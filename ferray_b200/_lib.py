@@ -69,6 +69,11 @@ SIGNATURES = {
     "fg_npy_parse": (_i, [_p, _sz, C.POINTER(_i), C.POINTER(_i64), C.POINTER(_i), C.POINTER(_i),
                           C.POINTER(_sz)]),
     "fg_npy_upload": (_i, [_p, _p, _sz, C.POINTER(_p), C.POINTER(_i), C.POINTER(_i64), C.POINTER(_i), _p]),
+    "fg_npz_count": (_i, [_p, _sz, C.POINTER(_sz)]),
+    "fg_npz_name": (_i, [_p, _sz, _sz, C.c_char_p, _sz, C.POINTER(_sz)]),
+    "fg_npz_read": (_i, [_p, _sz, C.c_char_p, _p, _sz, C.POINTER(_sz)]),
+    "fg_npz_upload": (_i, [_p, _p, _sz, C.c_char_p, C.POINTER(_p), C.POINTER(_i), C.POINTER(_i64),
+                           C.POINTER(_i), _p]),
     "fg_multi_dot": (_i, [_p, _i, _i, _sz, C.POINTER(_p), C.POINTER(_i64), _p, _p]),
     "fg_multi_dot_order": (_i, [_sz, C.POINTER(_i64), C.POINTER(_sz)]),
     "fg_matrix_power": (_i, [_p, _i, _i, _sz, _p, _i64, _p, _p]),

@@ -51,7 +51,7 @@ def build(verbose=False):
         objs = list(ex.map(lambda s: _compile(s, verbose), srcs))
     if os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(o) for o in objs):
         return LIB
-    cmd = [NVCC, "-shared", "-o", LIB] + objs + ["-lcudart"]
+    cmd = [NVCC, "-shared", "-o", LIB] + objs + ["-lcudart", "-lz"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("link failed:\n%s%s" % (r.stdout, r.stderr))

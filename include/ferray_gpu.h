@@ -128,6 +128,25 @@ fg_status fg_npy_parse(const void *bytes, size_t len, fg_dtype *dtype, int64_t *
 fg_status fg_npy_upload(fg_ctx *ctx, const void *bytes, size_t len, void **dptr, fg_dtype *dtype,
                         int64_t *shape, int *ndim, fg_stream stream);
 
+/* .npz archives held in memory (ferray-io/src/npz/mod.rs:88-200, NpzFile):
+ * member names are the archive's file names without a trailing ".npy";
+ * a name is fetched from the member "<name>.npy".  Stored and deflate
+ * members, ZIP64 archives; every member's CRC-32 is checked.  Host only,
+ * except fg_npz_upload. */
+fg_status fg_npz_count(const void *bytes, size_t len, size_t *count);
+/* Name of member `index` (NUL-terminated into out[cap]; out may be null to
+ * ask for *name_len only). */
+fg_status fg_npz_name(const void *bytes, size_t len, size_t index, char *out, size_t cap,
+                      size_t *name_len);
+/* The .npy bytes of array `name` (inflated) into out[cap]; out may be null
+ * to ask for *size only.  FG_ERR_INVALID when the name is not listed. */
+fg_status fg_npz_read(const void *bytes, size_t len, const char *name, void *out, size_t cap,
+                      size_t *size);
+/* Array `name` into a new device buffer, as fg_npy_upload (stored members
+ * are copied straight from `bytes`). */
+fg_status fg_npz_upload(fg_ctx *ctx, const void *bytes, size_t len, const char *name, void **dptr,
+                        fg_dtype *dtype, int64_t *shape, int *ndim, fg_stream stream);
+
 /* ------------------------------------------------------------ GEMM chains */
 /* multi_dot (products/mod.rs:776-902): mats[i] is a contiguous row-major
  * dims[i] x dims[i+1] device matrix (a 1-D first / last operand is passed as
