@@ -4,6 +4,7 @@
 #include "runtime.h"
 #include "simt_gemm.cuh"
 #include "dmma_gemm.cuh"
+#include "ffma_sgemm.cuh"
 #include "tune.h"
 
 #include <algorithm>
@@ -111,6 +112,75 @@ static fg_status launch_dmma(fg_ctx* ctx, const Gemm& g, BatchMap bm, int splits
     return FG_OK;
 }
 
+// Plain SGEMM on the cp.async FFMA kernel (ffma_sgemm.cuh): A transposed
+// into packed scratch, B in place when aligned (else packed), same split-K
+// scheme.  Results are bit-identical to simt_gemm_real<float, 8, 8, 8>.
+static fg_status launch_ffma(const Gemm& g, int splits_want, cudaStream_t st) {
+    static std::once_flag once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(once, [] {
+        attr_err = cudaFuncSetAttribute(ffma_sgemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(FfmaCfg::SMEM));
+    });
+    FG_CUDA(attr_err);
+    const long long M = g.M, N = g.N, K = g.K;
+    const long long Mp = (M + 3) / 4 * 4, Np = (N + 3) / 4 * 4;
+    const float* A = static_cast<const float*>(g.A);
+    const float* B = static_cast<const float*>(g.B);
+    Scratch sa, sb;
+    FG_TRY(sa.alloc(static_cast<size_t>(g.a_count * K * Mp) * sizeof(float), st));
+    float* At = static_cast<float*>(sa.p);
+    transpose_pack_kernel<<<dim3(static_cast<unsigned>((Mp + 31) / 32), static_cast<unsigned>((K + 31) / 32),
+                                 static_cast<unsigned>(g.a_count)),
+                            dim3(32, 8), 0, st>>>(A, (int)M, (int)K, g.lda, g.a_mstride, At, Mp);
+    count_launch();
+    const bool direct = (reinterpret_cast<uintptr_t>(B) % 16) == 0 && g.ldb % 4 == 0 && N % 4 == 0;
+    const float* Bk = B;
+    long long ldbk = g.ldb;
+    BatchMap bm = batch_map(g);
+    for (int d = 0; d < 4; ++d) bm.a_bstride[d] = g.a_istride[d] * K * Mp;
+    if (!direct) {
+        FG_TRY(sb.alloc(static_cast<size_t>(g.b_count * K * Np) * sizeof(float), st));
+        float* Bp = static_cast<float*>(sb.p);
+        pack_rows_kernel<<<dim3(static_cast<unsigned>(std::min<long long>((K * Np + 255) / 256, 4096)),
+                                static_cast<unsigned>(g.b_count)),
+                           256, 0, st>>>(B, (int)K, (int)N, g.ldb, g.b_mstride, Bp, Np);
+        count_launch();
+        Bk = Bp;
+        ldbk = Np;
+        for (int d = 0; d < 4; ++d) bm.b_bstride[d] = g.b_istride[d] * K * Np;
+    }
+    const int bcols = static_cast<int>(direct ? N : Np);
+    constexpr long long KUNIT = 64;
+    const long long kunits = (K + KUNIT - 1) / KUNIT;
+    int kps = static_cast<int>(kunits);
+    const int splits = plan_splits(splits_want, static_cast<int>(kunits), M * N * g.batch, sizeof(float), &kps);
+    if ((long long)splits * g.batch > 65535) return set_error(FG_ERR_UNSUPPORTED, "batch above 65535");
+    dim3 grid((N + FfmaCfg::BN - 1) / FfmaCfg::BN, (M + FfmaCfg::BM - 1) / FfmaCfg::BM, g.batch * splits);
+    if (splits <= 1) {
+        ffma_sgemm_kernel<<<grid, FfmaCfg::THREADS, FfmaCfg::SMEM, st>>>(
+            (int)M, (int)N, (int)K, (float)g.alpha_re, At, Mp, Bk, ldbk, bcols, (float)g.beta_re,
+            static_cast<float*>(g.C), g.ldc, bm, g.batch, (int)K);
+        count_launch();
+        FG_CUDA(cudaGetLastError());
+        return FG_OK;
+    }
+    Scratch ws;
+    const long long out_elems = M * N * g.batch;
+    FG_TRY(ws.alloc(static_cast<size_t>(splits * out_elems) * sizeof(float), st));
+    BatchMap wbm = bm;
+    wbm.c_bstride = M * N;
+    ffma_sgemm_kernel<<<grid, FfmaCfg::THREADS, FfmaCfg::SMEM, st>>>(
+        (int)M, (int)N, (int)K, 1.f, At, Mp, Bk, ldbk, bcols, 0.f, static_cast<float*>(ws.p), N, wbm, g.batch,
+        (int)(kps * KUNIT));
+    splitk_reduce_kernel<float><<<grid_for(out_elems), 256, 0, st>>>(
+        static_cast<const float*>(ws.p), splits, M, N, g.batch, static_cast<float*>(g.C), g.ldc, g.c_stride,
+        (float)g.alpha_re, (float)g.beta_re, 0);
+    count_launch(2);
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
 // Matrix-vector shapes (one operand is a vector; ferray's matmul of a 1-D
 // operand, products/mod.rs:362-437) go to the GEMV kernels.
 template <typename T>
@@ -179,6 +249,10 @@ fg_status launch_simt(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
                 case 1: return launch_simt_real<float, 4, 4>(g, bm, c.splits, st);
                 case 2: return launch_simt_real<float, 2, 8>(g, bm, c.splits, st);
                 case 3: return launch_simt_real<float, 8, 2>(g, bm, c.splits, st);
+                case 4:
+                    // the packed transpose wants a K grid below 65536 blocks
+                    if (g.M > 0 && g.N > 0 && g.K > 0 && g.K <= 32LL * 65535) return launch_ffma(g, c.splits, st);
+                    return launch_simt_real<float, 8, 8>(g, bm, c.splits, st);
                 default: return launch_simt_real<float, 8, 8>(g, bm, c.splits, st);
             }
         }

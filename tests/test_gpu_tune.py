@@ -81,7 +81,7 @@ def test_split_f32_variants(fg, oracle, variant, splits, m, n, k):
 
 
 @pytest.mark.parametrize("op,dt,u,variant", [("f64", np.float64, U64, v) for v in range(5)] +
-                         [("f32", np.float32, U32, v) for v in range(4)])
+                         [("f32", np.float32, U32, v) for v in range(5)])
 @pytest.mark.parametrize("splits", SPLITS)
 @pytest.mark.parametrize("m,n,k", SHAPES + [(257, 300, 501)])
 def test_plain_variants(fg, oracle, op, dt, u, variant, splits, m, n, k):
@@ -154,3 +154,35 @@ def test_ozaki_groups_pair_kernel_bitwise_equal(fg, oracle, m, n, k, dt):
     ref = 0.75 * oracle.dd_full(a, b) + 0.5 * c0
     scale = np.linalg.norm(a) * np.linalg.norm(b)
     assert np.linalg.norm(outs[1] - ref) / scale <= 4 * k * U64
+
+
+@pytest.mark.parametrize("splits", [1, 3])
+@pytest.mark.parametrize("m,n,k", [(130, 48, 77), (257, 45, 300), (64, 260, 1000), (1, 7, 5)])
+def test_ffma_cp_async_kernel_bit_identical(fg, m, n, k, splits):
+    """f32 variant 4 (cp.async ring, A transposed into scratch, B in place or
+    packed) keeps the register tile and k order of variant 0: same bits."""
+    r = rng(m * 3 + n + k)
+    a = r.standard_normal((m, k)).astype(np.float32)
+    b = r.standard_normal((k, n)).astype(np.float32)
+    c0 = r.standard_normal((m, n)).astype(np.float32)
+    out = []
+    for variant in (0, 4):
+        with fg.tune_forced("f32", variant, splits):
+            c = c0.copy()
+            assert fg.gemm_f32(m, n, k, 0.75, a, b, -1.5, c)
+            out.append(c)
+    np.testing.assert_array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("n", [45, 48])
+def test_ffma_cp_async_broadcast_batch(fg, n):
+    r = rng(n)
+    a = r.standard_normal((2, 3, 33, 700)).astype(np.float32)
+    b = r.standard_normal((3, 700, n)).astype(np.float32)
+    res = []
+    for variant in (0, 4):
+        with fg.tune_forced("f32", variant, 1):
+            res.append(fg.matmul(fg.DeviceArray.from_numpy(a), fg.DeviceArray.from_numpy(b)).to_numpy())
+    np.testing.assert_array_equal(res[0], res[1])
+    want = np.einsum("...ik,...kj->...ij", a.astype(np.float64), b.astype(np.float64))
+    assert np.abs(res[1] - want).max() <= 700 * 2.0 ** -23 * np.abs(a).max() * np.abs(b).max() * 4
