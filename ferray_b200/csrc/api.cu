@@ -544,9 +544,21 @@ fg_status fg_gemm_host(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, int slices, si
     uint8_t* dc = static_cast<uint8_t*>(sc.p);
     const uint8_t* ha = static_cast<const uint8_t*>(a);
     uint8_t* hc = static_cast<uint8_t*>(c);
-    for (long long i = 0; i < panels; ++i) {
-        const size_t r0 = static_cast<size_t>(i * rows);
+    // The last panel's GEMM and copy-out run after every input has arrived,
+    // so the schedule ends on a 256-row piece to keep that tail short.
+    std::vector<std::pair<size_t, size_t>> parts;  // (first row, rows)
+    for (size_t r0 = 0; r0 < m;) {
         const size_t mi = std::min<size_t>(m - r0, static_cast<size_t>(rows));
+        if (panels > 1 && r0 + mi == m && mi > 512) {
+            parts.emplace_back(r0, mi - 256);
+            parts.emplace_back(r0 + mi - 256, 256);
+            break;
+        }
+        parts.emplace_back(r0, mi);
+        r0 += mi;
+    }
+    for (const auto& part : parts) {
+        const size_t r0 = part.first, mi = part.second;
         const size_t oa = r0 * k * ein, na = mi * k * ein, oc = r0 * n * eout, nc = mi * n * eout;
         if (na) FG_CUDA(cudaMemcpyAsync(da + oa, ha + oa, na, cudaMemcpyHostToDevice, s_in));
         if (reads_c) FG_CUDA(cudaMemcpyAsync(dc + oc, hc + oc, nc, cudaMemcpyHostToDevice, s_in));
