@@ -68,6 +68,24 @@ static __global__ void pack_rows_kernel(const float* __restrict__ B, int K, int 
     }
 }
 
+// CGEMM as a real GEMM (the ZGEMM embedding of dmma_gemm.cuh in f32):
+// interleaved complex A (M x K) is the real M x 2K matrix it lies as, and
+// B' (2K x 2N, pitch 2N) holds [[br, bi], [-bi, br]] for every complex b,
+// so columns 2n and 2n + 1 of A B' are Re and Im of (AB)[:, n].
+static __global__ void cgemm_expand_b_kernel(const float2* __restrict__ B, long long K, long long N, long long ldb,
+                                             float* __restrict__ Bx) {
+    const long long total = K * N;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long k = e / N, n = e - k * N;
+        const float2 b = B[k * ldb + n];
+        float* r0 = Bx + (2 * k) * (2 * N) + 2 * n;
+        float* r1 = r0 + 2 * N;
+        *reinterpret_cast<float2*>(r0) = make_float2(b.x, b.y);
+        *reinterpret_cast<float2*>(r1) = make_float2(-b.y, b.x);
+    }
+}
+
 // C = alpha At^T B + beta C.  At: packed K x ldat per A matrix (batch
 // offsets from bm.a_bstride in packed elements); B: K x ldb with columns
 // valid below `bcols` (a multiple of 4; chunks at or past it read zero).

@@ -286,6 +286,30 @@ fg_status launch_simt(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
             break;
         }
         case FG_C32: {
+            // Real scalars, one output matrix and a tuned f32 choice of the
+            // cp.async FFMA kernel for the embedded shape: the real-embedded
+            // GEMM (M x 2K) (2K x 2N) on it (same 8MNK flops, one FMA per
+            // product); otherwise the 4M kernel.
+            if (g.batch == 1 && g.alpha_im == 0.0 && g.beta_im == 0.0 && g.M > 0 && g.N > 0 && g.K > 0 &&
+                2 * g.K <= 32LL * 65535 && (reinterpret_cast<uintptr_t>(g.B) & 7) == 0) {
+                const TuneChoice c = tune_lookup(TUNE_F32, g.M, 2 * g.N, 2 * g.K);
+                if (c.variant == 4) {
+                    Scratch bx;
+                    FG_TRY(bx.alloc(static_cast<size_t>(4 * g.K * g.N) * sizeof(float), st));
+                    cgemm_expand_b_kernel<<<grid_for(g.K * g.N), 256, 0, st>>>(
+                        static_cast<const float2*>(g.B), g.K, g.N, g.ldb, static_cast<float*>(bx.p));
+                    count_launch();
+                    Gemm r = g;
+                    r.dtype = FG_F32;
+                    r.N = 2 * g.N;
+                    r.K = 2 * g.K;
+                    r.lda = 2 * g.lda;
+                    r.B = bx.p;
+                    r.ldb = 2 * g.N;
+                    r.ldc = 2 * g.ldc;
+                    return launch_ffma(r, c.splits, st);
+                }
+            }
             dim3 grid((g.N + 63) / 64, (g.M + 63) / 64, g.batch);
             simt_gemm_cplx<float, 8><<<grid, 256, 0, st>>>(
                 (int)g.M, (int)g.N, (int)g.K, (float)g.alpha_re, (float)g.alpha_im,

@@ -186,3 +186,24 @@ def test_ffma_cp_async_broadcast_batch(fg, n):
     np.testing.assert_array_equal(res[0], res[1])
     want = np.einsum("...ik,...kj->...ij", a.astype(np.float64), b.astype(np.float64))
     assert np.abs(res[1] - want).max() <= 700 * 2.0 ** -23 * np.abs(a).max() * np.abs(b).max() * 4
+
+
+@pytest.mark.parametrize("m,n,k", [(130, 70, 300), (257, 129, 64), (33, 5, 1000)])
+def test_cgemm_real_embedding_on_ffma(fg, oracle, m, n, k):
+    """Plain CGEMM: with the FFMA kernel chosen for the embedded shape it runs
+    as the real GEMM (M x 2K) x (2K x 2N); the 4M kernel otherwise."""
+    r = rng(m + n + k)
+    a = (r.standard_normal((m, k)) + 1j * r.standard_normal((m, k))).astype(np.complex64)
+    b = (r.standard_normal((k, n)) + 1j * r.standard_normal((k, n))).astype(np.complex64)
+    c0 = (r.standard_normal((m, n)) + 1j * r.standard_normal((m, n))).astype(np.complex64)
+    exact = a.astype(np.complex128) @ b.astype(np.complex128)
+    scale = np.linalg.norm(a.astype(np.complex128)) * np.linalg.norm(b.astype(np.complex128))
+    for variant in (0, 4):
+        with fg.tune_forced("f32", variant, 1):
+            c = np.zeros((m, n), np.complex64)
+            assert fg.gemm_c32(m, n, k, 1.0, 0.0, a, b, 0.0, 0.0, c)
+            assert oracle.error_vs_dd(a, b, c) <= 2 * k * U32
+            c = c0.copy()
+            assert fg.gemm_c32(m, n, k, 0.5, 0.0, a, b, -1.0, 0.0, c)
+            ref = 0.5 * exact - c0.astype(np.complex128)
+            assert np.linalg.norm(c - ref) <= (2 * k + 4) * U32 * scale + 2 * U32 * np.linalg.norm(ref)
