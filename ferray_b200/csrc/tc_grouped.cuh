@@ -386,8 +386,8 @@ struct SimtGroupedArgs {
 
 static __global__ void __launch_bounds__(256) simt_grouped_sgemm(const SimtGroupedArgs g) {
     constexpr int BM = 64, BN = 64, BK = 16;
-    __shared__ float As[BK][BM + 4];
-    __shared__ float Bs[BK][BN + 4];
+    __shared__ __align__(16) float As[2][BK][BM + 4];
+    __shared__ __align__(16) float Bs[2][BK][BN + 4];
     const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
     for (long long t = blockIdx.x; t < g.total_tiles; t += gridDim.x) {
         const TileRec tr = g.tiles[t];
@@ -397,33 +397,49 @@ static __global__ void __launch_bounds__(256) simt_grouped_sgemm(const SimtGroup
         const float* B = static_cast<const float*>(g.b[pi]);
         const long long lda = g.lda[pi], ldb = g.ldb[pi];
         const int m0 = tr.tm * BM, n0 = tr.tn * BN;
-        float acc[4][4] = {};
-        for (int k0 = 0; k0 < pr.K; k0 += BK) {
-            // A tile 64x16: 1024 elements, 4 per thread (row-major reads along k)
+        // Next K block into registers while this one is computed; shared
+        // tiles double-buffered, one barrier per K block.
+        float ra[4], rb[4];
+        auto load = [&](int k0) {
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const int e = tid + q * 256;
                 const int ar = e / BK, ac = e % BK;
                 const int gr = m0 + ar, gk = k0 + ac;
-                As[ac][ar] = (gr < pr.M && gk < pr.K) ? A[(long long)gr * lda + gk] : 0.f;
+                ra[q] = (gr < pr.M && gk < pr.K) ? A[(long long)gr * lda + gk] : 0.f;
                 const int br = e / BN, bc = e % BN;
                 const int gk2 = k0 + br, gn = n0 + bc;
-                Bs[br][bc] = (gk2 < pr.K && gn < pr.N) ? B[(long long)gk2 * ldb + gn] : 0.f;
+                rb[q] = (gk2 < pr.K && gn < pr.N) ? B[(long long)gk2 * ldb + gn] : 0.f;
             }
-            __syncthreads();
+        };
+        auto store = [&](int buf) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int e = tid + q * 256;
+                As[buf][e % BK][e / BK] = ra[q];
+                Bs[buf][e / BN][e % BN] = rb[q];
+            }
+        };
+        float acc[4][4] = {};
+        const int kblocks = (pr.K + BK - 1) / BK;
+        load(0);
+        __syncthreads();  // the previous tile's readers are done with buffer 0
+        store(0);
+        __syncthreads();
+        for (int kb = 0; kb < kblocks; ++kb) {
+            const int cur = kb & 1;
+            if (kb + 1 < kblocks) load((kb + 1) * BK);
 #pragma unroll
             for (int kk = 0; kk < BK; ++kk) {
-                float af[4], bf[4];
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    af[i] = As[kk][ty * 4 + i];
-                    bf[i] = Bs[kk][tx * 4 + i];
-                }
+                const float4 a4 = *reinterpret_cast<const float4*>(&As[cur][kk][ty * 4]);
+                const float4 b4 = *reinterpret_cast<const float4*>(&Bs[cur][kk][tx * 4]);
+                const float af[4] = {a4.x, a4.y, a4.z, a4.w}, bf[4] = {b4.x, b4.y, b4.z, b4.w};
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
 #pragma unroll
                     for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(af[i], bf[j], acc[i][j]);
             }
+            if (kb + 1 < kblocks) store(cur ^ 1);
             __syncthreads();
         }
         float* C = static_cast<float*>(pr.C);
