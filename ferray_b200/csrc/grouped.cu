@@ -209,9 +209,17 @@ fg_status grouped_job_bind(GroupedJob* j, void* dev_base, void* host_stage) {
     char* d_arena = dbase + j->host_bytes();
     std::memcpy(hbase, j->probs.data(), sizeof(GroupedProblem) * np);
     TileRec* htiles = reinterpret_cast<TileRec*>(hbase + o_tiles);
-    for (int x = 0; x < np; ++x) {
+    // Tiles of the deepest problems first: the persistent CTAs take tiles
+    // t, t + grid, ... so, in descending cost order, every CTA's share
+    // differs from another's by at most one tile (longest-first balance;
+    // in problem order one CTA could draw several 512-deep tiles).
+    std::vector<int> order(static_cast<size_t>(np));
+    for (int x = 0; x < np; ++x) order[x] = x;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int u, int v) { return j->probs[u].k_blocks > j->probs[v].k_blocks; });
+    long long t = 0;
+    for (int x : order) {
         const GroupedProblem& g = j->probs[x];
-        long long t = g.tile_start;
         for (int tm = 0; tm < g.tiles_m; ++tm)
             for (int tn = 0; tn < g.tiles_n; ++tn) htiles[t++] = TileRec{x, tm, tn, 0};
     }
