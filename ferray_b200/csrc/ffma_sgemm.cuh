@@ -187,4 +187,116 @@ static __global__ void __launch_bounds__(FfmaCfg::THREADS, 2)
     }
 }
 
+// Skinny form for few rows (M <= 32 per tile): a 32 x 256 CTA tile, each
+// thread 2 consecutive rows x 16 columns (four 4-column groups 64 apart),
+// the same cp.async ring and the same per-output k order (one FMA per
+// product, k ascending), so it too is bit-identical to the 128 x 128
+// kernels at equal split-K.  With few rows the work per B element is small,
+// so the host splits K to fill the GPU.
+struct FfmaSkinnyCfg {
+    static constexpr int BM = 32, BN = 256, BK = 16, STAGES = 4, THREADS = 256, PAD = 4;
+    static constexpr int AS = BK * (BM + PAD), BS = BK * (BN + PAD);
+    static constexpr size_t SMEM = size_t(STAGES) * (AS + BS) * sizeof(float);
+};
+
+static __global__ void __launch_bounds__(FfmaSkinnyCfg::THREADS, 2)
+    ffma_sgemm_skinny_kernel(int M, int N, int K, float alpha, const float* __restrict__ At, long long ldat,
+                             const float* __restrict__ B, long long ldb, int bcols, float beta,
+                             float* __restrict__ C, long long ldc, BatchMap bm, int nbatch, int ksplit) {
+    using Cfg = FfmaSkinnyCfg;
+    constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, PAD = Cfg::PAD, STAGES = Cfg::STAGES;
+    extern __shared__ __align__(16) float ffma_sk_sm[];
+    float* As = ffma_sk_sm;                     // [STAGES][BK][BM + PAD]
+    float* Bs = ffma_sk_sm + STAGES * Cfg::AS;  // [STAGES][BK][BN + PAD]
+
+    const int zb = blockIdx.z % nbatch, zs = blockIdx.z / nbatch;
+    long long oa, ob;
+    batch_offsets(bm, zb, oa, ob);
+    const int k_begin = zs * ksplit;
+    At += oa + (long long)k_begin * ldat;
+    B += ob + (long long)k_begin * ldb;
+    C += blockIdx.z * bm.c_bstride;
+    K = min(K - k_begin, ksplit);
+
+    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int kblocks = (K + BK - 1) / BK;
+    constexpr int A_CH = BK * BM / 4;                  // 128 chunks: threads 0..127 take one
+    constexpr int B_CH = BK * BN / 4 / Cfg::THREADS;   // 4 chunks a thread
+
+    auto load = [&](int stage, int kb) {
+        const int k0 = kb * BK;
+        float* as = As + stage * Cfg::AS;
+        float* bs = Bs + stage * Cfg::BS;
+        if (tid < A_CH) {
+            const int r = tid / (BM / 4), col = (tid % (BM / 4)) * 4;
+            const int gk = k0 + r, gm = m0 + col;
+            const bool ok = gk < K && gm < ldat;
+            cp_async16(as + r * (BM + PAD) + col, ok ? At + (long long)gk * ldat + gm : At, ok);
+        }
+#pragma unroll
+        for (int i = 0; i < B_CH; ++i) {
+            const int c = tid + Cfg::THREADS * i;
+            const int r = c / (BN / 4), col = (c % (BN / 4)) * 4;
+            const int gk = k0 + r, gn = n0 + col;
+            const bool ok = gk < K && gn < bcols;
+            cp_async16(bs + r * (BN + PAD) + col, ok ? B + (long long)gk * ldb + gn : B, ok);
+        }
+    };
+
+    float acc[2][16];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 16; ++j) acc[i][j] = 0.f;
+
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; ++s) {
+        if (s < kblocks) load(s, s);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
+    for (int kb = 0; kb < kblocks; ++kb) {
+        asm volatile("cp.async.wait_group %0;" ::"n"(STAGES - 2) : "memory");
+        __syncthreads();
+        {
+            const int nk = kb + STAGES - 1;
+            if (nk < kblocks) load(nk % STAGES, nk);
+            asm volatile("cp.async.commit_group;" ::: "memory");
+        }
+        const float* as = As + (kb % STAGES) * Cfg::AS;
+        const float* bs = Bs + (kb % STAGES) * Cfg::BS;
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            const float2 a2 = *reinterpret_cast<const float2*>(as + kk * (BM + PAD) + ty * 2);
+            const float af[2] = {a2.x, a2.y};
+            float bf[16];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float4 b = *reinterpret_cast<const float4*>(bs + kk * (BN + PAD) + q * 64 + tx * 4);
+                bf[q * 4] = b.x; bf[q * 4 + 1] = b.y; bf[q * 4 + 2] = b.z; bf[q * 4 + 3] = b.w;
+            }
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 16; ++j) acc[i][j] = fmaf(af[i], bf[j], acc[i][j]);
+        }
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const int r = m0 + ty * 2 + i;
+        if (r >= M) continue;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int c = n0 + (j / 4) * 64 + tx * 4 + (j % 4);
+            if (c >= N) continue;
+            float* p = C + (long long)r * ldc + c;
+            float v = alpha * acc[i][j];
+            if (beta != 0.f) v = fmaf(beta, *p, v);
+            *p = v;
+        }
+    }
+}
+
 }  // namespace fg

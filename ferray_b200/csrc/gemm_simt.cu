@@ -115,12 +115,15 @@ static fg_status launch_dmma(fg_ctx* ctx, const Gemm& g, BatchMap bm, int splits
 // Plain SGEMM on the cp.async FFMA kernel (ffma_sgemm.cuh): A transposed
 // into packed scratch, B in place when aligned (else packed), same split-K
 // scheme.  Results are bit-identical to simt_gemm_real<float, 8, 8, 8>.
+template <class Cfg>
 static fg_status launch_ffma(const Gemm& g, int splits_want, cudaStream_t st) {
+    constexpr bool kSkinny = Cfg::BM == 32;
+    auto kern = kSkinny ? ffma_sgemm_skinny_kernel : ffma_sgemm_kernel;
     static std::once_flag once;
     static cudaError_t attr_err = cudaSuccess;
-    std::call_once(once, [] {
-        attr_err = cudaFuncSetAttribute(ffma_sgemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(FfmaCfg::SMEM));
+    std::call_once(once, [kern] {
+        attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(Cfg::SMEM));
     });
     FG_CUDA(attr_err);
     const long long M = g.M, N = g.N, K = g.K;
@@ -156,9 +159,9 @@ static fg_status launch_ffma(const Gemm& g, int splits_want, cudaStream_t st) {
     int kps = static_cast<int>(kunits);
     const int splits = plan_splits(splits_want, static_cast<int>(kunits), M * N * g.batch, sizeof(float), &kps);
     if ((long long)splits * g.batch > 65535) return set_error(FG_ERR_UNSUPPORTED, "batch above 65535");
-    dim3 grid((N + FfmaCfg::BN - 1) / FfmaCfg::BN, (M + FfmaCfg::BM - 1) / FfmaCfg::BM, g.batch * splits);
+    dim3 grid((N + Cfg::BN - 1) / Cfg::BN, (M + Cfg::BM - 1) / Cfg::BM, g.batch * splits);
     if (splits <= 1) {
-        ffma_sgemm_kernel<<<grid, FfmaCfg::THREADS, FfmaCfg::SMEM, st>>>(
+        kern<<<grid, Cfg::THREADS, Cfg::SMEM, st>>>(
             (int)M, (int)N, (int)K, (float)g.alpha_re, At, Mp, Bk, ldbk, bcols, (float)g.beta_re,
             static_cast<float*>(g.C), g.ldc, bm, g.batch, (int)K);
         count_launch();
@@ -170,7 +173,7 @@ static fg_status launch_ffma(const Gemm& g, int splits_want, cudaStream_t st) {
     FG_TRY(ws.alloc(static_cast<size_t>(splits * out_elems) * sizeof(float), st));
     BatchMap wbm = bm;
     wbm.c_bstride = M * N;
-    ffma_sgemm_kernel<<<grid, FfmaCfg::THREADS, FfmaCfg::SMEM, st>>>(
+    kern<<<grid, Cfg::THREADS, Cfg::SMEM, st>>>(
         (int)M, (int)N, (int)K, 1.f, At, Mp, Bk, ldbk, bcols, 0.f, static_cast<float*>(ws.p), N, wbm, g.batch,
         (int)(kps * KUNIT));
     splitk_reduce_kernel<float><<<grid_for(out_elems), 256, 0, st>>>(
@@ -251,8 +254,13 @@ fg_status launch_simt(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
                 case 3: return launch_simt_real<float, 8, 2>(g, bm, c.splits, st);
                 case 4:
                     // the packed transpose wants a K grid below 65536 blocks
-                    if (g.M > 0 && g.N > 0 && g.K > 0 && g.K <= 32LL * 65535) return launch_ffma(g, c.splits, st);
+                    if (g.M > 0 && g.N > 0 && g.K > 0 && g.K <= 32LL * 65535)
+                        return launch_ffma<FfmaCfg>(g, c.splits, st);
                     return launch_simt_real<float, 8, 8>(g, bm, c.splits, st);
+                case 5:
+                    if (g.M > 0 && g.N > 0 && g.K > 0 && g.K <= 32LL * 65535)
+                        return launch_ffma<FfmaSkinnyCfg>(g, c.splits, st);
+                    return launch_simt_real<float, 2, 8>(g, bm, c.splits, st);
                 default: return launch_simt_real<float, 8, 8>(g, bm, c.splits, st);
             }
         }
@@ -307,7 +315,7 @@ fg_status launch_simt(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
                     r.B = bx.p;
                     r.ldb = 2 * g.N;
                     r.ldc = 2 * g.ldc;
-                    return launch_ffma(r, c.splits, st);
+                    return launch_ffma<FfmaCfg>(r, c.splits, st);
                 }
             }
             dim3 grid((g.N + 63) / 64, (g.M + 63) / 64, g.batch);

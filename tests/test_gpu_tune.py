@@ -81,7 +81,7 @@ def test_split_f32_variants(fg, oracle, variant, splits, m, n, k):
 
 
 @pytest.mark.parametrize("op,dt,u,variant", [("f64", np.float64, U64, v) for v in range(5)] +
-                         [("f32", np.float32, U32, v) for v in range(5)])
+                         [("f32", np.float32, U32, v) for v in range(6)])
 @pytest.mark.parametrize("splits", SPLITS)
 @pytest.mark.parametrize("m,n,k", SHAPES + [(257, 300, 501)])
 def test_plain_variants(fg, oracle, op, dt, u, variant, splits, m, n, k):
@@ -157,21 +157,23 @@ def test_ozaki_groups_pair_kernel_bitwise_equal(fg, oracle, m, n, k, dt):
 
 
 @pytest.mark.parametrize("splits", [1, 3])
-@pytest.mark.parametrize("m,n,k", [(130, 48, 77), (257, 45, 300), (64, 260, 1000), (1, 7, 5)])
+@pytest.mark.parametrize("m,n,k", [(130, 48, 77), (257, 45, 300), (64, 260, 1000), (1, 7, 5), (32, 600, 2000)])
 def test_ffma_cp_async_kernel_bit_identical(fg, m, n, k, splits):
-    """f32 variant 4 (cp.async ring, A transposed into scratch, B in place or
-    packed) keeps the register tile and k order of variant 0: same bits."""
+    """f32 variants 4 and 5 (cp.async ring, A transposed into scratch, B in
+    place or packed; 128 x 128 and skinny 32 x 256 tiles) keep the per-output
+    k order of variant 0: same bits."""
     r = rng(m * 3 + n + k)
     a = r.standard_normal((m, k)).astype(np.float32)
     b = r.standard_normal((k, n)).astype(np.float32)
     c0 = r.standard_normal((m, n)).astype(np.float32)
     out = []
-    for variant in (0, 4):
+    for variant in (0, 4, 5):
         with fg.tune_forced("f32", variant, splits):
             c = c0.copy()
             assert fg.gemm_f32(m, n, k, 0.75, a, b, -1.5, c)
             out.append(c)
     np.testing.assert_array_equal(out[0], out[1])
+    np.testing.assert_array_equal(out[0], out[2])
 
 
 @pytest.mark.parametrize("n", [45, 48])
