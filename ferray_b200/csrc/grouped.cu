@@ -336,7 +336,7 @@ static fg_status grouped_job_kernels(GroupedJob* j, cudaStream_t st) {
     const int grid = static_cast<int>(std::min<long long>(j->total_tiles, ctx->sm_count));
     if (j->kind == 0) {
         ProfScope prof("simt_grouped_sgemm", st);
-        simt_grouped_sgemm<<<std::min<long long>(j->total_tiles, ctx->sm_count * 4), 256, 0, st>>>(j->sargs);
+        simt_grouped_sgemm<<<std::min<long long>(j->total_tiles, ctx->sm_count * 8), 128, 0, st>>>(j->sargs);
         prof.stop();
     } else if (j->kind == 1) {
         ProfScope prof("tc_grouped_i8", st);

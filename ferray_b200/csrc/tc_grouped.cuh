@@ -370,7 +370,7 @@ static __global__ void grouped_prep_kernel(const PrepSeg* __restrict__ segs, int
 }
 
 // ------------------------------------------------------------------ SIMT
-// Plain FP32 grouped GEMM (FFMA): 64x64 tiles, 256 threads, 4x4 outputs per
+// Plain FP32 grouped GEMM (FFMA): 64x64 tiles, 128 threads, 4x8 outputs per
 // thread, persistent over the global tile list.
 struct SimtGroupedArgs {
     const GroupedProblem* problems;
@@ -384,11 +384,13 @@ struct SimtGroupedArgs {
     float alpha, beta;
 };
 
-static __global__ void __launch_bounds__(256) simt_grouped_sgemm(const SimtGroupedArgs g) {
-    constexpr int BM = 64, BN = 64, BK = 16;
+static __global__ void __launch_bounds__(128) simt_grouped_sgemm(const SimtGroupedArgs g) {
+    constexpr int BM = 64, BN = 64, BK = 16, NT = 128;
+    constexpr int PER = BM * BK / NT;  // elements of each operand a thread loads per K block
     __shared__ __align__(16) float As[2][BK][BM + 4];
     __shared__ __align__(16) float Bs[2][BK][BN + 4];
-    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+    // 16 x 8 threads, 4 rows x 8 columns each (two 4-column groups 32 apart)
+    const int tid = threadIdx.x, tx = tid % 8, ty = tid / 8;
     for (long long t = blockIdx.x; t < g.total_tiles; t += gridDim.x) {
         const TileRec tr = g.tiles[t];
         const int pi = tr.problem;
@@ -399,11 +401,11 @@ static __global__ void __launch_bounds__(256) simt_grouped_sgemm(const SimtGroup
         const int m0 = tr.tm * BM, n0 = tr.tn * BN;
         // Next K block into registers while this one is computed; shared
         // tiles double-buffered, one barrier per K block.
-        float ra[4], rb[4];
+        float ra[PER], rb[PER];
         auto load = [&](int k0) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int e = tid + q * 256;
+            for (int q = 0; q < PER; ++q) {
+                const int e = tid + q * NT;
                 const int ar = e / BK, ac = e % BK;
                 const int gr = m0 + ar, gk = k0 + ac;
                 ra[q] = (gr < pr.M && gk < pr.K) ? A[(long long)gr * lda + gk] : 0.f;
@@ -414,13 +416,13 @@ static __global__ void __launch_bounds__(256) simt_grouped_sgemm(const SimtGroup
         };
         auto store = [&](int buf) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int e = tid + q * 256;
+            for (int q = 0; q < PER; ++q) {
+                const int e = tid + q * NT;
                 As[buf][e % BK][e / BK] = ra[q];
                 Bs[buf][e / BN][e % BN] = rb[q];
             }
         };
-        float acc[4][4] = {};
+        float acc[4][8] = {};
         const int kblocks = (pr.K + BK - 1) / BK;
         load(0);
         __syncthreads();  // the previous tile's readers are done with buffer 0
@@ -432,12 +434,14 @@ static __global__ void __launch_bounds__(256) simt_grouped_sgemm(const SimtGroup
 #pragma unroll
             for (int kk = 0; kk < BK; ++kk) {
                 const float4 a4 = *reinterpret_cast<const float4*>(&As[cur][kk][ty * 4]);
-                const float4 b4 = *reinterpret_cast<const float4*>(&Bs[cur][kk][tx * 4]);
-                const float af[4] = {a4.x, a4.y, a4.z, a4.w}, bf[4] = {b4.x, b4.y, b4.z, b4.w};
+                const float4 b0 = *reinterpret_cast<const float4*>(&Bs[cur][kk][tx * 4]);
+                const float4 b1 = *reinterpret_cast<const float4*>(&Bs[cur][kk][32 + tx * 4]);
+                const float af[4] = {a4.x, a4.y, a4.z, a4.w};
+                const float bf[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(af[i], bf[j], acc[i][j]);
+                    for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(af[i], bf[j], acc[i][j]);
             }
             if (kb + 1 < kblocks) store(cur ^ 1);
             __syncthreads();
@@ -448,8 +452,8 @@ static __global__ void __launch_bounds__(256) simt_grouped_sgemm(const SimtGroup
             const int gr = m0 + ty * 4 + i;
             if (gr >= pr.M) continue;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int gc = n0 + tx * 4 + j;
+            for (int j = 0; j < 8; ++j) {
+                const int gc = n0 + (j / 4) * 32 + tx * 4 + (j % 4);
                 if (gc >= pr.N) continue;
                 float* p = C + (long long)gr * pr.ldc + gc;
                 float o = g.alpha * acc[i][j];
