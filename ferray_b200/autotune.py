@@ -37,7 +37,7 @@ SPLITS = [1, 2, 4, 8, 16]
 MARGIN = 1.03  # a candidate must beat the untuned kernel by 3%
 # tile edge per variant (output tiles per block row / column)
 TILES = {"i8": [(128, 256), (128, 128), (256, 256), (256, 512)], "split_f32": [(128, 128), (128, 64), (256, 128)],
-         "f64": [(128, 128), (64, 64), (32, 128), (128, 32), (128, 128)],
+         "f64": [(128, 128), (64, 64), (32, 128), (128, 32), (128, 128), (32, 256)],
          "f32": [(128, 128), (64, 64), (32, 128), (128, 32), (128, 128), (32, 256)]}
 # K per split unit: one tcgen05 K block, or the SIMT split granularity
 KUNIT = {"i8": 128, "split_f32": 64, "f64": 64, "f32": 64}

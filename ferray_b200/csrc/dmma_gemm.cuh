@@ -27,13 +27,20 @@ namespace fg {
 #ifndef FG_DMMA_BK
 #define FG_DMMA_BK 16
 #endif
-struct DmmaCfg {
-    static constexpr int BM = 128, BN = 128, BK = FG_DMMA_BK, STAGES = 3, THREADS = 256;
+// WARPS_M x WARPS_N warps, each MT x 4 MMA tiles of 8 x 8 (MT * 8 rows x 32
+// columns); BM = WARPS_M * MT * 8, BN = WARPS_N * 32.
+template <int WARPS_M_, int WARPS_N_, int MT_>
+struct DmmaTile {
+    static constexpr int WARPS_M = WARPS_M_, WARPS_N = WARPS_N_, MT = MT_;
+    static constexpr int BM = WARPS_M * MT * 8, BN = WARPS_N * 32, BK = FG_DMMA_BK, STAGES = 3, THREADS = 256;
+    static_assert(WARPS_M * WARPS_N == 8, "256 threads");
     static constexpr int APAD = 4, BPAD = 4;
     static constexpr int A_ELEMS = BM * (BK + APAD);
     static constexpr int B_ELEMS = BK * (BN + BPAD);
     static constexpr size_t SMEM = size_t(STAGES) * (A_ELEMS + B_ELEMS) * sizeof(double);
 };
+using DmmaCfg = DmmaTile<2, 4, 8>;        // 128 x 128, warps of 64 x 32
+using DmmaSkinnyCfg = DmmaTile<1, 8, 4>;  // 32 x 256 for few rows, warps of 32 x 32
 
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
     const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
@@ -53,12 +60,13 @@ __device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
                  : "d"(a), "d"(b));
 }
 
-__global__ void __launch_bounds__(DmmaCfg::THREADS, 1)
+template <class Cfg>
+__global__ void __launch_bounds__(256, 1)
     dmma_gemm_f64_kernel(int M, int N, int K, double alpha, const double* __restrict__ A,
                          long long lda, const double* __restrict__ B, long long ldb, double beta,
                          double* __restrict__ C, long long ldc, BatchMap bm, int nbatch,
                          int ksplit) {
-    using Cfg = DmmaCfg;
+    constexpr int MT = Cfg::MT;
     extern __shared__ __align__(16) double dsm[];
     double* As = dsm;                                  // [STAGES][BM][BK + APAD]
     double* Bs = dsm + Cfg::STAGES * Cfg::A_ELEMS;     // [STAGES][BK][BN + BPAD]
@@ -73,7 +81,7 @@ __global__ void __launch_bounds__(DmmaCfg::THREADS, 1)
     K = min(K - k_begin, ksplit);
 
     const int tid = threadIdx.x, lane = tid % 32, warp = tid / 32;
-    const int wm = warp / 4, wn = warp % 4;  // 2 x 4 warps of 64 x 32
+    const int wm = warp / Cfg::WARPS_N, wn = warp % Cfg::WARPS_N;  // warps of MT * 8 x 32
     const int m0 = blockIdx.y * Cfg::BM, n0 = blockIdx.x * Cfg::BN;
     const int kblocks = (K + Cfg::BK - 1) / Cfg::BK;
 
@@ -93,16 +101,16 @@ __global__ void __launch_bounds__(DmmaCfg::THREADS, 1)
 #pragma unroll
         for (int i = 0; i < Cfg::BK * Cfg::BN / 256; ++i) {
             const int e = tid + 256 * i;
-            const int r = e / Cfg::BN, c = e % Cfg::BN;  // B: 128 n per row
+            const int r = e / Cfg::BN, c = e % Cfg::BN;  // B: BN n per row
             const int gk = k0 + r, gn = n0 + c;
             const bool ok = gk < K && gn < N;
             cp_async8(bs + r * (Cfg::BN + Cfg::BPAD) + c, ok ? B + (long long)gk * ldb + gn : B, ok);
         }
     };
 
-    double acc[8][4][2];
+    double acc[MT][4][2];
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
+    for (int i = 0; i < MT; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
@@ -124,15 +132,15 @@ __global__ void __launch_bounds__(DmmaCfg::THREADS, 1)
         const double* bs = Bs + (kb % Cfg::STAGES) * Cfg::B_ELEMS;
 #pragma unroll
         for (int kk = 0; kk < Cfg::BK; kk += 4) {
-            double af[8], bf[4];
+            double af[MT], bf[4];
 #pragma unroll
-            for (int i = 0; i < 8; ++i)
-                af[i] = as[(wm * 64 + i * 8 + fr) * (Cfg::BK + Cfg::APAD) + kk + fc];
+            for (int i = 0; i < MT; ++i)
+                af[i] = as[(wm * MT * 8 + i * 8 + fr) * (Cfg::BK + Cfg::APAD) + kk + fc];
 #pragma unroll
             for (int j = 0; j < 4; ++j)
                 bf[j] = bs[(kk + fc) * (Cfg::BN + Cfg::BPAD) + wn * 32 + j * 8 + fr];
 #pragma unroll
-            for (int i = 0; i < 8; ++i)
+            for (int i = 0; i < MT; ++i)
 #pragma unroll
                 for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j], af[i], bf[j]);
         }
@@ -140,8 +148,8 @@ __global__ void __launch_bounds__(DmmaCfg::THREADS, 1)
     cp_async_wait<0>();
 
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const int r = m0 + wm * 64 + i * 8 + fr;
+    for (int i = 0; i < MT; ++i) {
+        const int r = m0 + wm * MT * 8 + i * 8 + fr;
         if (r >= M) continue;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {

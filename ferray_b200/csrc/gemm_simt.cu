@@ -70,13 +70,14 @@ static fg_status launch_simt_real(const Gemm& g, BatchMap bm, int splits_want, c
 }
 
 // Plain DGEMM on the FP64 tensor path (DMMA), same split-K scheme.
+template <class Cfg = DmmaCfg>
 static fg_status launch_dmma(fg_ctx* ctx, const Gemm& g, BatchMap bm, int splits_want, cudaStream_t st) {
     (void)ctx;
     static std::once_flag once;
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(once, [] {
-        attr_err = cudaFuncSetAttribute(dmma_gemm_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(DmmaCfg::SMEM));
+        attr_err = cudaFuncSetAttribute(dmma_gemm_f64_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(Cfg::SMEM));
     });
     FG_CUDA(attr_err);
     constexpr long long KUNIT = 64;
@@ -85,11 +86,11 @@ static fg_status launch_dmma(fg_ctx* ctx, const Gemm& g, BatchMap bm, int splits
     const int splits = plan_splits(splits_want, static_cast<int>(kunits), g.M * g.N * g.batch,
                                    sizeof(double), &kps);
     if ((long long)splits * g.batch > 65535) return set_error(FG_ERR_UNSUPPORTED, "batch above 65535");
-    dim3 grid((g.N + DmmaCfg::BN - 1) / DmmaCfg::BN, (g.M + DmmaCfg::BM - 1) / DmmaCfg::BM, g.batch * splits);
+    dim3 grid((g.N + Cfg::BN - 1) / Cfg::BN, (g.M + Cfg::BM - 1) / Cfg::BM, g.batch * splits);
     const double* A = static_cast<const double*>(g.A);
     const double* B = static_cast<const double*>(g.B);
     if (splits <= 1) {
-        dmma_gemm_f64_kernel<<<grid, DmmaCfg::THREADS, DmmaCfg::SMEM, st>>>(
+        dmma_gemm_f64_kernel<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM, st>>>(
             (int)g.M, (int)g.N, (int)g.K, g.alpha_re, A, g.lda, B, g.ldb, g.beta_re,
             static_cast<double*>(g.C), g.ldc, bm, g.batch, (int)g.K);
         count_launch();
@@ -101,7 +102,7 @@ static fg_status launch_dmma(fg_ctx* ctx, const Gemm& g, BatchMap bm, int splits
     FG_TRY(ws.alloc(static_cast<size_t>(splits * out_elems) * sizeof(double), st));
     BatchMap wbm = bm;
     wbm.c_bstride = g.M * g.N;
-    dmma_gemm_f64_kernel<<<grid, DmmaCfg::THREADS, DmmaCfg::SMEM, st>>>(
+    dmma_gemm_f64_kernel<Cfg><<<grid, Cfg::THREADS, Cfg::SMEM, st>>>(
         (int)g.M, (int)g.N, (int)g.K, 1.0, A, g.lda, B, g.ldb, 0.0, static_cast<double*>(ws.p), g.N, wbm,
         g.batch, (int)(kps * KUNIT));
     splitk_reduce_kernel<double><<<grid_for(out_elems), 256, 0, st>>>(
@@ -243,6 +244,7 @@ fg_status launch_simt(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
                 case 2: return launch_simt_real<double, 2, 8>(g, bm, c.splits, st);
                 case 3: return launch_simt_real<double, 8, 2>(g, bm, c.splits, st);
                 case 4: return launch_dmma(ctx, g, bm, c.splits, st);
+                case 5: return launch_dmma<DmmaSkinnyCfg>(ctx, g, bm, c.splits, st);
                 default: return launch_simt_real<double, 8, 8>(g, bm, c.splits, st);
             }
         }

@@ -17,7 +17,7 @@ struct TuneEntry {
 // kTuneTable[op][bm][bn][bk]; generated by ferray_b200/autotune.py.
 #include "tune_table.inc"
 
-constexpr int kVariants[TUNE_OPS] = {4, 3, 5, 6};
+constexpr int kVariants[TUNE_OPS] = {4, 3, 6, 6};
 
 std::atomic<int> g_force_variant[TUNE_OPS] = {{-1}, {-1}, {-1}, {-1}};
 std::atomic<int> g_force_splits[TUNE_OPS] = {{1}, {1}, {1}, {1}};

@@ -72,7 +72,7 @@ def test_tune_table_lookup_and_force_without_device():
     from ferray_b200 import _lib, autotune
     lib = _lib.load()
     n = C.c_int()
-    for op, want in zip(range(4), (4, 3, 5, 6)):
+    for op, want in zip(range(4), (4, 3, 6, 6)):
         assert lib.fg_tune_variants(op, C.byref(n)) == 0 and n.value == want
     assert lib.fg_tune_variants(9, C.byref(n)) == _lib.FG_ERR_INVALID
     # every shape maps to a valid choice
@@ -88,7 +88,7 @@ def test_tune_table_lookup_and_force_without_device():
     assert fg.tune_lookup("i8", 300, 300, 5000) == before
     assert lib.fg_tune_force(0, 4, 1) == _lib.FG_ERR_INVALID
     assert lib.fg_tune_force(1, 3, 1) == _lib.FG_ERR_INVALID
-    assert lib.fg_tune_force(2, 5, 1) == _lib.FG_ERR_INVALID
+    assert lib.fg_tune_force(2, 6, 1) == _lib.FG_ERR_INVALID
     assert lib.fg_tune_force(3, 6, 1) == _lib.FG_ERR_INVALID
     assert lib.fg_tune_force(0, 0, 17) == _lib.FG_ERR_INVALID
     # the compiled-in table is the committed include: check one entry per op

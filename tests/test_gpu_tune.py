@@ -80,7 +80,7 @@ def test_split_f32_variants(fg, oracle, variant, splits, m, n, k):
                                            + 2 * U32 * np.linalg.norm(ref))
 
 
-@pytest.mark.parametrize("op,dt,u,variant", [("f64", np.float64, U64, v) for v in range(5)] +
+@pytest.mark.parametrize("op,dt,u,variant", [("f64", np.float64, U64, v) for v in range(6)] +
                          [("f32", np.float32, U32, v) for v in range(6)])
 @pytest.mark.parametrize("splits", SPLITS)
 @pytest.mark.parametrize("m,n,k", SHAPES + [(257, 300, 501)])
@@ -209,3 +209,21 @@ def test_cgemm_real_embedding_on_ffma(fg, oracle, m, n, k):
             assert fg.gemm_c32(m, n, k, 0.5, 0.0, a, b, -1.0, 0.0, c)
             ref = 0.5 * exact - c0.astype(np.complex128)
             assert np.linalg.norm(c - ref) <= (2 * k + 4) * U32 * scale + 2 * U32 * np.linalg.norm(ref)
+
+
+@pytest.mark.parametrize("splits", [1, 4])
+@pytest.mark.parametrize("m,n,k", [(32, 600, 2000), (17, 300, 77), (70, 257, 500)])
+def test_dmma_skinny_bit_identical(fg, m, n, k, splits):
+    """f64 variant 5 (DMMA, 32 x 256 tiles of 32 x 32 warp tiles) runs the
+    same m8n8k4 MMA sequence per output as variant 4: same bits."""
+    r = rng(m * 7 + n + k)
+    a = r.standard_normal((m, k))
+    b = r.standard_normal((k, n))
+    c0 = r.standard_normal((m, n))
+    out = []
+    for variant in (4, 5):
+        with fg.tune_forced("f64", variant, splits):
+            c = c0.copy()
+            assert fg.gemm_f64(m, n, k, 0.75, a, b, -1.5, c)
+            out.append(c)
+    np.testing.assert_array_equal(out[0], out[1])
