@@ -79,7 +79,9 @@ def test_tune_table_lookup_and_force_without_device():
     for op in fg.TUNE_OPS:
         for m, nn, k in [(1, 1, 1), (128, 129, 8192), (5000, 70, 100000)]:
             v, s = fg.tune_lookup(op, m, nn, k)
-            assert 0 <= v < 5 and 1 <= s <= 16
+            n = C.c_int()
+            assert lib.fg_tune_variants(fg.TUNE_OPS[op], C.byref(n)) == 0
+            assert 0 <= v < n.value and 1 <= s <= 16
     # forced choices win everywhere, then the table comes back
     before = fg.tune_lookup("i8", 300, 300, 5000)
     with fg.tune_forced("i8", 1, 8):
