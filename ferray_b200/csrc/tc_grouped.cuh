@@ -311,20 +311,31 @@ struct PrepSeg {
 // One 16-byte destination chunk of segment row r at byte / element offset c.
 __device__ __forceinline__ void prep_chunk(const PrepSeg& sg, long long r, long long c) {
     if (sg.op == 0) {
-        const uint8_t* src = static_cast<const uint8_t*>(sg.src) + r * sg.ld_src;
-        uint32_t w[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            uint32_t v = 0;
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const long long cc = c + 4 * q + j;
-                if (cc < sg.cols) v |= static_cast<uint32_t>(__ldg(src + cc)) << (8 * j);
+        // 16 bytes of an unaligned row from the one or two aligned 16-byte
+        // granules that hold them: a granule is read only when it holds a
+        // byte of the row, so every read stays on memory the row occupies.
+        // Bytes past the row end become 0.
+        const uint8_t* src = static_cast<const uint8_t*>(sg.src) + r * sg.ld_src + c;
+        const long long valid = sg.cols - c;  // bytes of the row from c on
+        unsigned long long o0 = 0, o1 = 0;
+        if (valid > 0) {
+            const uintptr_t a = reinterpret_cast<uintptr_t>(src);
+            const uintptr_t base = a & ~static_cast<uintptr_t>(15);
+            const int sh = static_cast<int>(a - base);
+            const ulonglong2 w0 = __ldg(reinterpret_cast<const ulonglong2*>(base));
+            ulonglong2 w1 = make_ulonglong2(0ull, 0ull);
+            if (sh + valid > 16) w1 = __ldg(reinterpret_cast<const ulonglong2*>(base + 16));
+            const bool hi = sh >= 8;
+            const unsigned long long x0 = hi ? w0.y : w0.x, x1 = hi ? w1.x : w0.y, x2 = hi ? w1.y : w1.x;
+            const int sb = (sh & 7) * 8;
+            o0 = sb ? (x0 >> sb) | (x1 << (64 - sb)) : x0;
+            o1 = sb ? (x1 >> sb) | (x2 << (64 - sb)) : x1;
+            if (valid < 16) {
+                o1 = valid <= 8 ? 0ull : (o1 & ((1ull << (8 * (valid - 8))) - 1));
+                if (valid < 8) o0 &= (1ull << (8 * valid)) - 1;
             }
-            w[q] = v;
         }
-        *reinterpret_cast<uint4*>(static_cast<uint8_t*>(sg.dst0) + r * sg.ld_dst + c) =
-            make_uint4(w[0], w[1], w[2], w[3]);
+        *reinterpret_cast<ulonglong2*>(static_cast<uint8_t*>(sg.dst0) + r * sg.ld_dst + c) = make_ulonglong2(o0, o1);
     } else {
         const float* src = static_cast<const float*>(sg.src) + r * sg.ld_src;
         __align__(16) __nv_bfloat16 h[8], l[8];
