@@ -370,6 +370,38 @@ def test_host_path_row_panels_f32_beta(fg, oracle, mode):
     assert err <= tol + 2 * U32 * np.linalg.norm(ref) * blow / scale
 
 
+def test_host_path_column_panels_i8_exact(fg):
+    # 230 MB: 4 row panels, so B and C also go in 4 column panels (2-D copies)
+    m, n, k = 12000, 4096, 2048
+    r = rng(23)
+    a = r.integers(-128, 128, (m, k), dtype=np.int8)
+    b = r.integers(-128, 128, (k, n), dtype=np.int8)
+    c0 = r.integers(-2 ** 20, 2 ** 20, (m, n), dtype=np.int32)
+    want = (a.astype(np.float64) @ b.astype(np.float64)).astype(np.int64)
+    c = c0.copy()
+    assert fg.gemm_i8_signed(m, n, k, a, b, c, accumulate=True)
+    np.testing.assert_array_equal(c, (want + c0).astype(np.int32))
+
+
+def test_host_path_column_panels_f32_beta(fg, oracle):
+    # ragged last column panel (n = 4000 -> 1024-column panels, the last 928)
+    m, n, k = 12000, 4000, 1024
+    r = rng(24)
+    a = r.standard_normal((m, k), dtype=np.float32)
+    b = r.standard_normal((k, n), dtype=np.float32)
+    c0 = r.standard_normal((m, n), dtype=np.float32)
+    c = c0.copy()
+    assert fg.gemm_f32(m, n, k, 1.5, a, b, -0.5, c)
+    rows, cols = oracle.sample_indices(m, n, 64, 64, seed=4)
+    cols = np.unique(np.concatenate([cols, [0, 1023, 1024, 3071, 3072, 3999]]))
+    ref = 1.5 * oracle.dd_sampled(a, b, rows, cols) - 0.5 * c0[np.ix_(rows, cols)].astype(np.float64)
+    got = c[np.ix_(rows, cols)]
+    scale = np.linalg.norm(a.astype(np.float64)) * np.linalg.norm(b.astype(np.float64))
+    blow = np.sqrt(m * n / got.size)
+    err = np.linalg.norm(got - ref) * blow / scale
+    assert err <= (k + 4) * U32 + 2 * U32 * np.linalg.norm(ref) * blow / scale
+
+
 # ------------------------------------------------------------------ GEMV
 @pytest.mark.parametrize("dt,u", [(np.float64, U64), (np.float32, U32)])
 @pytest.mark.parametrize("m,n,k", [(1, 1, 1), (300, 1, 1001), (8192, 1, 4096), (1, 300, 1001),
