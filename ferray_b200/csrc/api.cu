@@ -539,22 +539,11 @@ fg_status fg_gemm_host(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, int slices, si
     long long rows = ((long long)m + panels - 1) / panels;
     rows = (rows + 255) / 256 * 256;
     panels = ((long long)m + rows - 1) / rows;
-    // Large calls also split B and C into 4 column panels, B uploaded panel
-    // by panel after A's first rows: C tiles then start their copy back
-    // while most inputs are still on the way, so both PCIe directions run
-    // concurrently for most of the call instead of only its second half.
-    long long ncp = 1, cols = static_cast<long long>(n);
-    if (panels >= 4 && n >= 1024) {
-        cols = ((static_cast<long long>(n) + 3) / 4 + 127) / 128 * 128;
-        ncp = (static_cast<long long>(n) + cols - 1) / cols;
-    }
+    if (ib) FG_CUDA(cudaMemcpyAsync(sb.p, b, ib, cudaMemcpyHostToDevice, s_in));
     uint8_t* da = static_cast<uint8_t*>(sa.p);
-    uint8_t* db = static_cast<uint8_t*>(sb.p);
     uint8_t* dc = static_cast<uint8_t*>(sc.p);
     const uint8_t* ha = static_cast<const uint8_t*>(a);
-    const uint8_t* hb = static_cast<const uint8_t*>(b);
     uint8_t* hc = static_cast<uint8_t*>(c);
-    if (ncp == 1 && ib) FG_CUDA(cudaMemcpyAsync(db, hb, ib, cudaMemcpyHostToDevice, s_in));
     // The last panel's GEMM and copy-out run after every input has arrived,
     // so the schedule ends on a 256-row piece to keep that tail short.
     std::vector<std::pair<size_t, size_t>> parts;  // (first row, rows)
@@ -568,37 +557,23 @@ fg_status fg_gemm_host(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, int slices, si
         parts.emplace_back(r0, mi);
         r0 += mi;
     }
-    const size_t bpitch = n * ein, cpitch = n * eout;
-    for (long long jp = 0; jp < ncp; ++jp) {
-        const size_t j0 = static_cast<size_t>(jp * cols);
-        const size_t nj = std::min<size_t>(n - j0, static_cast<size_t>(cols));
-        if (ncp > 1 && k)
-            FG_CUDA(cudaMemcpy2DAsync(db + j0 * ein, bpitch, hb + j0 * ein, bpitch, nj * ein, k,
-                                      cudaMemcpyHostToDevice, s_in));
-        for (const auto& part : parts) {
-            const size_t r0 = part.first, mi = part.second;
-            const size_t oa = r0 * k * ein, na = mi * k * ein, oc = r0 * cpitch + j0 * eout;
-            if (jp == 0 && na) FG_CUDA(cudaMemcpyAsync(da + oa, ha + oa, na, cudaMemcpyHostToDevice, s_in));
-            if (reads_c)
-                FG_CUDA(cudaMemcpy2DAsync(dc + oc, cpitch, hc + oc, cpitch, nj * eout, mi,
-                                          cudaMemcpyHostToDevice, s_in));
-            cudaEvent_t in_ready, out_ready;
-            FG_CUDA(cudaEventCreateWithFlags(&in_ready, cudaEventDisableTiming));
-            cudaEventRecord(in_ready, s_in);  // after this tile's B columns, A rows and C tile
-            cudaStreamWaitEvent(s_cmp, in_ready, 0);
-            cudaEventDestroy(in_ready);
-            FG_TRY(fg_gemm(ctx, dtype, mode, slices, mi, nj, k, alpha, da + oa, k, db + j0 * ein, n, beta,
-                           dc + oc, n, accumulate, s_cmp));
-            FG_CUDA(cudaEventCreateWithFlags(&out_ready, cudaEventDisableTiming));
-            cudaEventRecord(out_ready, s_cmp);
-            cudaStreamWaitEvent(s_out, out_ready, 0);
-            cudaEventDestroy(out_ready);
-            if (ncp == 1)
-                FG_CUDA(cudaMemcpyAsync(hc + oc, dc + oc, mi * cpitch, cudaMemcpyDeviceToHost, s_out));
-            else
-                FG_CUDA(cudaMemcpy2DAsync(hc + oc, cpitch, dc + oc, cpitch, nj * eout, mi,
-                                          cudaMemcpyDeviceToHost, s_out));
-        }
+    for (const auto& part : parts) {
+        const size_t r0 = part.first, mi = part.second;
+        const size_t oa = r0 * k * ein, na = mi * k * ein, oc = r0 * n * eout, nc = mi * n * eout;
+        if (na) FG_CUDA(cudaMemcpyAsync(da + oa, ha + oa, na, cudaMemcpyHostToDevice, s_in));
+        if (reads_c) FG_CUDA(cudaMemcpyAsync(dc + oc, hc + oc, nc, cudaMemcpyHostToDevice, s_in));
+        cudaEvent_t in_ready, out_ready;
+        FG_CUDA(cudaEventCreateWithFlags(&in_ready, cudaEventDisableTiming));
+        cudaEventRecord(in_ready, s_in);  // after B and this panel's copies
+        cudaStreamWaitEvent(s_cmp, in_ready, 0);
+        cudaEventDestroy(in_ready);
+        FG_TRY(fg_gemm(ctx, dtype, mode, slices, mi, n, k, alpha, da + oa, k, sb.p, n, beta,
+                       dc + oc, n, accumulate, s_cmp));
+        FG_CUDA(cudaEventCreateWithFlags(&out_ready, cudaEventDisableTiming));
+        cudaEventRecord(out_ready, s_cmp);
+        cudaStreamWaitEvent(s_out, out_ready, 0);
+        cudaEventDestroy(out_ready);
+        FG_CUDA(cudaMemcpyAsync(hc + oc, dc + oc, nc, cudaMemcpyDeviceToHost, s_out));
     }
     FG_CUDA(cudaStreamSynchronize(s_out));
     FG_CUDA(cudaStreamSynchronize(s_cmp));

@@ -370,8 +370,8 @@ def test_host_path_row_panels_f32_beta(fg, oracle, mode):
     assert err <= tol + 2 * U32 * np.linalg.norm(ref) * blow / scale
 
 
-def test_host_path_column_panels_i8_exact(fg):
-    # 230 MB: 4 row panels, so B and C also go in 4 column panels (2-D copies)
+def test_host_path_many_panels_i8_exact(fg):
+    # 230 MB of operands and result: 4 row panels, the last cut to 256 rows
     m, n, k = 12000, 4096, 2048
     r = rng(23)
     a = r.integers(-128, 128, (m, k), dtype=np.int8)
@@ -383,8 +383,8 @@ def test_host_path_column_panels_i8_exact(fg):
     np.testing.assert_array_equal(c, (want + c0).astype(np.int32))
 
 
-def test_host_path_column_panels_f32_beta(fg, oracle):
-    # ragged last column panel (n = 4000 -> 1024-column panels, the last 928)
+def test_host_path_many_panels_f32_beta(fg, oracle):
+    # 262 MB, beta != 0 (C is read through the panels); n not a power of two
     m, n, k = 12000, 4000, 1024
     r = rng(24)
     a = r.standard_normal((m, k), dtype=np.float32)
