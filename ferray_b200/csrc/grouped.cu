@@ -128,7 +128,7 @@ fg_status grouped_job_build(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, const fg_
     // longest K first: the static strided tile walk then balances SMs
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return table[x].k > table[y].k; });
     const int np = static_cast<int>(order.size());
-    const int bm = j->kind == 0 ? 64 : 128, bn = bm;
+    const int bm = j->kind == 0 ? 64 : 128;
     j->probs_in.resize(np);
     j->probs.resize(np);
     j->oa.resize(np);
@@ -141,8 +141,17 @@ fg_status grouped_job_build(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, const fg_
         g.M = static_cast<int>(q.m);
         g.N = static_cast<int>(q.n);
         g.K = static_cast<int>(q.k);
-        g.tiles_m = static_cast<int>((q.m + bm - 1) / bm);
-        g.tiles_n = static_cast<int>((q.n + bn - 1) / bn);
+        // plain FP32: a 32 x 32 tile where it pads at most 0.7x the area a
+        // 64 x 64 one does (small problems; its FMAs cost more each)
+        int tb = bm;
+        if (j->kind == 0) {
+            const long long a64 = (q.m + 63) / 64 * 64 * ((q.n + 63) / 64 * 64);
+            const long long a32 = (q.m + 31) / 32 * 32 * ((q.n + 31) / 32 * 32);
+            if (10 * a32 <= 7 * a64) tb = 32;
+        }
+        g.tile = tb;
+        g.tiles_m = static_cast<int>((q.m + tb - 1) / tb);
+        g.tiles_n = static_cast<int>((q.n + tb - 1) / tb);
         g.tile_start = j->total_tiles;
         j->total_tiles += (long long)g.tiles_m * g.tiles_n;
         g.C = q.c;

@@ -21,6 +21,7 @@ struct GroupedProblem {
     long long tile_start;  // first global tile of this problem
     void* C;
     long long ldc;         // elements
+    int tile;              // plain FP32 batches: square tile edge, 64 or 32
 };
 
 // Per global tile: problem index, tile row, tile column (written by the host
@@ -395,6 +396,76 @@ struct SimtGroupedArgs {
     float alpha, beta;
 };
 
+// A 32 x 32 tile of a small problem on the same 128 threads: 2 rows x 4
+// columns a thread, the same double-buffered K blocks of 16 and the same
+// per-output k order (one FMA per product, k ascending).  Uses the caller's
+// shared tiles (the first 32 columns of each row).
+__device__ __forceinline__ void grouped_tile32(const SimtGroupedArgs& g, const GroupedProblem& pr,
+                                               const float* __restrict__ A, const float* __restrict__ B,
+                                               long long lda, long long ldb, int m0, int n0,
+                                               float (*As)[16][68], float (*Bs)[16][68]) {
+    constexpr int BK = 16;
+    const int tid = threadIdx.x, tx = tid % 8, ty = tid / 8;
+    float ra[4], rb[4];
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int e = tid + q * 128;  // 512 elements of each 32 x 16 / 16 x 32 tile
+            const int ar = e / BK, ac = e % BK;
+            const int gr = m0 + ar, gk = k0 + ac;
+            ra[q] = (gr < pr.M && gk < pr.K) ? A[(long long)gr * lda + gk] : 0.f;
+            const int br = e / 32, bc = e % 32;
+            const int gk2 = k0 + br, gn = n0 + bc;
+            rb[q] = (gk2 < pr.K && gn < pr.N) ? B[(long long)gk2 * ldb + gn] : 0.f;
+        }
+    };
+    auto store = [&](int buf) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int e = tid + q * 128;
+            As[buf][e % BK][e / BK] = ra[q];
+            Bs[buf][e / 32][e % 32] = rb[q];
+        }
+    };
+    float acc[2][4] = {};
+    const int kblocks = (pr.K + BK - 1) / BK;
+    load(0);
+    __syncthreads();  // the previous tile's readers are done with buffer 0
+    store(0);
+    __syncthreads();
+    for (int kb = 0; kb < kblocks; ++kb) {
+        const int cur = kb & 1;
+        if (kb + 1 < kblocks) load((kb + 1) * BK);
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            const float2 a2 = *reinterpret_cast<const float2*>(&As[cur][kk][ty * 2]);
+            const float4 b4 = *reinterpret_cast<const float4*>(&Bs[cur][kk][tx * 4]);
+            const float af[2] = {a2.x, a2.y}, bf[4] = {b4.x, b4.y, b4.z, b4.w};
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(af[i], bf[j], acc[i][j]);
+        }
+        if (kb + 1 < kblocks) store(cur ^ 1);
+        __syncthreads();
+    }
+    float* C = static_cast<float*>(pr.C);
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const int gr = m0 + ty * 2 + i;
+        if (gr >= pr.M) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int gc = n0 + tx * 4 + j;
+            if (gc >= pr.N) continue;
+            float* p = C + (long long)gr * pr.ldc + gc;
+            float o = g.alpha * acc[i][j];
+            if (g.beta != 0.f) o = fmaf(g.beta, *p, o);
+            *p = o;
+        }
+    }
+}
+
 static __global__ void __launch_bounds__(128) simt_grouped_sgemm(const SimtGroupedArgs g) {
     constexpr int BM = 64, BN = 64, BK = 16, NT = 128;
     constexpr int PER = BM * BK / NT;  // elements of each operand a thread loads per K block
@@ -409,6 +480,10 @@ static __global__ void __launch_bounds__(128) simt_grouped_sgemm(const SimtGroup
         const float* A = static_cast<const float*>(g.a[pi]);
         const float* B = static_cast<const float*>(g.b[pi]);
         const long long lda = g.lda[pi], ldb = g.ldb[pi];
+        if (pr.tile == 32) {
+            grouped_tile32(g, pr, A, B, lda, ldb, tr.tm * 32, tr.tn * 32, As, Bs);
+            continue;
+        }
         const int m0 = tr.tm * BM, n0 = tr.tn * BN;
         // Next K block into registers while this one is computed; shared
         // tiles double-buffered, one barrier per K block.
