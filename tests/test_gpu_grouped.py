@@ -57,7 +57,7 @@ def test_grouped_one_shot(fg, oracle, dtype, mode):
     check(fg, oracle, probs, host, dtype, mode)
 
 
-@pytest.mark.parametrize("dtype,mode", [(np.int8, "plain"), (np.float32, "split")])
+@pytest.mark.parametrize("dtype,mode", [(np.int8, "plain"), (np.float32, "split"), (np.float32, "plain")])
 def test_grouped_plan_replay(fg, oracle, dtype, mode):
     rng = np.random.default_rng(12)
     dims = ragged_dims(rng, 64)
