@@ -94,6 +94,15 @@ def reference_peaks(n=8192):
     return {"reference_peaks": out, "n": n, "how": "best of 5 after 3 warm-ups, CUDA events"}
 
 
+def max_over_ranks(dist, torch, x, device="cuda"):
+    """The largest of every rank's x (the job's time is its slowest rank's);
+    every rank gets it.  `device` is where the reduction tensor lives: cuda
+    for NCCL, cpu for gloo."""
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_env():
     return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
             int(os.environ.get("LOCAL_RANK", "0")))
@@ -577,9 +586,7 @@ def main():
         launches = fg.launch_count() - lc0
         ms = e0.elapsed_time(e1) / steps
         if dist:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+            ms = max_over_ranks(dist, torch, ms)
             dist.barrier()
         return ms, launches, prof
 
@@ -647,9 +654,7 @@ def main():
             assert st == 0, lib.fg_last_error()
         dt = (time.perf_counter() - t0) / k
         if dist:
-            t = torch.tensor([dt], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dt = float(t.item())
+            dt = max_over_ranks(dist, torch, dt)
         for arr in (a_h, b_h, c_h):
             lib.fg_host_unregister(ctx.handle, arr.ctypes.data)
         e2e = {"value": round(world * flops / dt / 1e12, 3), "unit": "TFLOP/s",

@@ -31,7 +31,7 @@ __all__ = [
     "gemm_i8_signed", "gemm_i16", "gemm_bf16_f32", "gemm_f16_f32", "quantized_matmul", "matmul", "matmul_complex",
     "gemm_batched_strided", "gemm_grouped", "GroupedPlan", "Server", "launch_count", "PLAIN",
     "SPLIT", "TUNE_OPS", "tune_lookup", "tune_forced", "multi_dot", "multi_dot_order", "matrix_power", "tensordot", "einsum",
-    "trsm_left_lower_f64", "trsm_left_upper_f64", "trsm_left_lower_f32", "trsm_left_upper_f32", "npy_parse", "npy_load", "npz_names", "npz_read", "npz_load",
+    "trsm_left_lower_f64", "trsm_left_upper_f64", "trsm_left_lower_f32", "trsm_left_upper_f32", "npy_parse", "npy_load", "npz_names", "npz_read", "npz_load", "shard_problems",
 ]
 
 PLAIN, SPLIT = "plain", "split"
@@ -685,6 +685,28 @@ class tune_forced:
     def __exit__(self, *exc):
         L.load().fg_tune_force(self.op, -1, 1)
         return False
+
+
+def shard_problems(dims, world, rank):
+    """Indices of the problems of a ragged batch (rows of (m, n, k)) that rank
+    `rank` of `world` runs: longest-processing-time-first by 2mnk, each
+    problem to the least-loaded rank so far (lowest rank on ties).  Every
+    rank computes the same assignment from the same table, so sharding a
+    batch across GPUs needs no communication; the shards are disjoint, cover
+    every problem, and differ in load by at most one problem's work."""
+    if world < 1 or not 0 <= rank < world:
+        raise InvalidValue(f"rank {rank} outside a world of {world}")
+    d = np.asarray(dims, dtype=np.int64).reshape(-1, 3)
+    work = 2 * d[:, 0] * d[:, 1] * d[:, 2]
+    order = np.argsort(-work, kind="stable")
+    load = [0] * world
+    mine = []
+    for i in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        load[r] += int(work[i])
+        if r == rank:
+            mine.append(int(i))
+    return sorted(mine)
 
 
 def gemm_grouped(problems, dtype=np.float32, mode=PLAIN):

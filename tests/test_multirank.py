@@ -1,0 +1,69 @@
+"""The N > 1 host logic on CPU: two ranks over gloo (127.0.0.1) -- the
+max-over-ranks timing bench.py uses for every multi-GPU number, and the
+communication-free sharding of a ragged batch across GPUs."""
+import datetime
+import json
+import os
+import socket
+
+import numpy as np
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _ragged_dims():
+    rng = np.random.default_rng(42)
+    return np.rint(np.exp(rng.uniform(np.log(8), np.log(512), (4096, 3)))).astype(int)
+
+
+def _worker(rank, world, port, out_dir):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        import bench
+        import ferray_b200 as fg
+        slowest = bench.max_over_ranks(dist, torch, 1.5 + rank, device="cpu")
+        mine = fg.shard_problems(_ragged_dims(), world, rank)
+        shards = [None] * world
+        dist.all_gather_object(shards, mine)
+        with open(os.path.join(out_dir, "rank%d.json" % rank), "w") as f:
+            json.dump({"max": slowest, "shards": shards}, f)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_over_gloo(tmp_path):
+    world = 2
+    mp.spawn(_worker, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True)
+    res = [json.load(open(tmp_path / ("rank%d.json" % r))) for r in range(world)]
+    assert all(r["max"] == 2.5 for r in res)  # every rank sees the slowest rank's time
+    shards = res[0]["shards"]
+    assert res[1]["shards"] == shards  # both ranks agree without a data-path exchange
+    dims = _ragged_dims()
+    flat = sorted(i for s in shards for i in s)
+    assert flat == list(range(len(dims)))  # disjoint and complete
+    work = 2 * dims[:, 0] * dims[:, 1] * dims[:, 2]
+    loads = [int(work[s].sum()) for s in shards]
+    assert max(loads) - min(loads) <= int(work.max())
+
+
+def test_shard_problems_single_rank_and_errors():
+    import ferray_b200 as fg
+    dims = _ragged_dims()[:10]
+    assert fg.shard_problems(dims, 1, 0) == list(range(10))
+    for bad in ((2, 2), (0, 0), (2, -1)):
+        try:
+            fg.shard_problems(dims, *bad)
+        except fg.InvalidValue:
+            continue
+        raise AssertionError("accepted world=%d rank=%d" % bad)
