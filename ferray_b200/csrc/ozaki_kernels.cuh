@@ -47,25 +47,26 @@ __device__ __forceinline__ double scale_from_max_bits(unsigned long long bits) {
 }
 
 // Row maxima of a real (cplx = 0) or complex (cplx = 1: Re and Im) matrix,
-// one warp per row.
+// one warp per row (grid-stride over rows, so any grid covers every row).
 // `shift` (may be null) holds the balancing exponent of each K index: the row
 // maxima are those of A * diag(2^shift).
 static __global__ void ozaki_row_scale_kernel(const double* __restrict__ A, long long M,
                                               long long K, long long lda, int cplx,
                                               const int* __restrict__ shift,
                                               double* __restrict__ scale) {
-    const long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32;
     const int lane = threadIdx.x % 32;
-    if (row >= M) return;
+    const long long warps = (long long)gridDim.x * blockDim.x / 32;
     const long long len = cplx ? 2 * K : K;
-    const double* r = A + row * (cplx ? 2 * lda : lda);
-    unsigned long long mx = 0;
-    for (long long k = lane; k < len; k += 32) {
-        const int sh = shift ? shift[cplx ? (k >> 1) : k] : 0;
-        mx = max(mx, abs_bits(ldexp(r[k], sh)));
+    for (long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32; row < M; row += warps) {
+        const double* r = A + row * (cplx ? 2 * lda : lda);
+        unsigned long long mx = 0;
+        for (long long k = lane; k < len; k += 32) {
+            const int sh = shift ? shift[cplx ? (k >> 1) : k] : 0;
+            mx = max(mx, abs_bits(ldexp(r[k], sh)));
+        }
+        for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+        if (lane == 0) scale[row] = scale_from_max_bits(mx);
     }
-    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
-    if (lane == 0) scale[row] = scale_from_max_bits(mx);
 }
 
 // Column maxima, pass 1: each thread scans `rows_per` rows of one (complex:
@@ -114,19 +115,20 @@ static __global__ void ozaki_a_colmax_kernel(const double* __restrict__ A, long 
     atomicMax(out + k, mx);
 }
 
-// Pass 2: row maxima of B, one warp per row.
+// Pass 2: row maxima of B, one warp per row (grid-stride over rows).
 static __global__ void ozaki_b_rowmax_kernel(const double* __restrict__ B, long long K, long long N,
                                              long long ldb, int cplx,
                                              unsigned long long* __restrict__ out) {
-    const long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32;
     const int lane = threadIdx.x % 32;
-    if (row >= K) return;
+    const long long warps = (long long)gridDim.x * blockDim.x / 32;
     const long long len = cplx ? 2 * N : N;
-    const double* r = B + row * (cplx ? 2 * ldb : ldb);
-    unsigned long long mx = 0;
-    for (long long j = lane; j < len; j += 32) mx = max(mx, abs_bits(r[j]));
-    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
-    if (lane == 0) out[row] = mx;
+    for (long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32; row < K; row += warps) {
+        const double* r = B + row * (cplx ? 2 * ldb : ldb);
+        unsigned long long mx = 0;
+        for (long long j = lane; j < len; j += 32) mx = max(mx, abs_bits(r[j]));
+        for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+        if (lane == 0) out[row] = mx;
+    }
 }
 
 // Pass 3: shift_k = floor((eB_k - eA_k) / 2), so column k of A D and row k of
@@ -134,25 +136,27 @@ static __global__ void ozaki_b_rowmax_kernel(const double* __restrict__ B, long 
 static __global__ void ozaki_shift_kernel(const unsigned long long* __restrict__ a_colmax,
                                           const unsigned long long* __restrict__ b_rowmax,
                                           long long K, int* __restrict__ shift) {
-    const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (k >= K) return;
-    const double ma = __longlong_as_double(static_cast<long long>(a_colmax[k]));
-    const double mb = __longlong_as_double(static_cast<long long>(b_rowmax[k]));
-    int sh = 0;
-    if (ma > 0.0 && mb > 0.0 && isfinite(ma) && isfinite(mb)) {
-        int ea, eb;
-        frexp(ma, &ea);
-        frexp(mb, &eb);
-        const int d = eb - ea;
-        sh = d >= 0 ? d / 2 : -((-d + 1) / 2);
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < K;
+         k += (long long)gridDim.x * blockDim.x) {
+        const double ma = __longlong_as_double(static_cast<long long>(a_colmax[k]));
+        const double mb = __longlong_as_double(static_cast<long long>(b_rowmax[k]));
+        int sh = 0;
+        if (ma > 0.0 && mb > 0.0 && isfinite(ma) && isfinite(mb)) {
+            int ea, eb;
+            frexp(ma, &ea);
+            frexp(mb, &eb);
+            const int d = eb - ea;
+            sh = d >= 0 ? d / 2 : -((-d + 1) / 2);
+        }
+        shift[k] = sh;
     }
-    shift[k] = sh;
 }
 
 static __global__ void ozaki_col_scale_kernel(const unsigned long long* __restrict__ colmax_bits,
                                               long long N, double* __restrict__ scale) {
-    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (j < N) scale[j] = scale_from_max_bits(colmax_bits[j]);
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < N;
+         j += (long long)gridDim.x * blockDim.x)
+        scale[j] = scale_from_max_bits(colmax_bits[j]);
 }
 
 // Signed base-128 digits of t = x / scale, |t| < 1, by repeated exact

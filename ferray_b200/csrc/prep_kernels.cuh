@@ -175,16 +175,18 @@ static __global__ void pad_rows_kernel(const uint8_t* __restrict__ X, long long 
     }
 }
 
-// row_sum[i] = sum_k a[i, k] (u8), one warp per row, wrapping i32.
+// row_sum[i] = sum_k a[i, k] (u8), one warp per row, wrapping i32.  The
+// warps stride over the rows, so a capped grid still writes every row.
 static __global__ void row_sum_u8_kernel(const uint8_t* __restrict__ A, long long M, long long K,
                                   long long lda, int* __restrict__ out) {
-    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32;
     const int lane = threadIdx.x % 32;
-    if (warp >= M) return;
-    uint32_t s = 0;
-    for (long long k = lane; k < K; k += 32) s += A[warp * lda + k];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
-    if (lane == 0) out[warp] = static_cast<int>(s);
+    const long long warps = (long long)gridDim.x * blockDim.x / 32;
+    for (long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32; row < M; row += warps) {
+        uint32_t s = 0;
+        for (long long k = lane; k < K; k += 32) s += A[row * lda + k];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
+        if (lane == 0) out[row] = static_cast<int>(s);
+    }
 }
 
 // col_sum[j] += sum over rows [y * rows_per, (y + 1) * rows_per) of b[k, j]

@@ -95,8 +95,9 @@ extern "C" fg_status fg_quantized_matmul_noalloc(fg_ctx* ctx, size_t m, size_t n
         return set_error(FG_ERR_UNSUPPORTED,
                          "quantized_matmul_noalloc: k and n must be multiples of 16 and a, b 16-byte "
                          "aligned (padding the operands would need scratch); use fg_quantized_matmul");
+    if (ctx->device < 0 || ctx->device >= kMaxDevices)
+        return set_error(FG_ERR_UNSUPPORTED, "quantized_matmul_noalloc: device index above 63");
     FG_CUDA(cudaSetDevice(ctx->device));
-    if (ctx->device < 0 || ctx->device >= kMaxDevices) return set_error(FG_ERR_UNSUPPORTED, "device index");
     cudaStream_t st = stream_of(ctx, stream);
     if (k == 0) {  // gemm/mod.rs:509-519: zeros, or C untouched when accumulating
         if (!accumulate) FG_CUDA(cudaMemsetAsync(c, 0, m * n * sizeof(float), st));

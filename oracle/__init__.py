@@ -44,10 +44,12 @@ def _declare(L):
                               C.c_double, C.c_double, _p]
     L.fr_gemm_c32.argtypes = [_sz, _sz, _sz, C.c_float, C.c_float, _p, _p,
                               C.c_float, C.c_float, _p]
-    for name in ("fr_gemm_i8_signed", "fr_gemm_i16", "fr_gemm_i8_vnni", "fr_gemm_i8_avx2"):
+    for name in ("fr_gemm_i8_signed", "fr_gemm_i8_signed_rows", "fr_gemm_i16", "fr_gemm_i8_vnni",
+                 "fr_gemm_i8_avx2"):
         getattr(L, name).argtypes = [_sz, _sz, _sz, _p, _p, _p, C.c_int]
     L.fr_quantized_matmul.argtypes = [_sz, _sz, _sz, _p, C.c_uint8, C.c_float, _p,
                                       C.c_int8, C.c_float, _p, C.c_int, C.c_int]
+    L.fr_pick_grid.argtypes = [_sz, _sz, _sz, _sz, C.c_int, _p, _p]
     L.fr_matmul_raw_f64.argtypes = [_p, _p, _sz, _sz, _sz, _p]
     L.fr_matmul_raw_f32.argtypes = [_p, _p, _sz, _sz, _sz, _p]
     for name in ("dd_gemm_f64_sampled", "dd_gemm_f32_sampled"):
@@ -259,6 +261,21 @@ def _int_gemm(name, a, b, c, accumulate):
 def gemm_i8_signed(a, b, c=None, accumulate=False):
     return _int_gemm("fr_gemm_i8_signed", a.astype(np.int8, copy=False),
                      b.astype(np.int8, copy=False), c, accumulate)
+
+
+def gemm_i8_signed_rows(a, b, c=None, accumulate=False):
+    """The same product as gemm_i8_signed by a plain row loop (exact sums,
+    no packing): the cross-check for the packed restatement."""
+    return _int_gemm("fr_gemm_i8_signed_rows", a.astype(np.int8, copy=False),
+                     b.astype(np.int8, copy=False), c, accumulate)
+
+
+def pick_grid(m, n, k, workers, f32=False):
+    """(parallel, mw, nw): the thread grid ferray's GEMM driver picks
+    (gemm/outer.rs:343-383, 692-726)."""
+    mw, nw = C.c_size_t(), C.c_size_t()
+    par = lib().fr_pick_grid(m, n, k, workers, int(bool(f32)), C.byref(mw), C.byref(nw))
+    return bool(par), mw.value, nw.value
 
 
 def gemm_i16(a, b, c=None, accumulate=False):

@@ -230,3 +230,55 @@ def test_trsm_restatement_split_rule(oracle):
         b = np.random.default_rng(m).standard_normal((m, 5))
         x = oracle.trsm_left(a, b)
         np.testing.assert_allclose(x, np.linalg.solve(a, b), rtol=1e-12, atol=1e-12)
+
+
+def _pick_grid_py(m, n, k, workers, budget, mr=4):
+    """outer.rs:343-383 (f64 budget 128 Ki, f32 256 Ki elements)."""
+    import math
+    if workers <= 1 or m == 0 or n == 0:
+        return max(workers, 1), 1
+    kc_eff = min(256, max(k, 1))
+    chunks = m // mr
+    if chunks >= workers and kc_eff * n <= budget:
+        return workers, 1
+    best, score_best = (1, workers), math.inf
+    for mw in range(1, min(max(chunks, 1), workers) + 1):
+        if workers % mw:
+            continue
+        nw = workers // mw
+        sc = abs(math.log(m / mw) - math.log(n / nw))
+        if sc < score_best or (sc == score_best and mw > best[0]):
+            best, score_best = (mw, nw), sc
+    return best
+
+
+@pytest.mark.parametrize("m,n,k", [(8192, 8192, 8192), (160, 8192, 8192), (1024, 1024, 1024),
+                                   (4096, 64, 300), (9, 5000, 40), (300, 300, 300), (32, 32, 32)])
+def test_pick_grid_matches_reference_rule(oracle, m, n, k):
+    for workers in (1, 3, 8):
+        for f32 in (False, True):
+            par, mw, nw = oracle.pick_grid(m, n, k, workers, f32)
+            assert (mw, nw) == _pick_grid_py(m, n, k, workers, 256 * 1024 if f32 else 128 * 1024)
+            assert par == (max(m, n, k) >= 256 and m >= 8)
+
+
+def test_thread_grid_never_changes_a_bit(oracle):
+    # 1-D slabs, 2-D cells and the sequential path agree bit for bit
+    # (every element's chain is independent of the grid and of packing).
+    rng = np.random.default_rng(12)
+    for m, n, k in [(8, 4096, 300), (520, 600, 257), (64, 33, 700)]:
+        a32, b32 = rng.standard_normal((m, k), dtype=np.float32), rng.standard_normal((k, n), dtype=np.float32)
+        a64, b64 = a32.astype(np.float64), b32.astype(np.float64)
+        ac = (a64 + 1j * a64[::-1]).astype(np.complex64)
+        bc = (b64 - 1j * b64[::-1]).astype(np.complex64)
+        a8, b8 = rng.integers(-128, 128, (m, k), dtype=np.int8), rng.integers(-128, 128, (k, n), dtype=np.int8)
+        outs = []
+        for th in (1, 3, 8):
+            oracle.set_threads(th)
+            outs.append((oracle.gemm_f32(a32, b32), oracle.gemm_f64(a64, b64), oracle.gemm_complex(ac, bc),
+                         oracle.gemm_i8_signed(a8, b8)))
+        oracle.set_threads(0)
+        for o in outs[1:]:
+            for x, y in zip(o, outs[0]):
+                assert np.array_equal(x.view(np.uint8), y.view(np.uint8))
+        np.testing.assert_array_equal(outs[0][3], oracle.gemm_i8_signed_rows(a8, b8))
