@@ -53,7 +53,7 @@ def parse():
                     help="skip the DGEMM / grouped / serving side measurements")
     ap.add_argument("--serving", action="store_true", help="only the served-stream sweep")
     ap.add_argument("--rates", default="1000,3000,10000,30000,100000")
-    ap.add_argument("--requests", type=int, default=2000)
+    ap.add_argument("--requests", type=int, default=10000)
     ap.add_argument("--peaks", action="store_true",
                     help="measure library reference rates (cuBLAS via torch) for INT8, FP64, FP32")
     ap.add_argument("--side", default="",
@@ -248,59 +248,46 @@ def _time_calls(torch, stream, fn, steps, warmup):
 
 
 def side_measurements(fg, L, lib, ctx, stream, n, only=""):
-    """The other configs, one short measurement each (device-timed):
-    DGEMM plain vs Ozaki split at N=n with their DD-oracle errors; square i8
-    at N=n (bit-exact on a sampled block); i16 and quantized u8 x i8; skinny
-    shapes against the HBM roof; the 4096-problem ragged batch as one
-    grouped graph replay vs a loop of per-problem launches; the lower
-    triangular solve at m = n (plain and split trailing updates); the served
-    stream at 10k req/s, server vs plain one-call-at-a-time.  `only="ozaki"` runs
-    the per-spread / per-slice-count DGEMM and ZGEMM sweep (N = 2048..8192)."""
+    """The other configs, one short measurement each (device-timed), each
+    with its error against the double-double oracle (or a bit-exact check)
+    and the CPU rate of ferray's restated GEMM on the same shape: library
+    reference rates (cuBLAS / cuBLASLt via torch) for INT8, FP64 and FP32;
+    DGEMM 1024^3; the SGEMM sweep N = 256 .. 4096 (plain, 3- and 6-product
+    split); CGEMM 4096; DGEMM / ZGEMM N = 2048 .. 8192 at exponent spreads
+    0, 4, 8 (plain vs Ozaki 8 / 9 slices); square i8 at 1024, 4096, 8192;
+    the 4096-problem ragged batch (one grouped graph replay vs a loop of
+    per-problem launches, and ferray's per-problem CPU loop); i16 and
+    quantized u8 x i8; skinny shapes against the HBM roof; the lower
+    triangular solve at m = n; the served stream.  `only` runs one of them
+    (`ozaki_all` adds 6 and 7 slices to the Ozaki sweep)."""
     import torch
     import oracle
     import bench_serving
     sh = C.c_void_p(stream.cuda_stream)
     res = {}
     rng = np.random.default_rng(SEED)
+    import bench_configs as bc
+    R = bc.Runner(fg, L, lib, ctx, stream)
+    if not only or only == "peaks":
+        res["peaks"] = reference_peaks()
+    int8_peak = res.get("peaks", {}).get("reference_peaks", {}).get("int8_tops")
     if not only or only == "dgemm":
-        # --- DGEMM plain vs split (spread 0 operands, N(0,1))
-        a = rng.standard_normal((n, n))
-        b = rng.standard_normal((n, n))
-        da, db = fg.DeviceArray.from_numpy(a, ctx), fg.DeviceArray.from_numpy(b, ctx)
-        dc = fg.DeviceArray((n, n), np.float64, ctx)
-        rows, cols = oracle.sample_indices(n, n, 48, 48, seed=11)
-        ref = oracle.dd_sampled(a, b, rows, cols)
-        na, nb = oracle.fro(a), oracle.fro(b)
-        d = {}
-        for name, mode in (("plain", L.FG_MODE_PLAIN), ("split_ozaki9", L.FG_MODE_SPLIT)):
-            ms = _time_calls(torch, stream, lambda: lib.fg_gemm_f64(ctx.handle, mode, 0, n, n, n, 1.0, da.ptr,
-                                                                      db.ptr, 0.0, dc.ptr, sh), 3, 1)
-            err = oracle.normwise_error(dc.to_numpy()[np.ix_(rows, cols)], ref, n, n, na, nb)
-            d[name] = {"tflops": round(2.0 * n ** 3 / ms / 1e9, 2), "ms": round(ms, 3), "normwise_err": err}
-        d["split_over_plain"] = round(d["split_ozaki9"]["tflops"] / d["plain"]["tflops"], 2)
-        res["dgemm_f64_%d" % n] = d
-        del da, db, dc
+        res["dgemm_f64_1024"] = bc.dgemm_1024(R)
+        torch.cuda.empty_cache()
+    if not only or only == "sweep":
+        res["sgemm_f32_sweep"] = bc.sgemm_sweep(R)
+        torch.cuda.empty_cache()
+    if not only or only == "cgemm":
+        res["cgemm_c32_4096"] = bc.cgemm_4096(R)
     if not only or only == "i8":
-        # --- square i8
-        a8 = rng.integers(-128, 128, (n, n), dtype=np.int8)
-        b8 = rng.integers(-128, 128, (n, n), dtype=np.int8)
-        da, db = fg.DeviceArray.from_numpy(a8, ctx), fg.DeviceArray.from_numpy(b8, ctx)
-        dc = fg.DeviceArray((n, n), np.int32, ctx)
-        ms = _time_calls(torch, stream, lambda: lib.fg_gemm_i8_signed(ctx.handle, n, n, n, da.ptr, db.ptr,
-                                                                        dc.ptr, 0, sh), 10, 3)
-        r8, c8 = oracle.sample_indices(n, n, 32, 32, seed=5)
-        got = dc.to_numpy()[np.ix_(r8, c8)]
-        want = (a8[r8].astype(np.int64) @ b8[:, c8].astype(np.int64)).astype(np.int32)
-        tops = 2.0 * n ** 3 / ms / 1e9
-        v, sp = fg.tune_lookup("i8", n, n, n)
-        res["i8_square_%d" % n] = {"tops": round(tops, 1), "ms": round(ms, 4),
-                                   "frac_of_nominal_dense_int8_4500": round(tops / 4500.0, 3),
-                                   "variant": v, "splits": sp,
-                                   "bit_exact_sampled": bool(np.array_equal(got, want))}
-        del da, db, dc
+        res["i8_square"] = bc.i8_square(R, int8_peak=int8_peak)
+    if not only or only == "ozaki":
+        res["ozaki_f64_c128"] = bc.ozaki_sweep(R)
+    if only == "ozaki_all":
+        res["ozaki_sweep_all_slices"] = bc.ozaki_sweep(R, slices=(6, 7, 8, 9), cpu=False)
     if not only or only == "ragged":
         # --- ragged grouped batch, 4096 problems, dims log-uniform in [8, 512]
-        dims = np.rint(np.exp(rng.uniform(np.log(8), np.log(512), (4096, 3)))).astype(int)
+        dims = ragged_dims()
         gflop = float(sum(2.0 * m * nn * k for m, nn, k in dims)) / 1e9
         g = {}
         for name, dt, mode in (("i8", L.FG_I8, 0), ("f32_split", L.FG_F32, 1), ("f32_plain", L.FG_F32, 0)):
@@ -328,7 +315,7 @@ def side_measurements(fg, L, lib, ctx, stream, n, only=""):
             g[name] = {"grouped_ms": round(ms_g, 4), "grouped_tflops": round(gflop / ms_g, 2),
                        "loop_ms": round(ms_l, 3), "speedup_vs_loop": round(ms_l / ms_g, 1)}
             del bufs
-        res["ragged_4096"] = {"gflop": round(gflop, 2), **g}
+        res["ragged_4096"] = {"gflop": round(gflop, 2), **g, "cpu": bc.ragged_cpu(dims)}
         torch.cuda.empty_cache()
     if not only or only == "int":
         # --- i16 x i16 -> i32 (4 byte-slice products) and the quantized
@@ -381,54 +368,6 @@ def side_measurements(fg, L, lib, ctx, stream, n, only=""):
                         "normwise_err_vs_widened": err}
             del da, db, dc
         res["half_f32_%d" % n] = hv
-    if only == "ozaki":
-        # --- DGEMM / ZGEMM plain vs Ozaki INT8 per exponent spread and slice
-        # count: A = diag(10^(s u)) G diag(10^(s v)), B built the same way
-        # independently, G ~ N(0, 1), u, v ~ U[-1, 1]; error vs the DD oracle
-        # on a sampled 64 x 64 block (normwise estimate).
-        oz = {}
-        for nn in (2048, 4096, 8192):
-            if nn > n:
-                continue
-            for cplx in (False, True):
-                for spread in (0, 4, 8):
-                    r2 = np.random.default_rng(SEED + spread + nn)
-
-                    def spread_mat():
-                        g = r2.standard_normal((nn, nn))
-                        if cplx:
-                            g = g + 1j * r2.standard_normal((nn, nn))
-                        du = 10.0 ** (spread * r2.uniform(-1, 1, nn))
-                        dv = 10.0 ** (spread * r2.uniform(-1, 1, nn))
-                        return (du[:, None] * g) * dv[None, :]
-                    a, b = spread_mat(), spread_mat()
-                    dt = np.complex128 if cplx else np.float64
-                    da, db = fg.DeviceArray.from_numpy(a, ctx), fg.DeviceArray.from_numpy(b, ctx)
-                    dc = fg.DeviceArray((nn, nn), dt, ctx)
-                    rows, cols = oracle.sample_indices(nn, nn, 64, 64, seed=13)
-                    ref = oracle.dd_sampled(a, b, rows, cols)
-                    na, nb = oracle.fro(a), oracle.fro(b)
-                    flops = (8.0 if cplx else 2.0) * nn ** 3
-                    entry = {}
-                    for name, mode, sl in (("plain", L.FG_MODE_PLAIN, 0), ("ozaki6", L.FG_MODE_SPLIT, 6),
-                                           ("ozaki7", L.FG_MODE_SPLIT, 7), ("ozaki8", L.FG_MODE_SPLIT, 8),
-                                           ("ozaki9", L.FG_MODE_SPLIT, 9)):
-                        if cplx:
-                            call = lambda: lib.fg_gemm_c64(ctx.handle, mode, sl, nn, nn, nn, 1.0, 0.0, da.ptr,
-                                                           db.ptr, 0.0, 0.0, dc.ptr, sh)
-                        else:
-                            call = lambda: lib.fg_gemm_f64(ctx.handle, mode, sl, nn, nn, nn, 1.0, da.ptr,
-                                                           db.ptr, 0.0, dc.ptr, sh)
-                        ms = _time_calls(torch, stream, call, 2, 1)
-                        err = oracle.normwise_error(dc.to_numpy()[np.ix_(rows, cols)], ref, nn, nn, na, nb)
-                        entry[name] = {"tflops": round(flops / ms / 1e9, 2), "ms": round(ms, 3), "err": err}
-                    for name in ("ozaki6", "ozaki7", "ozaki8", "ozaki9"):
-                        entry[name]["speed_over_plain"] = round(entry[name]["tflops"] / entry["plain"]["tflops"], 2)
-                        entry[name]["err_over_plain"] = round(entry[name]["err"] / entry["plain"]["err"], 3)
-                    oz["%s_%d_spread%d" % ("zgemm" if cplx else "dgemm", nn, spread)] = entry
-                    del da, db, dc, a, b
-                    torch.cuda.empty_cache()
-        res["ozaki_sweep"] = oz
     if not only or only == "skinny":
         # --- skinny shapes on the HBM roof: algorithmic bytes / device time
         _, hbm, _ = peaks()
@@ -494,8 +433,66 @@ def side_measurements(fg, L, lib, ctx, stream, n, only=""):
         torch.cuda.empty_cache()
     if not only or only == "serving":
         # --- served stream, one rate
-        res["serving_10k_req_s"] = bench_serving.sweep(fg, L, lib, ctx, [10000.0], 1500)[0]
+        sw = bench_serving.sweep(fg, L, lib, ctx, [1000.0, 10000.0, 100000.0], 10000)
+        res["serving"] = {"%dk_req_s" % int(x["server"]["rate_req_s"] / 1000): x for x in sw}
     return res
+
+
+def ragged_dims(seed=SEED):
+    """The ragged batch: 4096 problems, M, N, K = round(exp(U[ln 8, ln 512]))."""
+    rng = np.random.default_rng(seed)
+    return np.rint(np.exp(rng.uniform(np.log(8), np.log(512), (4096, 3)))).astype(int)
+
+
+def ragged_sharded(fg, L, lib, ctx, stream, dist, torch, rank, world):
+    """The 4096-problem ragged batch split across the ranks with no exchange
+    (fg_shard_plan, heaviest first to the least-loaded rank): each rank
+    replays one grouped plan over its shard; time = max over ranks of the
+    CUDA-event time of one replay (strong scaling: the batch is fixed)."""
+    dims = ragged_dims()
+    mine = fg.shard_problems(dims, world, rank)
+    gflop_all = float(sum(2.0 * m * n * k for m, n, k in dims)) / 1e9
+    sh = C.c_void_p(stream.cuda_stream)
+    out = {"problems": len(dims), "world": world, "gflop": round(gflop_all, 2), "policy": "LPT by 2mnk"}
+    for name, dt, mode in (("i8", L.FG_I8, 0), ("f32_split", L.FG_F32, 1)):
+        bufs, tab = [], (L.fg_problem * max(len(mine), 1))()
+        for j, i in enumerate(mine):
+            m, nn, k = (int(x) for x in dims[i])
+            if dt == L.FG_I8:
+                ta = torch.randint(-100, 100, (m * k,), dtype=torch.int8, device="cuda")
+                tb = torch.randint(-100, 100, (k * nn,), dtype=torch.int8, device="cuda")
+            else:
+                ta, tb = torch.randn(m * k, device="cuda"), torch.randn(k * nn, device="cuda")
+            tc = torch.zeros(m * nn * 4, dtype=torch.int8, device="cuda")
+            bufs.append((ta, tb, tc))
+            tab[j] = L.fg_problem(m, nn, k, ta.data_ptr(), tb.data_ptr(), tc.data_ptr(), k, nn, nn)
+        h = C.c_void_p()
+        if mine:
+            assert lib.fg_grouped_plan_create(ctx.handle, dt, mode, tab, len(mine), sh, C.byref(h)) == 0, \
+                lib.fg_last_error()
+        run = (lambda: lib.fg_grouped_plan_run(h, sh)) if mine else (lambda: None)
+        for _ in range(3):
+            run()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 10
+        e0.record(stream)
+        for _ in range(reps):
+            run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        if dist:
+            ms = max_over_ranks(dist, torch, ms)
+        if mine:
+            lib.fg_grouped_plan_destroy(h)
+        out[name] = {"problems_rank0": len(mine), "ms_max_over_ranks": round(ms, 4),
+                     "tflops_all_ranks": round(gflop_all / ms, 2)}
+        del bufs
+    torch.cuda.empty_cache()
+    return out
 
 
 def cpu_baseline(n):
@@ -613,7 +610,7 @@ def main():
     sampler.start()
     ms_split, launches, prof_split = timed(L.FG_MODE_SPLIT, args.steps, args.warmup)
     clocks = sampler.stop()
-    ms_plain, _, _ = timed(L.FG_MODE_PLAIN, max(2, args.steps // 3), 2)
+    ms_plain, _, prof_plain = timed(L.FG_MODE_PLAIN, max(2, args.steps // 3), 2)
     ctx.sync()
 
     # accuracy of both forms vs the double-double oracle (sampled rows x cols)
@@ -679,6 +676,10 @@ def main():
                "h2d_bytes_per_step": int(a_h.nbytes + b_h.nbytes),
                "d2h_bytes_per_step": int(c_h.nbytes), "ms_per_step": round(dt * 1e3, 3)}
 
+    sharded = None
+    if not args.no_extra:
+        sharded = ragged_sharded(fg, L, lib, ctx, stream, dist, torch, rank, world)
+
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -724,7 +725,8 @@ def main():
         "split": {"tflops": round(tf_split, 3), "ms": round(ms_split, 4),
                   "normwise_err": err_split},
         "plain": {"tflops": round(tf_plain, 3), "ms": round(ms_plain, 4),
-                  "normwise_err": err_plain, "kernel": "simt_sgemm"},
+                  "normwise_err": err_plain,
+                  "kernel": max(prof_plain, key=lambda q: prof_plain[q][1]) if prof_plain else None},
         "split_over_plain": round(tf_split / tf_plain, 3),
         "err_split_over_plain": round(err_split / err_plain, 3) if err_plain else None,
         "split6": {"tflops": round(flops / (ms_split6 * 1e-3) / 1e12, 3), "ms": round(ms_split6, 4),
@@ -737,6 +739,8 @@ def main():
         "clocks": clocks,
         "e2e": e2e,
     }
+    if sharded:
+        out["ragged_4096_sharded"] = sharded
     if not args.no_cpu and world == 1:
         out["cpu_baseline"] = cpu_baseline(n)
     if not args.no_extra and world == 1:

@@ -687,26 +687,35 @@ class tune_forced:
         return False
 
 
-def shard_problems(dims, world, rank):
-    """Indices of the problems of a ragged batch (rows of (m, n, k)) that rank
-    `rank` of `world` runs: longest-processing-time-first by 2mnk, each
-    problem to the least-loaded rank so far (lowest rank on ties).  Every
-    rank computes the same assignment from the same table, so sharding a
-    batch across GPUs needs no communication; the shards are disjoint, cover
-    every problem, and differ in load by at most one problem's work."""
+def _shard(dims, weights, world, rank, policy):
     if world < 1 or not 0 <= rank < world:
         raise InvalidValue(f"rank {rank} outside a world of {world}")
-    d = np.asarray(dims, dtype=np.int64).reshape(-1, 3)
-    work = 2 * d[:, 0] * d[:, 1] * d[:, 2]
-    order = np.argsort(-work, kind="stable")
-    load = [0] * world
-    mine = []
-    for i in order:
-        r = min(range(world), key=lambda q: (load[q], q))
-        load[r] += int(work[i])
-        if r == rank:
-            mine.append(int(i))
-    return sorted(mine)
+    d = np.ascontiguousarray(np.asarray(dims, dtype=np.int64).reshape(-1, 3))
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    out = np.empty(len(d), np.int64)
+    cnt = C.c_size_t()
+    check(L.load().fg_shard_plan(d.ctypes.data, None if w is None else w.ctypes.data, len(d), world, rank,
+                                 policy, out.ctypes.data, C.byref(cnt)), "shard_plan")
+    return [int(x) for x in out[:cnt.value]]
+
+
+def shard_problems(dims, world, rank):
+    """Indices of the problems of a ragged batch (rows of (m, n, k)) that rank
+    `rank` of `world` runs (fg_shard_plan, FG_SHARD_LPT): heaviest first by
+    2mnk, each problem to the least-loaded rank so far (lowest rank on
+    ties).  Every rank computes the same assignment from the same table, so
+    sharding a batch across GPUs needs no communication; the shards are
+    disjoint, cover every problem, and differ in load by at most one
+    problem's work."""
+    return _shard(dims, None, world, rank, L.FG_SHARD_LPT)
+
+
+def shard_requests(dims, world, rank, weights=None):
+    """Indices of the requests of a served stream (rows of (m, n, k) in
+    arrival order) that rank `rank` of `world` serves (FG_SHARD_ONLINE): each
+    request to the rank with the least cost so far -- `weights` (estimated
+    seconds, say) or 2mnk -- so a rank can route a request as it arrives."""
+    return _shard(dims, weights, world, rank, L.FG_SHARD_ONLINE)
 
 
 def gemm_grouped(problems, dtype=np.float32, mode=PLAIN):
@@ -772,6 +781,17 @@ class Server:
 
     def wait(self, ticket, timeout_ms=-1):
         check(self._lib.fg_server_wait(self.handle, ticket, int(timeout_ms)), "wait")
+
+    def wait_times(self, ticket, timeout_ms=-1):
+        """wait(), returning (submitted, completed) in seconds of clock()."""
+        t0, t1 = C.c_double(), C.c_double()
+        check(self._lib.fg_server_wait_times(self.handle, ticket, int(timeout_ms), C.byref(t0), C.byref(t1)),
+              "wait")
+        return t0.value, t1.value
+
+    def clock(self):
+        """The server's monotonic clock (seconds)."""
+        return self._lib.fg_server_clock()
 
     def stats(self):
         s = L.fg_server_stats()

@@ -25,6 +25,7 @@ FG_ERR_BROADCAST = 9
 FG_F64, FG_F32, FG_C64, FG_C32, FG_I8, FG_U8I8, FG_I16, FG_BF16, FG_F16 = range(9)
 # fg_mode
 FG_MODE_PLAIN, FG_MODE_SPLIT = 0, 1
+FG_SHARD_LPT, FG_SHARD_ONLINE = 0, 1
 
 
 class fg_problem(C.Structure):
@@ -116,10 +117,14 @@ SIGNATURES = {
     "fg_grouped_plan_create": (_i, [_p, _i, _i, C.POINTER(fg_problem), _sz, _p,
                                     C.POINTER(_p)]),
     "fg_grouped_plan_run": (_i, [_p, _p]),
+    "fg_shard_plan": (_i, [_p, _p, _sz, _i, _i, _i, _p, C.POINTER(_sz)]),
+    "fg_gemm_grouped_shard": (_i, [_p, _i, _i, C.POINTER(fg_problem), _sz, _i, _i, _p]),
     "fg_grouped_plan_destroy": (_i, [_p]),
     "fg_server_start": (_i, [_p, _sz, _i, _i, C.POINTER(_p)]),
     "fg_server_submit": (_i, [_p, C.POINTER(fg_request), C.POINTER(_u64)]),
     "fg_server_wait": (_i, [_p, _u64, _i64]),
+    "fg_server_wait_times": (_i, [_p, _u64, _i64, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "fg_server_clock": (C.c_double, []),
     "fg_server_stats_get": (_i, [_p, C.POINTER(fg_server_stats)]),
     "fg_server_stop": (_i, [_p]),
 }

@@ -235,7 +235,13 @@ fg_status launch_simt(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
     const BatchMap bm = batch_map(g);
     if (g.batch > 65535) return set_error(FG_ERR_UNSUPPORTED, "batch above 65535");
     static const char* names[] = {"simt_dgemm", "simt_sgemm", "simt_zgemm", "simt_cgemm"};
-    ProfScope prof(g.dtype <= FG_C32 ? names[g.dtype] : "simt", st);
+    const char* fam = g.dtype <= FG_C32 ? names[g.dtype] : "simt";
+    if (g.dtype == FG_F64 || g.dtype == FG_F32) {  // profile under the tuned kernel's name
+        const TuneChoice c = tune_lookup(g.dtype == FG_F64 ? TUNE_F64 : TUNE_F32, g.M, g.N, g.K);
+        if (c.variant == 4) fam = g.dtype == FG_F64 ? "dmma_dgemm" : "ffma_sgemm";
+        if (c.variant == 5) fam = g.dtype == FG_F64 ? "dmma_dgemm_skinny" : "ffma_sgemm_skinny";
+    }
+    ProfScope prof(fam, st);
     switch (g.dtype) {
         case FG_F64: {
             const TuneChoice c = tune_lookup(TUNE_F64, g.M, g.N, g.K);

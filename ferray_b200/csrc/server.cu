@@ -331,6 +331,13 @@ fg_status fg_server_submit(fg_server* s, const fg_request* req, uint64_t* ticket
 }
 
 fg_status fg_server_wait(fg_server* s, uint64_t ticket, int64_t timeout_ms) {
+    return fg_server_wait_times(s, ticket, timeout_ms, nullptr, nullptr);
+}
+
+double fg_server_clock(void) { return now_s(); }
+
+fg_status fg_server_wait_times(fg_server* s, uint64_t ticket, int64_t timeout_ms, double* submit_s,
+                               double* done_s) {
     if (!s) return set_error(FG_ERR_INVALID, "null server");
     std::unique_lock<std::mutex> lk(s->mu);
     auto it = s->reqs.find(ticket);
@@ -342,6 +349,8 @@ fg_status fg_server_wait(fg_server* s, uint64_t ticket, int64_t timeout_ms) {
         return set_error(FG_ERR_TIMEOUT, "ticket not complete");
     }
     const fg_status st = s->reqs[ticket].status;
+    if (submit_s) *submit_s = s->reqs[ticket].t_submit;
+    if (done_s) *done_s = s->reqs[ticket].t_done;
     s->reqs.erase(ticket);
     if (st != FG_OK) return set_error(st, "request failed");
     return FG_OK;

@@ -367,6 +367,26 @@ fg_status fg_grouped_plan_create(fg_ctx *ctx, fg_dtype dtype, fg_mode mode,
 fg_status fg_grouped_plan_run(fg_grouped_plan *plan, fg_stream stream);
 fg_status fg_grouped_plan_destroy(fg_grouped_plan *plan);
 
+/* ------------------------------------------------------------ sharding */
+/* Multi-GPU runs are one process per GPU; independent problems (a ragged
+ * batch) and requests (a served stream) are split across the processes
+ * with no exchange: every rank computes the same assignment from the same
+ * list.  ferray's counterpart is the rayon split of a stacked matmul's batch
+ * inside one process (products/mod.rs:625-638). */
+typedef enum fg_shard_policy {
+    FG_SHARD_LPT = 0,    /* heaviest unit first, each to the least-loaded rank */
+    FG_SHARD_ONLINE = 1  /* arrival order, each to the least-loaded rank       */
+} fg_shard_policy;
+/* Indices (ascending) of the units rank `rank` of `world` runs.  `dims` is
+ * count x 3 (m, n, k) int64; a unit costs weight[i] when `weight` is not
+ * NULL, else 2mnk.  Ties go to the lower rank.  `out` holds up to `count`. */
+fg_status fg_shard_plan(const int64_t *dims, const double *weight, size_t count, int world,
+                        int rank, int policy, int64_t *out, size_t *out_count);
+/* fg_gemm_grouped over this rank's FG_SHARD_LPT shard of `table`. */
+fg_status fg_gemm_grouped_shard(fg_ctx *ctx, fg_dtype dtype, fg_mode mode,
+                                const fg_problem *table, size_t count, int world, int rank,
+                                fg_stream stream);
+
 /* ------------------------------------------------------------ serving */
 /* Continuous-batching request loop.  Host threads submit matmul requests
  * (mixed shapes and dtypes) whose operands are already on the device; the
@@ -401,6 +421,14 @@ fg_status fg_server_submit(fg_server *srv, const fg_request *req, uint64_t *tick
 /* Waits up to timeout_ms (<0: forever) for the ticket; FG_ERR_TIMEOUT if
  * it has not completed. */
 fg_status fg_server_wait(fg_server *srv, uint64_t ticket, int64_t timeout_ms);
+/* fg_server_wait that also returns when the ticket was submitted and when
+ * its work was seen complete on the GPU, in seconds of fg_server_clock, so
+ * a caller that waits on tickets in any order still gets each request's
+ * own completion time. */
+fg_status fg_server_wait_times(fg_server *srv, uint64_t ticket, int64_t timeout_ms,
+                               double *submit_s, double *done_s);
+/* The server's monotonic clock in seconds. */
+double fg_server_clock(void);
 fg_status fg_server_stats_get(fg_server *srv, fg_server_stats *out);
 fg_status fg_server_stop(fg_server *srv);
 

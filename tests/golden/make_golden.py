@@ -1,7 +1,7 @@
 """Generate the golden fixtures under tests/golden/ from the ferray sources.
 
-Run in a checkout that has the ferray workspace at FERRAY_ROOT (default
-/root/reference); the JSON files it writes are committed, so nothing at test
+Run with the environment variable FERRAY_ROOT set to a checkout of the
+ferray workspace; the JSON files it writes are committed, so nothing at test
 time reads the ferray tree.
 
 Fixtures:
@@ -29,7 +29,7 @@ import re
 
 import numpy as np
 
-FERRAY_ROOT = os.environ.get("FERRAY_ROOT", "/root/reference")
+FERRAY_ROOT = os.environ.get("FERRAY_ROOT", "")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -191,4 +191,6 @@ def main():
 
 
 if __name__ == "__main__":
+    if not FERRAY_ROOT or not os.path.isdir(FERRAY_ROOT):
+        raise SystemExit("set FERRAY_ROOT to a checkout of the ferray workspace")
     main()
