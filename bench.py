@@ -94,6 +94,20 @@ def reference_peaks(n=8192):
     return {"reference_peaks": out, "n": n, "how": "best of 5 after 3 warm-ups, CUDA events"}
 
 
+def probe_peaks(lib, ctx):
+    """Measured dense pipe rates (fg_probe_peak: each pipe busy on on-chip
+    data, ~5 ms per probe): INT8 and BF16 tcgen05.mma, FP64 DMMA, FFMA;
+    TOPS / TFLOP/s."""
+    from ferray_b200 import _lib as L
+    out = {}
+    for name, which in (("int8_tops", L.FG_PROBE_INT8), ("bf16_tflops", L.FG_PROBE_BF16),
+                        ("fp64_tflops", L.FG_PROBE_FP64), ("ffma_tflops", L.FG_PROBE_FFMA)):
+        v = C.c_double()
+        st = lib.fg_probe_peak(ctx.handle, which, C.byref(v))
+        out[name] = round(v.value / 1e12, 1) if st == 0 else None
+    return out
+
+
 def max_over_ranks(dist, torch, x, device="cuda"):
     """The largest of every rank's x (the job's time is its slowest rank's);
     every rank gets it.  `device` is where the reduction tensor lives: cuda
@@ -270,7 +284,10 @@ def side_measurements(fg, L, lib, ctx, stream, n, only=""):
     R = bc.Runner(fg, L, lib, ctx, stream)
     if not only or only == "peaks":
         res["peaks"] = reference_peaks()
-    int8_peak = res.get("peaks", {}).get("reference_peaks", {}).get("int8_tops")
+        res["peaks"]["probe_peaks"] = probe_peaks(lib, ctx)
+        res["peaks"]["probe_how"] = ("fg_probe_peak: one pipe busy on on-chip data on every SM, "
+                                     "~5 ms, CUDA events")
+    int8_peak = res.get("peaks", {}).get("probe_peaks", {}).get("int8_tops")
     if not only or only == "dgemm":
         res["dgemm_f64_1024"] = bc.dgemm_1024(R)
         torch.cuda.empty_cache()
@@ -645,6 +662,11 @@ def main():
     torch.cuda.synchronize()
     ms_split6 = e6a.elapsed_time(e6b) / 3
     err_split6 = oracle.normwise_error(dc.to_numpy()[np.ix_(rows, cols)], ref, n, n, na, nb)
+    # FP16 slices of power-of-two-scaled operands, 3 products (FG_MODE_SPLIT_F16)
+    ms_f16, _, prof_f16 = timed(L.FG_MODE_SPLIT_F16, max(3, args.steps // 2), 2)
+    step(L.FG_MODE_SPLIT_F16)
+    torch.cuda.synchronize()
+    err_f16 = oracle.normwise_error(dc.to_numpy()[np.ix_(rows, cols)], ref, n, n, na, nb)
 
     flops = 2.0 * n ** 3
     tf_split = flops / (ms_split * 1e-3) / 1e12
@@ -733,6 +755,12 @@ def main():
                    "normwise_err": err_split6,
                    "err_over_plain": round(err_split6 / err_plain, 3) if err_plain else None,
                    "note": "3 BF16 slices, 6 products: exact slicing of f32"},
+        "split_f16": {"tflops": round(flops / (ms_f16 * 1e-3) / 1e12, 3), "ms": round(ms_f16, 4),
+                      "normwise_err": err_f16,
+                      "err_over_plain": round(err_f16 / err_plain, 3) if err_plain else None,
+                      "speed_over_plain": round(ms_plain / ms_f16, 2),
+                      "kernels": {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in prof_f16.items()},
+                      "note": "2 FP16 slices of power-of-two-scaled operands, 3 products"},
         "roofline": roofline,
         "kernels": {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in prof_split.items()},
         "gpu_launches": int(launches),

@@ -202,11 +202,11 @@ def sgemm_sweep(R, sizes=(256, 1024, 2048, 4096)):
         na, nb = oracle.fro(a), oracle.fro(b)
         d = {}
         for name, mode, sl in (("plain", L.FG_MODE_PLAIN, 0), ("split3", L.FG_MODE_SPLIT, 2),
-                               ("split6", L.FG_MODE_SPLIT, 3)):
+                               ("split6", L.FG_MODE_SPLIT, 3), ("split_f16", L.FG_MODE_SPLIT_F16, 0)):
             ms = R.time(R.gemm(L.FG_F32, mode, sl, n, n, n, da.ptr, db.ptr, dc.ptr))
             err = _err(oracle, dc.to_numpy()[np.ix_(rows, cols)], ar, bc, n, n, na, nb)
             d[name] = _entry(2.0 * n ** 3, ms, err)
-        for name in ("split3", "split6"):
+        for name in ("split3", "split6", "split_f16"):
             d[name]["speed_over_plain"] = round(d["plain"]["ms"] / d[name]["ms"], 2)
             d[name]["err_over_plain"] = round(d[name]["normwise_err"] / d["plain"]["normwise_err"], 3)
         d["cpu"] = cpu_rate("f32", n, n, n)
@@ -232,11 +232,11 @@ def cgemm_4096(R, n=4096):
     na, nb = oracle.fro(a), oracle.fro(b)
     d = {}
     for name, mode, sl in (("plain", L.FG_MODE_PLAIN, 0), ("split3", L.FG_MODE_SPLIT, 2),
-                           ("split6", L.FG_MODE_SPLIT, 3)):
+                           ("split6", L.FG_MODE_SPLIT, 3), ("split_f16", L.FG_MODE_SPLIT_F16, 0)):
         ms = R.time(R.gemm(L.FG_C32, mode, sl, n, n, n, da.ptr, db.ptr, dc.ptr))
         err = _err(oracle, dc.to_numpy()[np.ix_(rows, cols)], ar, bc, n, n, na, nb)
         d[name] = _entry(8.0 * n ** 3, ms, err)
-    for name in ("split3", "split6"):
+    for name in ("split3", "split6", "split_f16"):
         d[name]["speed_over_plain"] = round(d["plain"]["ms"] / d[name]["ms"], 2)
         d[name]["err_over_plain"] = round(d[name]["normwise_err"] / d["plain"]["normwise_err"], 3)
     d["cpu"] = cpu_rate("c64", n, n, n)
@@ -328,7 +328,7 @@ def i8_square(R, sizes=(1024, 4096, 8192), int8_peak=None):
              "variant": v, "splits": sp, "bit_exact_sampled": bool(np.array_equal(got, want)),
              "cpu": cpu_rate("i8", n, n, n)}
         if int8_peak:
-            d["frac_of_measured_int8"] = round(tops / int8_peak, 3)
+            d["frac_of_probe_int8"] = round(tops / int8_peak, 3)
         out[str(n)] = d
         del a, b, c
     torch.cuda.empty_cache()

@@ -34,7 +34,7 @@ __all__ = [
     "trsm_left_lower_f64", "trsm_left_upper_f64", "trsm_left_lower_f32", "trsm_left_upper_f32", "npy_parse", "npy_load", "npz_names", "npz_read", "npz_load", "shard_problems",
 ]
 
-PLAIN, SPLIT = "plain", "split"
+PLAIN, SPLIT, SPLIT_F16 = "plain", "split", "split_f16"
 
 
 class FerrayError(Exception):
@@ -151,6 +151,8 @@ def _mode(mode):
         return L.FG_MODE_PLAIN
     if mode in (SPLIT, L.FG_MODE_SPLIT):
         return L.FG_MODE_SPLIT
+    if mode in (SPLIT_F16, L.FG_MODE_SPLIT_F16):
+        return L.FG_MODE_SPLIT_F16
     raise InvalidValue(f"unknown mode {mode!r}")
 
 
@@ -255,7 +257,9 @@ def gemm_f64(m, n, k, alpha, a, b, beta, c, mode=PLAIN, ozaki_slices=0):
 
 def gemm_f32(m, n, k, alpha, a, b, beta, c, mode=PLAIN, bf16_slices=0):
     """C = alpha*A@B + beta*C (gemm/mod.rs:940).  mode='split': 3xBF16
-    (bf16_slices=2, default) or the 6-product 3-slice form (bf16_slices=3)."""
+    (bf16_slices=2, default) or the 6-product 3-slice form (bf16_slices=3);
+    mode='split_f16': 3 products of two FP16 slices of power-of-two-scaled
+    operands."""
     _need(a, m * k, np.float32, "a"); _need(b, k * n, np.float32, "b")
     _need(c, m * n, np.float32, "c")
     return _run_gemm(L.FG_F32, mode, bf16_slices, m, n, k, [alpha], a, b, [beta], c, 0,

@@ -24,8 +24,9 @@ FG_ERR_BROADCAST = 9
 # fg_dtype
 FG_F64, FG_F32, FG_C64, FG_C32, FG_I8, FG_U8I8, FG_I16, FG_BF16, FG_F16 = range(9)
 # fg_mode
-FG_MODE_PLAIN, FG_MODE_SPLIT = 0, 1
+FG_MODE_PLAIN, FG_MODE_SPLIT, FG_MODE_SPLIT_F16 = 0, 1, 2
 FG_SHARD_LPT, FG_SHARD_ONLINE = 0, 1
+FG_PROBE_INT8, FG_PROBE_BF16, FG_PROBE_FP64, FG_PROBE_FFMA = 0, 1, 2, 3
 
 
 class fg_problem(C.Structure):
@@ -117,6 +118,7 @@ SIGNATURES = {
     "fg_grouped_plan_create": (_i, [_p, _i, _i, C.POINTER(fg_problem), _sz, _p,
                                     C.POINTER(_p)]),
     "fg_grouped_plan_run": (_i, [_p, _p]),
+    "fg_probe_peak": (_i, [_p, _i, C.POINTER(C.c_double)]),
     "fg_shard_plan": (_i, [_p, _p, _sz, _i, _i, _i, _p, C.POINTER(_sz)]),
     "fg_gemm_grouped_shard": (_i, [_p, _i, _i, C.POINTER(fg_problem), _sz, _i, _i, _p]),
     "fg_grouped_plan_destroy": (_i, [_p]),

@@ -145,10 +145,10 @@ fg_status run_gemm(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
     switch (g.dtype) {
         case FG_F64:
         case FG_C64:
-            return g.mode == FG_MODE_SPLIT ? launch_ozaki(ctx, g, st) : launch_simt(ctx, g, st);
+            return g.mode != FG_MODE_PLAIN ? launch_ozaki(ctx, g, st) : launch_simt(ctx, g, st);
         case FG_F32:
         case FG_C32:
-            return g.mode == FG_MODE_SPLIT ? launch_split_bf16(ctx, g, st) : launch_simt(ctx, g, st);
+            return g.mode != FG_MODE_PLAIN ? launch_split_bf16(ctx, g, st) : launch_simt(ctx, g, st);
         case FG_I8:
         case FG_U8I8:
         case FG_I16:
@@ -392,7 +392,7 @@ fg_status fg_gemm(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, int ozaki_slices, s
                   int accumulate, fg_stream stream) {
     if (!ctx) return set_error(FG_ERR_INVALID, "null context");
     if (!valid_dtype(dtype)) return set_error(FG_ERR_DTYPE, "unknown dtype");
-    if (mode != FG_MODE_PLAIN && mode != FG_MODE_SPLIT) return set_error(FG_ERR_INVALID, "unknown mode");
+    if (mode != FG_MODE_PLAIN && mode != FG_MODE_SPLIT && mode != FG_MODE_SPLIT_F16) return set_error(FG_ERR_INVALID, "unknown mode");
     Gemm g;
     g.dtype = dtype;
     g.mode = mode;

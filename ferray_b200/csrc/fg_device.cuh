@@ -338,4 +338,32 @@ __device__ __forceinline__ uint32_t elect_one() {
     return pred;
 }
 
+// FP16 split-mode operand scaling (the split kernels in prep_kernels.cuh
+// scale by 2^s, the F32 GEMM epilogue by 2^-(sA + sB)).
+// s for an operand whose max |x| has float bits `maxbits`; 0 (no scaling)
+// for an all-zero operand or one holding Inf / NaN, so those propagate as in
+// an f32 GEMM.
+__device__ __forceinline__ int f16_scale_exp(unsigned maxbits) {
+    const float mx = __uint_as_float(maxbits);
+    if (!(mx > 0.f) || !isfinite(mx)) return 0;
+    int e;
+    frexpf(mx, &e);  // mx = m 2^e, m in [0.5, 1)
+    return 15 - e;
+}
+
+// x * 2^e, applied as products by normal powers of two (each exact unless
+// the result leaves the f32 range; past +-300 it is 0 or Inf either way).
+__device__ __forceinline__ float mul_pow2(float x, int e) {
+    e = max(-300, min(300, e));
+    while (e > 120) {
+        x *= 0x1p120f;
+        e -= 120;
+    }
+    while (e < -120) {
+        x *= 0x1p-120f;
+        e += 120;
+    }
+    return x * __int_as_float((127 + e) << 23);
+}
+
 }  // namespace fg

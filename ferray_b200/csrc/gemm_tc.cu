@@ -488,18 +488,64 @@ fg_status launch_split_bf16(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
         return FG_OK;
     }
     // Real-embedded sizes for complex: (M x 2K) * (2K x 2N).
-    const int ns = g.slices == 3 ? 3 : 2;  // bf16 slices per operand
+    const bool f16 = g.mode == FG_MODE_SPLIT_F16;  // two FP16 slices of scaled operands
+    const int ns = (!f16 && g.slices == 3) ? 3 : 2;  // slices per operand
     const long long M = g.M, K = cplx ? 2 * g.K : g.K, N = cplx ? 2 * g.N : g.N;
     const long long pa = round_up(K, 8), pb = round_up(N, 8);  // bf16 elements, 16-byte pitch
     const size_t a_elems = static_cast<size_t>(pa * M * g.a_count);
     const size_t b_elems = static_cast<size_t>(pb * K * g.b_count);
     Scratch s;
-    FG_TRY(s.alloc((ns * a_elems + ns * b_elems) * sizeof(__nv_bfloat16), st));
+    const size_t plane_bytes = (ns * a_elems + ns * b_elems) * sizeof(__nv_bfloat16);
+    FG_TRY(s.alloc(round_up(plane_bytes, 256) + (f16 ? 256 : 0), st));
     BfPlanes ap{}, bp{};
     __nv_bfloat16* base = static_cast<__nv_bfloat16*>(s.p);
     for (int i = 0; i < ns; ++i) ap.p[i] = base + i * a_elems;
     for (int i = 0; i < ns; ++i) bp.p[i] = base + ns * a_elems + i * b_elems;
-    if (cplx) {
+    unsigned* amax = nullptr;  // FP16 form: max |A| and max |B| as float bits
+    if (f16) {
+        amax = reinterpret_cast<unsigned*>(static_cast<uint8_t*>(s.p) + round_up(plane_bytes, 256));
+        FG_CUDA(cudaMemsetAsync(amax, 0, 2 * sizeof(unsigned), st));
+        // complex operands: max over the interleaved (re, im) floats
+        const int cw = cplx ? 2 : 1;
+        const unsigned ga = static_cast<unsigned>(std::max<long long>(1, std::min<long long>(
+                                (g.M * g.K * cw * g.a_count / 4 + 255) / 256, 4LL * ctx->sm_count)));
+        const unsigned gb = static_cast<unsigned>(std::max<long long>(1, std::min<long long>(
+                                (g.K * g.N * cw * g.b_count / 4 + 255) / 256, 4LL * ctx->sm_count)));
+        if (g.M * g.K > 0)
+            amax_bits_kernel<<<ga, 256, 0, st>>>(static_cast<const float*>(g.A), g.M, g.K * cw, g.lda * cw,
+                                                 g.a_count, g.a_mstride * cw, amax);
+        if (g.K * g.N > 0)
+            amax_bits_kernel<<<gb, 256, 0, st>>>(static_cast<const float*>(g.B), g.K, g.N * cw, g.ldb * cw,
+                                                 g.b_count, g.b_mstride * cw, amax + 1);
+        count_launch(2);
+    }
+    if (cplx && f16) {
+        if (g.M * g.K > 0) {
+            split_f16_cplx_a_kernel<<<grid_for(g.M * g.K), 256, 0, st>>>(static_cast<const float2*>(g.A), g.M,
+                                                                         g.K, g.lda, ap, pa, amax);
+            count_launch();
+        }
+        if (g.K * g.N > 0) {
+            split_f16_cplx_b_kernel<<<grid_for(g.K * g.N), 256, 0, st>>>(static_cast<const float2*>(g.B), g.K,
+                                                                         g.N, g.ldb, bp, pb, amax + 1);
+            count_launch();
+        }
+    } else if (f16) {
+        ProfScope prof("split_f16", st);
+        if (M * K > 0) {
+            const dim3 grid(static_cast<unsigned>(std::min<long long>(M, 8LL * ctx->sm_count)), static_cast<unsigned>(g.a_count));
+            split_f16_kernel<<<grid, 256, 0, st>>>(static_cast<const float*>(g.A), M, K, g.lda, ap, pa, g.a_mstride,
+                                                   pa * M, amax);
+            count_launch();
+        }
+        if (K * N > 0) {
+            const dim3 grid(static_cast<unsigned>(std::min<long long>(K, 8LL * ctx->sm_count)), static_cast<unsigned>(g.b_count));
+            split_f16_kernel<<<grid, 256, 0, st>>>(static_cast<const float*>(g.B), K, N, g.ldb, bp, pb, g.b_mstride,
+                                                   pb * K, amax + 1);
+            count_launch();
+        }
+        prof.stop();
+    } else if (cplx) {
         if (g.M * g.K > 0) {
             if (ns == 3)
                 split_bf16_cplx_a_kernel<3><<<grid_for(g.M * g.K), 256, 0, st>>>(
@@ -542,10 +588,12 @@ fg_status launch_split_bf16(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
     TcMaps maps;
     TcArgs args{};
     int r3;
+    const CUtensorMapDataType pdt = f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
     for (int i = 0; i < ns; ++i) {
-        FG_TRY(operand_map(&maps.a[i], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, ap.p[i], K, M, pa * 2, g.a_count, pa * M * 2, 64, 128, i == 0 ? &args.a_rank3 : &r3));
-        FG_TRY(operand_map(&maps.b[i], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, bp.p[i], N, K, pb * 2, g.b_count, pb * K * 2, 64, 64, i == 0 ? &args.b_rank3 : &r3));
+        FG_TRY(operand_map(&maps.a[i], pdt, ap.p[i], K, M, pa * 2, g.a_count, pa * M * 2, 64, 128, i == 0 ? &args.a_rank3 : &r3));
+        FG_TRY(operand_map(&maps.b[i], pdt, bp.p[i], N, K, pb * 2, g.b_count, pb * K * 2, 64, 64, i == 0 ? &args.b_rank3 : &r3));
     }
+    args.f16_amax = amax;
     args.M = static_cast<int>(M);
     args.N = static_cast<int>(N);
     args.K = static_cast<int>(K);
@@ -580,9 +628,10 @@ fg_status launch_split_bf16(fg_ctx* ctx, const Gemm& g, cudaStream_t st) {
         }
         return launch_cfg<CfgBf16x6>(ctx, maps, args, st);
     }
-    args.ops[0] = TcOp{1, 0, 0, 1, 1};  // lo * hi
-    args.ops[1] = TcOp{0, 1, 0, 1, 1};  // hi * lo
-    args.ops[2] = TcOp{0, 0, 0, 1, 1};  // hi * hi
+    const int sf = f16 ? 0 : 1;  // kind::f16 operand format: 0 F16, 1 BF16
+    args.ops[0] = TcOp{1, 0, 0, sf, sf};  // lo * hi
+    args.ops[1] = TcOp{0, 1, 0, sf, sf};  // hi * lo
+    args.ops[2] = TcOp{0, 0, 0, sf, sf};  // hi * hi
     // Tuned tile variant / split-K (real products only; the complex
     // embedding's interleaving epilogue runs unsplit with 128-wide tiles).
     const TuneChoice c = cplx ? TuneChoice{0, 1} : tune_lookup(TUNE_SPLIT_F32, M, N, K);

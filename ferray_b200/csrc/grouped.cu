@@ -107,7 +107,7 @@ fg_status grouped_job_build(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, const fg_
     j->ctx = ctx;
     j->dtype = dtype;
     j->mode = mode;
-    j->kind = dtype == FG_F32 ? (mode == FG_MODE_SPLIT ? 2 : 0) : 1;
+    j->kind = dtype == FG_F32 ? (mode != FG_MODE_PLAIN ? 2 : 0) : 1;
     std::vector<int> order;
     for (size_t i = 0; i < count; ++i) {
         const fg_problem& q = table[i];

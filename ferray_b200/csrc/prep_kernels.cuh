@@ -15,9 +15,12 @@
 //  * row/column sums for the quantized GEMM's zero-point correction.
 #pragma once
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <type_traits>
+
+#include "fg_device.cuh"
 
 namespace fg {
 
@@ -41,6 +44,168 @@ __device__ __forceinline__ void split_n(float x, int ns, __nv_bfloat16 (&o)[3]) 
 __device__ __forceinline__ uint32_t pack_bf16x2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
     return static_cast<uint32_t>(__bfloat16_as_ushort(lo)) |
            (static_cast<uint32_t>(__bfloat16_as_ushort(hi)) << 16);
+}
+
+// ---- FP16 slices of power-of-two-scaled operands (split mode FP16).
+// FP16 keeps 11 significant bits (BF16: 8), so two FP16 slices carry about
+// 23 bits of an f32 against 17 for two BF16 slices, but FP16 spans only
+// [2^-24, 65504].  Each operand is therefore multiplied by 2^s with s chosen
+// from its largest magnitude so that max |x| 2^s lies in [2^14, 2^15): the hi
+// slice cannot overflow, and an entry loses bits to the FP16 subnormal range
+// only below 2^-38 of the operand's maximum.  The GEMM epilogue multiplies
+// by 2^-(sA + sB).  Powers of two scale exactly (barring f32 under/overflow).
+
+// hi = fp16(x), lo = fp16(x - hi), both round-to-nearest-even; the residual
+// x - hi is exact in f32.
+// A non-finite x keeps its Inf / NaN in hi with lo = 0.
+__device__ __forceinline__ void split_f16x2(float x, uint16_t& hi, uint16_t& lo) {
+    const __half h = __float2half_rn(x);
+    hi = __half_as_ushort(h);
+    const float hf = __half2float(h);
+    lo = isfinite(hf) ? __half_as_ushort(__float2half_rn(x - hf)) : static_cast<uint16_t>(0);
+}
+
+// max |x| over the finite entries of a row-major stack of `count` rows x cols
+// matrices (pitch ldx, matrices mstride apart), folded into *out with
+// atomicMax on the float bits (non-negative floats order like their bit
+// patterns).  Inf / NaN entries are left out, so they do not disable the
+// scaling of the finite ones.  The caller zeroes *out.
+__device__ __forceinline__ unsigned finite_abs_bits(float x) {
+    return isfinite(x) ? __float_as_uint(fabsf(x)) : 0u;
+}
+
+static __global__ void amax_bits_kernel(const float* __restrict__ X, long long rows, long long cols,
+                                        long long ldx, long long count, long long mstride,
+                                        unsigned* __restrict__ out) {
+    const bool vec = (cols % 4 == 0) && (ldx % 4 == 0) && (mstride % 4 == 0) &&
+                     ((reinterpret_cast<uintptr_t>(X) & 15) == 0);
+    const long long cq = vec ? cols / 4 : cols;
+    const long long total = count * rows * cq;
+    unsigned m = 0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long mr = e / cq, c = e - mr * cq;
+        const long long z = mr / rows, r = mr - z * rows;
+        const float* xr = X + z * mstride + r * ldx;
+        if (vec) {
+            const float4 w = __ldg(reinterpret_cast<const float4*>(xr) + c);
+            m = max(m, max(max(finite_abs_bits(w.x), finite_abs_bits(w.y)),
+                           max(finite_abs_bits(w.z), finite_abs_bits(w.w))));
+        } else {
+            m = max(m, finite_abs_bits(__ldg(xr + c)));
+        }
+    }
+    m = __reduce_max_sync(0xFFFFFFFFu, m);
+    __shared__ unsigned red[32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        unsigned v = threadIdx.x < (blockDim.x + 31) / 32 ? red[threadIdx.x] : 0u;
+        v = __reduce_max_sync(0xFFFFFFFFu, v);
+        if (threadIdx.x == 0 && v) atomicMax(out, v);
+    }
+}
+
+// Real operand -> two FP16 planes of x 2^s (s from *amax), the layout of
+// split_bf16_kernel_t: (row, 8-element group) pairs walked grid-stride, one
+// 16-byte store per plane and group.
+static __global__ void split_f16_kernel(const float* __restrict__ X, long long rows, long long cols,
+                                        long long ldx, BfPlanes out, long long ldo, long long x_bstride,
+                                        long long o_bstride, const unsigned* __restrict__ amax) {
+    constexpr int U = 4;
+    const int sc = f16_scale_exp(*amax);
+    const float* Xb = X + blockIdx.y * x_bstride;
+    const long long cq = (cols + 7) / 8;
+    const long long total = rows * cq;
+    const bool vec_in = (ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(Xb) & 15) == 0);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long e0 = blockIdx.x * (long long)blockDim.x + threadIdx.x; e0 < total; e0 += U * stride) {
+        float v[U][8];
+        long long rr[U], cc[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const long long e = e0 + u * stride;
+            rr[u] = -1;
+            cc[u] = 0;
+            if (e < total) {
+                const long long r = e / cq, c = (e - r * cq) * 8;
+                rr[u] = r;
+                cc[u] = c;
+                const float* xr = Xb + r * ldx;
+                if (vec_in && c + 7 < cols) {
+                    const float4 w0 = __ldg(reinterpret_cast<const float4*>(xr + c));
+                    const float4 w1 = __ldg(reinterpret_cast<const float4*>(xr + c + 4));
+                    v[u][0] = w0.x; v[u][1] = w0.y; v[u][2] = w0.z; v[u][3] = w0.w;
+                    v[u][4] = w1.x; v[u][5] = w1.y; v[u][6] = w1.z; v[u][7] = w1.w;
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) v[u][j] = (c + j < cols) ? xr[c + j] : 0.f;
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (rr[u] < 0) break;
+            uint32_t ph[4], pl[4];
+#pragma unroll
+            for (int j = 0; j < 8; j += 2) {
+                uint16_t h0, l0, h1, l1;
+                split_f16x2(mul_pow2(v[u][j], sc), h0, l0);
+                split_f16x2(mul_pow2(v[u][j + 1], sc), h1, l1);
+                ph[j / 2] = static_cast<uint32_t>(h0) | (static_cast<uint32_t>(h1) << 16);
+                pl[j / 2] = static_cast<uint32_t>(l0) | (static_cast<uint32_t>(l1) << 16);
+            }
+            const long long off = blockIdx.y * o_bstride + rr[u] * ldo + cc[u];
+            *reinterpret_cast<uint4*>(out.p[0] + off) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
+            *reinterpret_cast<uint4*>(out.p[1] + off) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+        }
+    }
+}
+
+// Complex operands for FP16 slices: the real embeddings of
+// split_bf16_cplx_a_kernel / split_bf16_cplx_b_kernel, scaled by 2^s.
+static __global__ void split_f16_cplx_a_kernel(const float2* __restrict__ A, long long M, long long K,
+                                               long long lda, BfPlanes out, long long ldo,
+                                               const unsigned* __restrict__ amax) {
+    const int sc = f16_scale_exp(*amax);
+    uint16_t* p0 = reinterpret_cast<uint16_t*>(out.p[0]);
+    uint16_t* p1 = reinterpret_cast<uint16_t*>(out.p[1]);
+    const long long total = M * K;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long r = e / K, c = e - r * K;
+        const float2 v = A[r * lda + c];
+        uint16_t hr, lr, hi, li;
+        split_f16x2(mul_pow2(v.x, sc), hr, lr);
+        split_f16x2(mul_pow2(v.y, sc), hi, li);
+        p0[r * ldo + c] = hr;
+        p1[r * ldo + c] = lr;
+        p0[r * ldo + K + c] = hi;
+        p1[r * ldo + K + c] = li;
+    }
+}
+
+static __global__ void split_f16_cplx_b_kernel(const float2* __restrict__ B, long long K, long long N,
+                                               long long ldb, BfPlanes out, long long ldo,
+                                               const unsigned* __restrict__ amax) {
+    const int sc = f16_scale_exp(*amax);
+    const long long total = K * N;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long r = e / N, c = e - r * N;
+        const float2 v = B[r * ldb + c];
+        uint16_t hr[2], hi[2];
+        split_f16x2(mul_pow2(v.x, sc), hr[0], hr[1]);
+        split_f16x2(mul_pow2(v.y, sc), hi[0], hi[1]);
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            uint16_t* P = reinterpret_cast<uint16_t*>(out.p[s]);
+            P[r * ldo + c] = hr[s];                                   // Br
+            P[r * ldo + N + c] = hi[s];                               // Bi
+            P[(K + r) * ldo + c] = static_cast<uint16_t>(hi[s] ^ 0x8000u);  // -Bi (sign flip, exact)
+            P[(K + r) * ldo + N + c] = hr[s];                         // Br
+        }
+    }
 }
 
 // Real operand: X (rows x cols, pitch ldx) -> NS planes (pitch ldo, a

@@ -46,9 +46,9 @@ size_t request_bytes(const fg_request& r) {
     const size_t a = in * r.m * r.k, b = in * r.k * r.n, c = out * r.m * r.n;
     size_t scratch = r.scratch_bytes;
     if (!scratch) {
-        if (r.mode == FG_MODE_SPLIT && (r.dtype == FG_F32 || r.dtype == FG_C32))
+        if (r.mode != FG_MODE_PLAIN && (r.dtype == FG_F32 || r.dtype == FG_C32))
             scratch = (r.dtype == FG_C32 ? 4 : 1) * 2 * 2 * (r.m * r.k + r.k * r.n) * 2;
-        else if (r.mode == FG_MODE_SPLIT && (r.dtype == FG_F64 || r.dtype == FG_C64))
+        else if (r.mode != FG_MODE_PLAIN && (r.dtype == FG_F64 || r.dtype == FG_C64))
             scratch = (r.dtype == FG_C64 ? 4 : 1) * 9 * (r.m * r.k + r.k * r.n + 32 * (r.m + r.n));
         else if (r.dtype == FG_I16)
             scratch = 2 * (r.m * r.k + r.k * r.n) + 64 * (r.m + r.n);

@@ -93,6 +93,10 @@ struct TcArgs {
     long long ldc, strideC;    // elements
     int accumulate;            // integer epilogues: add into C
     float alpha, beta;         // EPI_F32 (beta == 0: C is not read)
+    // EPI_F32, FP16 split: max |A| and max |B| as float bits; the products
+    // were formed from A 2^sA and B 2^sB (f16_scale_exp), so the epilogue
+    // multiplies by 2^-sA 2^-sB.  Null: no scaling.
+    const unsigned* f16_amax;
     int cplx_half;             // EPI_F32: >0 writes column j<h as Re, j>=h as Im
     // EPI_QMM
     const int* row_sum;
@@ -324,6 +328,8 @@ __device__ __forceinline__ void epilogue_store(const TcArgs& p, int bz, int grow
         }
     } else {  // EPI_F32
         float* cbase = static_cast<float*>(p.C) + bz * p.strideC;
+        // the FP16 split's operand scaling, undone (exact powers of two)
+        const int unscale = p.f16_amax ? -(f16_scale_exp(p.f16_amax[0]) + f16_scale_exp(p.f16_amax[1])) : 0;
         if (p.cplx_half > 0) {
             // Column j of the real-embedded product is Re (j < h) or Im (j >= h)
             // of complex column j mod h; C is interleaved (re, im).
@@ -341,7 +347,9 @@ __device__ __forceinline__ void epilogue_store(const TcArgs& p, int bz, int grow
                 if (j < ncols) {
                     const int col = gcol0 + j;
                     const int cc = col < h ? col : col - h;
-                    float o = p.alpha * __uint_as_float(v[0][j]);
+                    float acc = __uint_as_float(v[0][j]);
+                    if (unscale) acc = mul_pow2(acc, unscale);
+                    float o = p.alpha * acc;
                     if (p.beta != 0.f) o = fmaf(p.beta, old[j], o);
                     crow[2 * cc + (col < h ? 0 : 1)] = o;
                 }
@@ -352,6 +360,10 @@ __device__ __forceinline__ void epilogue_store(const TcArgs& p, int bz, int grow
         float out[32];
 #pragma unroll
         for (int j = 0; j < 32; ++j) out[j] = p.alpha * __uint_as_float(v[0][j]);
+        if (unscale) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) out[j] = p.alpha * mul_pow2(__uint_as_float(v[0][j]), unscale);
+        }
         const bool vec = ncols == 32 && (reinterpret_cast<uintptr_t>(crow) & 15) == 0;
         if (vec) {
             if (p.beta != 0.f) {

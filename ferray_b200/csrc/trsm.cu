@@ -286,7 +286,7 @@ struct Trsm {
     fg_status update(long long rows, long long k, const T* a, const T* x, T* c) {
         const T minus_one = T(-1), one = T(1);
         fg_mode md = mode;
-        if (dtype == FG_F64 && mode == FG_MODE_SPLIT && (rows < ozaki_min() || k < ozaki_min() || n < ozaki_min()))
+        if (dtype == FG_F64 && mode != FG_MODE_PLAIN && (rows < ozaki_min() || k < ozaki_min() || n < ozaki_min()))
             md = FG_MODE_PLAIN;
         return fg_gemm(ctx, dtype, md, 0, static_cast<size_t>(rows), static_cast<size_t>(n),
                        static_cast<size_t>(k), &minus_one, a, static_cast<size_t>(lda), x,
@@ -339,7 +339,8 @@ fg_status fg_trsm_left(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, int upper, int
     if (!ctx) return set_error(FG_ERR_INVALID, "trsm: null context");
     if (dtype != FG_F64 && dtype != FG_F32)
         return set_error(FG_ERR_DTYPE, "trsm: f64 and f32 only (trsm.rs has no other element types)");
-    if (mode != FG_MODE_PLAIN && mode != FG_MODE_SPLIT) return set_error(FG_ERR_INVALID, "trsm: bad mode");
+    if (mode != FG_MODE_PLAIN && mode != FG_MODE_SPLIT && mode != FG_MODE_SPLIT_F16)
+        return set_error(FG_ERR_INVALID, "trsm: bad mode");
     if (m == 0 || n == 0) return FG_OK;  // trsm.rs:56-58: nothing to do, B untouched
     if (!a || !b) return set_error(FG_ERR_INVALID, "trsm: null operand");
     if (lda < m || ldb < n)

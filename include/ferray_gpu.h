@@ -70,7 +70,15 @@ typedef enum fg_mode {
     /* f32/c32: 3 x BF16 products on tcgen05 with FP32 accumulation;        */
     /* f64/c64: Ozaki INT8 slicing with exact INT32 accumulation.           */
     /* Integer dtypes ignore the mode (they are exact either way).          */
-    FG_MODE_SPLIT = 1
+    FG_MODE_SPLIT = 1,
+    /* f32/c32: 3 products (hi*hi + hi*lo + lo*hi) of two FP16 slices of    */
+    /* the operands scaled by powers of two from their largest magnitudes,  */
+    /* on tcgen05 with FP32 accumulation: about 23 bits per operand against */
+    /* 17 for two BF16 slices, at the same tensor-core rate.  Grouped      */
+    /* launches (ragged batches, the server's folded small requests) run it */
+    /* as FG_MODE_SPLIT; f64/c64 and integer dtypes treat it as             */
+    /* FG_MODE_SPLIT.  No reference counterpart.                            */
+    FG_MODE_SPLIT_F16 = 2
 } fg_mode;
 
 typedef struct fg_ctx fg_ctx;
@@ -101,6 +109,19 @@ typedef struct fg_profile_entry {
 } fg_profile_entry;
 fg_status fg_profile_enable(int on);
 fg_status fg_profile_collect(fg_profile_entry *out, int capacity, int *count);
+/* Measured dense throughput of one compute pipe of this GPU, for roofline
+ * fractions against a measured rather than a spec-sheet peak (no reference
+ * counterpart).  A persistent grid keeps the pipe busy on on-chip data for
+ * about 10 ms: INT8 and BF16 as tcgen05.mma (M 128, N 256) from shared
+ * memory into TMEM, FP64 as DMMA (mma.sync m8n8k4) and FP32 as FFMA on
+ * registers.  *per_second: ops (2 per multiply-add) per second. */
+typedef enum fg_probe_pipe {
+    FG_PROBE_INT8 = 0,
+    FG_PROBE_BF16 = 1,
+    FG_PROBE_FP64 = 2,
+    FG_PROBE_FFMA = 3
+} fg_probe_pipe;
+fg_status fg_probe_peak(fg_ctx *ctx, int which, double *per_second);
 /* Device properties used for roofline bookkeeping. */
 fg_status fg_device_info(fg_ctx *ctx, int *sm_count, int *cc_major, int *cc_minor,
                          size_t *hbm_bytes);

@@ -33,3 +33,4 @@ def test_selftest_rejects_unbounded_timeouts(fg):
     ctx = fg.default_context()
     assert ctx._lib.fg_selftest_wait_timeout(ctx.handle, 0, None) == L.FG_ERR_INVALID
     assert ctx._lib.fg_selftest_wait_timeout(ctx.handle, 2000000, None) == L.FG_ERR_INVALID
+
