@@ -8,9 +8,10 @@
 //    hi/lo planes in the arena; tcgen05 kind::f16 grouped kernel, three
 //    products, K-chunked FP32 accumulation;
 //  * dtype FG_F32, mode PLAIN: persistent FFMA grouped kernel.
-// Problems are ordered by decreasing K (longest first) so the static strided
-// tile walk balances SMs.  A plan keeps the tables and arena resident and
-// replays the prep + grouped launches from a CUDA graph.
+// Tiles are numbered deepest problem first and handed out by the kernels'
+// device-side scheduler (an atomic tile counter, zeroed before every launch).
+// A plan keeps the tables and arena resident and replays the counter reset,
+// prep and grouped launches from a CUDA graph.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -72,13 +73,15 @@ struct fgrt::GroupedJob {
     long long arena = 0;
     int nseg = 0;
     size_t sz_probs = 0, sz_maps = 0, sz_ptrs = 0, sz_segs = 0, sz_tiles = 0;
+    static constexpr size_t sz_sched = 256;  // the tile scheduler's counter
     // bound state
     void* dev = nullptr;
     const void* host = nullptr;
     GroupedArgs targs{};
     SimtGroupedArgs sargs{};
     PrepSeg* d_segs = nullptr;
-    size_t host_bytes() const { return sz_probs + sz_maps + sz_ptrs + sz_segs + sz_tiles; }
+    unsigned long long* d_counter = nullptr;
+    size_t host_bytes() const { return sz_probs + sz_maps + sz_ptrs + sz_segs + sz_tiles + sz_sched; }
     size_t dev_bytes() const { return host_bytes() + static_cast<size_t>(arena); }
 };
 
@@ -214,14 +217,15 @@ fg_status grouped_job_bind(GroupedJob* j, void* dev_base, void* host_stage) {
     char* dbase = static_cast<char*>(dev_base);
     char* hbase = static_cast<char*>(host_stage);
     const size_t o_maps = j->sz_probs, o_ptrs = o_maps + j->sz_maps, o_segs = o_ptrs + j->sz_ptrs;
-    const size_t o_tiles = o_segs + j->sz_segs;
+    const size_t o_tiles = o_segs + j->sz_segs, o_sched = o_tiles + j->sz_tiles;
     char* d_arena = dbase + j->host_bytes();
+    std::memset(hbase + o_sched, 0, j->sz_sched);
+    j->d_counter = reinterpret_cast<unsigned long long*>(dbase + o_sched);
     std::memcpy(hbase, j->probs.data(), sizeof(GroupedProblem) * np);
     TileRec* htiles = reinterpret_cast<TileRec*>(hbase + o_tiles);
-    // Tiles of the deepest problems first: the persistent CTAs take tiles
-    // t, t + grid, ... so, in descending cost order, every CTA's share
-    // differs from another's by at most one tile (longest-first balance;
-    // in problem order one CTA could draw several 512-deep tiles).
+    // Tiles of the deepest problems first: the scheduler hands them out in
+    // this order, so the long tiles start first and the short ones fill in
+    // behind them (longest-first balance).
     std::vector<int> order(static_cast<size_t>(np));
     for (int x = 0; x < np; ++x) order[x] = x;
     std::stable_sort(order.begin(), order.end(),
@@ -286,6 +290,7 @@ fg_status grouped_job_bind(GroupedJob* j, void* dev_base, void* host_stage) {
         const void** dpa = reinterpret_cast<const void**>(dbase + o_ptrs);
         j->sargs.problems = reinterpret_cast<const GroupedProblem*>(dbase);
         j->sargs.tiles = dtiles;
+        j->sargs.tile_counter = j->d_counter;
         j->sargs.a = dpa;
         j->sargs.b = dpa + npp;
         j->sargs.lda = reinterpret_cast<const long long*>(dpa + 2 * npp);
@@ -299,6 +304,7 @@ fg_status grouped_job_bind(GroupedJob* j, void* dev_base, void* host_stage) {
     j->targs = GroupedArgs{};
     j->targs.problems = reinterpret_cast<const GroupedProblem*>(dbase);
     j->targs.tiles = dtiles;
+    j->targs.tile_counter = j->d_counter;
     j->targs.maps = reinterpret_cast<const CUtensorMap*>(dbase + o_maps);
     j->targs.count = np;
     j->targs.total_tiles = j->total_tiles;
@@ -343,6 +349,7 @@ static fg_status grouped_job_kernels(GroupedJob* j, cudaStream_t st) {
         return FG_OK;
     }
     const int grid = static_cast<int>(std::min<long long>(j->total_tiles, ctx->sm_count));
+    FG_CUDA(cudaMemsetAsync(j->d_counter, 0, sizeof(unsigned long long), st));
     if (j->kind == 0) {
         ProfScope prof("simt_grouped_sgemm", st);
         simt_grouped_sgemm<<<std::min<long long>(j->total_tiles, ctx->sm_count * 8), 128, 0, st>>>(j->sargs);

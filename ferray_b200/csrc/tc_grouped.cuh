@@ -3,13 +3,18 @@
 // One launch runs `count` independent problems of different M, N, K.  A
 // device-side problem table holds, per problem, its shape, its tile range in
 // a global tile numbering (prefix sums), its output and the TMA descriptors
-// of its operands (written to global memory before the launch).  Every CTA
-// walks the global tile list with a static stride; the three warp roles of
-// tc_gemm.cuh (TMA producer, MMA issuer, epilogue) each read a tile's record
-// (problem, tile row, tile column) from a host-built table, so they agree on
-// the sequence without talking to each other.  The producer prefetches the
-// tensor maps of its next tile's problem while the current one loads.  The host orders problems by
-// decreasing K so the strided walk hands every SM a similar amount of work.
+// of its operands (written to global memory before the launch).  Tiles are
+// numbered deepest problem first.  A device-side tile scheduler hands them
+// out: each CTA's producer claims the next global tile with an atomic add
+// on a counter (zeroed before every launch), so CTAs that drew short tiles
+// come back for more and the heavy tiles go first (dynamic
+// longest-processing-time order).  The producer passes each claimed tile
+// index to the CTA's MMA and epilogue roles through a small ring of
+// shared-memory slots guarded by mbarriers, so all three roles of
+// tc_gemm.cuh (TMA producer, MMA issuer, epilogue) walk the same sequence;
+// a tile index past the end tells them to stop.  The producer claims one
+// tile ahead and prefetches that tile's tensor maps while the current one
+// loads.
 #pragma once
 #include "tc_gemm.cuh"
 
@@ -33,6 +38,7 @@ struct TileRec {
 struct GroupedArgs {
     const GroupedProblem* problems;
     const TileRec* tiles;     // [total_tiles]
+    unsigned long long* tile_counter;  // next unclaimed tile (zeroed before the launch)
     const CUtensorMap* maps;  // per problem: NA A maps then NB B maps
     int count;
     long long total_tiles;
@@ -87,8 +93,17 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
     const int lane = threadIdx.x % 32;
     volatile int* abort = &s.abort;
     constexpr int NMAPS = Cfg::NA + Cfg::NB;
+    // tile-scheduler ring: the producer writes claimed tile indices, the MMA
+    // thread and the four epilogue warps read them in order
+    constexpr int SLOTS = 16;
+    __shared__ uint64_t sched_full[SLOTS], sched_empty[SLOTS];
+    __shared__ long long sched_tile[SLOTS];
 
     if (threadIdx.x == 0) {
+        for (int i = 0; i < SLOTS; ++i) {
+            mbar_init(&sched_full[i], 1);
+            mbar_init(&sched_empty[i], 5);
+        }
         for (int i = 0; i < Cfg::STAGES; ++i) {
             mbar_init(&s.full[i], 1);
             mbar_init(&s.empty[i], 1);
@@ -118,16 +133,33 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
             // kept in registers
             uint32_t issued_mask = 0, issued_par = 0;
             bool ok = true;
-            for (long long t = blockIdx.x; t < g.total_tiles && ok; t += gridDim.x) {
+            int slot = 0;
+            uint32_t sph = 0;
+            long long t = static_cast<long long>(atomicAdd(g.tile_counter, 1ull));
+            while (ok) {
+                // publish the claimed tile (or the end marker) to the other roles
+                if (!mbar_wait(&sched_empty[slot], sph ^ 1u, g.timeout_ns, g.status, 0x35, abort)) {
+                    ok = false;
+                    break;
+                }
+                sched_tile[slot] = t;
+                mbar_arrive(&sched_full[slot]);
+                if (++slot == SLOTS) {
+                    slot = 0;
+                    sph ^= 1u;
+                }
+                if (t >= g.total_tiles) break;
                 const TileRec tr = g.tiles[t];
                 const int pi = tr.problem, tm = tr.tm, tn = tr.tn;
                 const GroupedProblem pr = g.problems[pi];
                 const CUtensorMap* mp = g.maps + (long long)pi * NMAPS;
-                if (t + gridDim.x < g.total_tiles) {
-                    const int pn = g.tiles[t + gridDim.x].problem;
+                const long long t_next = static_cast<long long>(atomicAdd(g.tile_counter, 1ull));
+                if (t_next < g.total_tiles) {
+                    const int pn = g.tiles[t_next].problem;
                     if (pn != pi)
                         for (int i = 0; i < NMAPS; ++i) tma_prefetch_desc(g.maps + (long long)pn * NMAPS + i);
                 }
+                t = t_next;
                 for (int kb = 0; kb < pr.k_blocks; ++kb) {
                     if (!mbar_wait(&s.empty[stage], phase ^ 1u, g.timeout_ns, g.status, 0x31, abort)) {
                         ok = false;
@@ -165,7 +197,20 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
             uint32_t phase = 0;
             int it = 0;
             bool ok = true;
-            for (long long t = blockIdx.x; t < g.total_tiles && ok; t += gridDim.x) {
+            int slot = 0;
+            uint32_t sph = 0;
+            while (ok) {
+                if (!mbar_wait(&sched_full[slot], sph, g.timeout_ns, g.status, 0x45, abort)) {
+                    ok = false;
+                    break;
+                }
+                const long long t = sched_tile[slot];
+                mbar_arrive(&sched_empty[slot]);
+                if (++slot == SLOTS) {
+                    slot = 0;
+                    sph ^= 1u;
+                }
+                if (t >= g.total_tiles) break;
                 const int pi = g.tiles[t].problem;
                 const int kblocks = g.problems[pi].k_blocks;
                 const int kchunk = (Cfg::CHUNKED && g.kchunk > 0) ? g.kchunk : max(kblocks, 1);
@@ -228,7 +273,21 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
         uint32_t (*stg)[33] = epi_stage[ew];
         int it = 0;
         bool ok = true;
-        for (long long t = blockIdx.x; t < g.total_tiles && ok; t += gridDim.x) {
+        int slot = 0;
+        uint32_t sph = 0;
+        while (ok) {
+            if (!mbar_wait(&sched_full[slot], sph, g.timeout_ns, g.status, 0x55, abort)) {
+                ok = false;
+                break;
+            }
+            const long long t = sched_tile[slot];
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&sched_empty[slot]);
+            if (++slot == SLOTS) {
+                slot = 0;
+                sph ^= 1u;
+            }
+            if (t >= g.total_tiles) break;
             const TileRec tr = g.tiles[t];
             const int tm = tr.tm, tn = tr.tn;
             const GroupedProblem pr = g.problems[tr.problem];
@@ -387,6 +446,7 @@ static __global__ void grouped_prep_kernel(const PrepSeg* __restrict__ segs, int
 struct SimtGroupedArgs {
     const GroupedProblem* problems;
     const TileRec* tiles;  // [total_tiles]
+    unsigned long long* tile_counter;  // next unclaimed tile (zeroed before the launch)
     const void* const* a;  // per problem operand pointers and leading dims
     const void* const* b;
     const long long* lda;
@@ -473,7 +533,15 @@ static __global__ void __launch_bounds__(128) simt_grouped_sgemm(const SimtGroup
     __shared__ __align__(16) float Bs[2][BK][BN + 4];
     // 16 x 8 threads, 4 rows x 8 columns each (two 4-column groups 32 apart)
     const int tid = threadIdx.x, tx = tid % 8, ty = tid / 8;
-    for (long long t = blockIdx.x; t < g.total_tiles; t += gridDim.x) {
+    // device-side tile scheduler: thread 0 claims the next tile for the CTA;
+    // two slots, so the claim for tile i + 1 cannot overwrite the index
+    // others may still be reading for tile i
+    __shared__ long long claim[2];
+    for (int i = 0;; ++i) {
+        if (tid == 0) claim[i & 1] = static_cast<long long>(atomicAdd(g.tile_counter, 1ull));
+        __syncthreads();
+        const long long t = claim[i & 1];
+        if (t >= g.total_tiles) break;
         const TileRec tr = g.tiles[t];
         const int pi = tr.problem;
         const GroupedProblem pr = g.problems[pi];

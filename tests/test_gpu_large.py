@@ -17,12 +17,12 @@ def _sampled_err(fg, oracle, a, b, c):
     return oracle.error_vs_dd(a, b, c, rows, cols)
 
 
-def test_f32_4096_plain_split3_split6(fg, oracle):
+def test_f32_4096_plain_and_split_forms(fg, oracle):
     r = np.random.default_rng(4096)
     a, b = r.standard_normal((N, N), dtype=np.float32), r.standard_normal((N, N), dtype=np.float32)
     errs = {}
     for form, kw in (("plain", {}), ("split3", {"mode": "split", "bf16_slices": 2}),
-                     ("split6", {"mode": "split", "bf16_slices": 3})):
+                     ("split6", {"mode": "split", "bf16_slices": 3}), ("split_f16", {"mode": "split_f16"})):
         c = np.zeros((N, N), np.float32)
         assert fg.gemm_f32(N, N, N, 1.0, a, b, 0.0, c, **kw)
         errs[form] = _sampled_err(fg, oracle, a, b, c)
@@ -30,6 +30,7 @@ def test_f32_4096_plain_split3_split6(fg, oracle):
     assert errs["split3"] <= 2.0 ** -15 + N * U32, errs
     # the 6-product form: no worse than twice the plain FFMA kernel's error
     assert errs["split6"] <= 2 * errs["plain"], errs
+    assert errs["split_f16"] <= 2 * errs["plain"], errs
 
 
 @pytest.mark.parametrize("mode", ["plain", "split"])
