@@ -9,6 +9,7 @@
 // int32: at most S products of K_chunk * 127^2, with K_chunk chosen so that
 // S * K_chunk * 127^2 < 2^31.
 #include <algorithm>
+#include <cstdlib>
 #include <mutex>
 
 #include "ozaki_kernels.cuh"
@@ -31,6 +32,16 @@ static int grid_for(long long total) {
 }
 
 static long long round_up(long long x, long long a) { return (x + a - 1) / a * a; }
+
+// One launch for all slice groups (default); FG_OZAKI_FUSED=0 restores one
+// launch per group.
+static bool fused_groups() {
+    static const bool v = [] {
+        const char* e = getenv("FG_OZAKI_FUSED");
+        return !(e && e[0] == '0');
+    }();
+    return v;
+}
 
 template <class Cfg>
 static fg_status launch_group(fg_ctx* ctx, const TcMaps& maps, TcArgs& args, cudaStream_t st) {
@@ -84,18 +95,21 @@ static fg_status slice_operands(const Gemm& g, bool cplx, long long Kc, long lon
     const double* B = static_cast<const double*>(g.B);
     const long long M = g.M, K = g.K, N = g.N;
     const int cx = cplx ? 1 : 0;
-    const long long rows_per = 256;
+    // column-max passes: rows per thread, 32 (more blocks in flight) unless
+    // the grid's y extent (65535) needs more
+    const long long rows_a = std::max<long long>(32, (M + 65534) / 65535);
+    const long long rows_b = std::max<long long>(32, (K + 65534) / 65535);
     // balancing exponents of the inner dimension
     FG_CUDA(cudaMemsetAsync(kmax_a, 0, K * sizeof(unsigned long long), st));
-    dim3 agrid(static_cast<unsigned>((K + 255) / 256), static_cast<unsigned>((M + rows_per - 1) / rows_per));
-    ozaki_a_colmax_kernel<<<agrid, 256, 0, st>>>(A, M, K, g.lda, cx, rows_per, kmax_a);
-    ozaki_b_rowmax_kernel<<<grid_for(K * 32), 256, 0, st>>>(B, K, N, g.ldb, cx, kmax_b);
+    dim3 agrid(static_cast<unsigned>((K + 255) / 256), static_cast<unsigned>((M + rows_a - 1) / rows_a));
+    ozaki_a_colmax_kernel<<<agrid, 256, 0, st>>>(A, M, K, g.lda, cx, rows_a, kmax_a);
+    ozaki_b_rowmax_kernel<<<static_cast<unsigned>(std::min<long long>(K, 65535)), 256, 0, st>>>(B, K, N, g.ldb, cx, kmax_b);
     ozaki_shift_kernel<<<grid_for(K), 256, 0, st>>>(kmax_a, kmax_b, K, shift);
     // row / column scales of the balanced operands
-    ozaki_row_scale_kernel<<<grid_for(M * 32), 256, 0, st>>>(A, M, K, g.lda, cx, shift, rsc);
+    ozaki_row_scale_kernel<<<static_cast<unsigned>(std::min<long long>(M, 65535)), 256, 0, st>>>(A, M, K, g.lda, cx, shift, rsc);
     FG_CUDA(cudaMemsetAsync(cmax, 0, N * sizeof(unsigned long long), st));
-    dim3 cgrid(static_cast<unsigned>((N + 255) / 256), static_cast<unsigned>((K + rows_per - 1) / rows_per));
-    ozaki_col_max_kernel<<<cgrid, 256, 0, st>>>(B, K, N, g.ldb, cx, rows_per, shift, cmax);
+    dim3 cgrid(static_cast<unsigned>((N + 255) / 256), static_cast<unsigned>((K + rows_b - 1) / rows_b));
+    ozaki_col_max_kernel<<<cgrid, 256, 0, st>>>(B, K, N, g.ldb, cx, rows_b, shift, cmax);
     ozaki_col_scale_kernel<<<grid_for(N), 256, 0, st>>>(cmax, N, csc);
     count_launch(6);
     // Slice chunk by chunk so each chunk's digit planes are contiguous.
@@ -178,6 +192,61 @@ fg_status launch_ozaki(fg_ctx* ctx, const Gemm& g0, cudaStream_t st) {
         default: sst = slice_operands<8>(g, cplx, Kc, nchunks, Np, a_all, b_all, rsc, csc, cmax, kmax_a, kmax_b, shift, st); break;
     }
     FG_TRY(sst);
+
+    // All S slice groups in one launch when the longest group's K (S Kc)
+    // keeps its int32 accumulation exact: each tile runs its groups back to
+    // back, so C is read and written from L2 between groups, the epilogue
+    // of one group overlaps the products of the next, and there is one
+    // launch instead of S.  Longer K: one launch per group (and K piece).
+    // Measured on B200: one launch wins up to about 24 M outputs (DGEMM
+    // 4096: 1.4-1.65x plain against 1.3x); beyond, the per-group launches
+    // keep the CTAs' K positions in step and reuse operand panels in L2
+    // better (DGEMM 8192: 1.8-2.05x against 1.5-1.8x).
+    if (fused_groups() && S * Kc <= kpiece && Kc % CfgOzaki::BK == 0 && M * Nw <= (24ll << 20)) {
+        TcMaps maps;
+        TcArgs args{};
+        {
+            uint64_t dims[2] = {static_cast<uint64_t>(S * Kc), static_cast<uint64_t>(M)};
+            uint64_t strides[1] = {static_cast<uint64_t>(S * Kc)};
+            uint32_t box[2] = {128, 128};
+            FG_TRY(encode_map(&maps.a[0], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, a_all, dims, strides, box));
+        }
+        {
+            uint64_t dims[2] = {static_cast<uint64_t>(Nw), static_cast<uint64_t>(S * Kc)};
+            uint64_t strides[1] = {static_cast<uint64_t>(Np)};
+            uint32_t box[2] = {128, 128};
+            FG_TRY(encode_map(&maps.b[0], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, b_all, dims, strides, box));
+        }
+        args.M = static_cast<int>(M);
+        args.N = static_cast<int>(Nw);
+        args.K = static_cast<int>(S * Kc);
+        args.tiles_m = static_cast<int>((M + 127) / 128);
+        args.tiles_n = static_cast<int>((Nw + CfgOzaki::BN - 1) / CfgOzaki::BN);
+        args.k_blocks = static_cast<int>(S * Kc / CfgOzaki::BK);
+        args.batch = 1;
+        args.bdims = 1;
+        args.bshape[0] = 1;
+        args.C = g.C;
+        args.ldc = cplx ? 2 * g.ldc : g.ldc;
+        args.cplx_half = cplx ? static_cast<int>(g.N) : 0;
+        args.row_scale = rsc;
+        args.col_scale = csc;
+        args.oz_w = g.alpha_re;
+        args.oz_beta = g.beta_re;
+        args.oz_first = 1;
+        args.oz_groups = S;
+        args.oz_d0 = S + 1;
+        args.oz_kc_blocks = static_cast<int>(Kc / CfgOzaki::BK);
+        args.oz_S = S;
+        args.ops[0] = TcOp{0, 0, 0, 1, 1};
+        // CTA pairs (256 x 256 tiles) where the tuned i8 table picks them for
+        // the group products' shape
+        if (tune_lookup(TUNE_I8, M, Nw, Kc).variant == 2) {
+            args.tiles_m = static_cast<int>((M + 255) / 256);
+            return launch_group<CfgOzakiPair>(ctx, maps, args, st);
+        }
+        return launch_group<CfgOzaki>(ctx, maps, args, st);
+    }
 
     bool first = true;
     for (int d = S + 1; d >= 2; --d) {

@@ -46,26 +46,41 @@ __device__ __forceinline__ double scale_from_max_bits(unsigned long long bits) {
     return ldexp(1.0, e);
 }
 
+// Block-wide max of one value per thread (blockDim.x a multiple of 32, at
+// most 1024); every thread gets the result.
+__device__ __forceinline__ unsigned long long block_max_u64(unsigned long long v) {
+    __shared__ unsigned long long red[32];
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
+    __syncthreads();  // red[] may still be read from the previous call
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    v = threadIdx.x < blockDim.x / 32 ? red[threadIdx.x] : 0ull;
+    if (threadIdx.x < 32)
+        for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
+    if (threadIdx.x == 0) red[0] = v;
+    __syncthreads();
+    return red[0];
+}
+
 // Row maxima of a real (cplx = 0) or complex (cplx = 1: Re and Im) matrix,
-// one warp per row (grid-stride over rows, so any grid covers every row).
+// one block per row (blocks stride over the rows), so a row's loads are
+// spread over the block's warps.
 // `shift` (may be null) holds the balancing exponent of each K index: the row
 // maxima are those of A * diag(2^shift).
 static __global__ void ozaki_row_scale_kernel(const double* __restrict__ A, long long M,
                                               long long K, long long lda, int cplx,
                                               const int* __restrict__ shift,
                                               double* __restrict__ scale) {
-    const int lane = threadIdx.x % 32;
-    const long long warps = (long long)gridDim.x * blockDim.x / 32;
     const long long len = cplx ? 2 * K : K;
-    for (long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32; row < M; row += warps) {
+    for (long long row = blockIdx.x; row < M; row += gridDim.x) {
         const double* r = A + row * (cplx ? 2 * lda : lda);
         unsigned long long mx = 0;
-        for (long long k = lane; k < len; k += 32) {
+        for (long long k = threadIdx.x; k < len; k += blockDim.x) {
             const int sh = shift ? shift[cplx ? (k >> 1) : k] : 0;
             mx = max(mx, abs_bits(ldexp(r[k], sh)));
         }
-        for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
-        if (lane == 0) scale[row] = scale_from_max_bits(mx);
+        mx = block_max_u64(mx);
+        if (threadIdx.x == 0) scale[row] = scale_from_max_bits(mx);
     }
 }
 
@@ -115,19 +130,17 @@ static __global__ void ozaki_a_colmax_kernel(const double* __restrict__ A, long 
     atomicMax(out + k, mx);
 }
 
-// Pass 2: row maxima of B, one warp per row (grid-stride over rows).
+// Pass 2: row maxima of B, one block per row (blocks stride over the rows).
 static __global__ void ozaki_b_rowmax_kernel(const double* __restrict__ B, long long K, long long N,
                                              long long ldb, int cplx,
                                              unsigned long long* __restrict__ out) {
-    const int lane = threadIdx.x % 32;
-    const long long warps = (long long)gridDim.x * blockDim.x / 32;
     const long long len = cplx ? 2 * N : N;
-    for (long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32; row < K; row += warps) {
+    for (long long row = blockIdx.x; row < K; row += gridDim.x) {
         const double* r = B + row * (cplx ? 2 * ldb : ldb);
         unsigned long long mx = 0;
-        for (long long j = lane; j < len; j += 32) mx = max(mx, abs_bits(r[j]));
-        for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
-        if (lane == 0) out[row] = mx;
+        for (long long j = threadIdx.x; j < len; j += blockDim.x) mx = max(mx, abs_bits(r[j]));
+        mx = block_max_u64(mx);
+        if (threadIdx.x == 0) out[row] = mx;
     }
 }
 

@@ -115,6 +115,13 @@ struct TcArgs {
     const double* col_scale;
     double oz_w, oz_beta;
     int oz_first;
+    // EPI_OZAKI, all slice groups in one launch (oz_groups > 0): every tile
+    // runs groups d = oz_d0, oz_d0 - 1, ... (oz_groups of them) back to back
+    // in this CTA, group d reading K blocks [0, (d-1) oz_kc_blocks) of A and
+    // B from K block (oz_S - d + 1) oz_kc_blocks on, with weight
+    // oz_w 2^(-7d); only the first group applies oz_beta.  The tile's C block
+    // stays in L2 between its groups.
+    int oz_groups, oz_d0, oz_kc_blocks, oz_S;
     TcOp ops[TC_MAX_OPS];
     DevStatus* status;
     unsigned long long timeout_ns;
@@ -155,6 +162,22 @@ __device__ __forceinline__ void unit_coords(const TcArgs& p, int t, int& zo, int
     }
 }
 
+// Sub-unit `gi` of a tile: its K-block range and the K offset of its B rows.
+// Without fused Ozaki groups a tile has one sub-unit, the given range.
+__device__ __forceinline__ void group_range(const TcArgs& p, int gi, int kb0, int kb1, int& g0, int& g1,
+                                            int& b_koff) {
+    if (p.oz_groups > 0) {
+        const int d = p.oz_d0 - gi;
+        g0 = 0;
+        g1 = (d - 1) * p.oz_kc_blocks;
+        b_koff = (p.oz_S - d + 1) * p.oz_kc_blocks;
+    } else {
+        g0 = kb0;
+        g1 = kb1;
+        b_koff = 0;
+    }
+}
+
 __device__ __forceinline__ void batch_operands(const TcArgs& p, int bz, int& za, int& zb) {
     long long ia = 0, ib = 0;
     int rem = bz;
@@ -183,7 +206,7 @@ struct TcSmem {
 
 template <class Cfg>
 __device__ __forceinline__ void epilogue_store(const TcArgs& p, int bz, int grow, int gcol0,
-                                               const uint32_t (&v)[Cfg::NACC][32]) {
+                                               const uint32_t (&v)[Cfg::NACC][32], int oz_grp = 0) {
     const uint32_t (&v_)[Cfg::NACC][32] = v;
     if (grow >= p.M) return;
     const int ncols = min(32, p.N - gcol0);
@@ -262,9 +285,12 @@ __device__ __forceinline__ void epilogue_store(const TcArgs& p, int bz, int grow
         }
     } else if constexpr (Cfg::EPI == EPI_OZAKI) {
         double* cbase = static_cast<double*>(p.C) + bz * p.strideC;
-        const double rs = p.row_scale[grow] * p.oz_w;
+        // fused groups: weight oz_w 2^(-7d) of group d = oz_d0 - oz_grp (exact)
+        const double w = p.oz_groups > 0 ? ldexp(p.oz_w, -7 * (p.oz_d0 - oz_grp)) : p.oz_w;
+        const bool first = p.oz_first && oz_grp == 0;
+        const double rs = p.row_scale[grow] * w;
         const int h = p.cplx_half;
-        const bool need_old = !p.oz_first || p.oz_beta != 0.0;
+        const bool need_old = !first || p.oz_beta != 0.0;
         double* crow = cbase + (long long)grow * p.ldc;
         const bool vec = h == 0 && ncols == 32 && ((reinterpret_cast<uintptr_t>(crow + gcol0) & 15) == 0);
         // Two halves of 16 columns; in each, all loads (scales, old C) are
@@ -307,7 +333,7 @@ __device__ __forceinline__ void epilogue_store(const TcArgs& p, int bz, int grow
             for (int u = 0; u < 16; ++u) {
                 // exact int32 -> f64, then power-of-two scalings (exact) and alpha
                 const double t = static_cast<double>(static_cast<int32_t>(v_[0][j0 + u])) * cs[u] * rs;
-                out[u] = p.oz_first ? (p.oz_beta != 0.0 ? fma(p.oz_beta, old[u], t) : t) : old[u] + t;
+                out[u] = first ? (p.oz_beta != 0.0 ? fma(p.oz_beta, old[u], t) : t) : old[u] + t;
             }
             if (vec) {
 #pragma unroll
@@ -445,11 +471,15 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
             // (register bitmasks; an indexed array would live in local memory)
             uint32_t issued_mask = 0, issued_par = 0;
             bool ok = true;
+            const int groups = max(p.oz_groups, 1);
             for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x) {
                 int zo, bz, tm, tn, za, zb, kb0, kb1;
                 unit_coords(p, t, zo, bz, tm, tn, kb0, kb1);
                 batch_operands(p, bz, za, zb);
-                for (int kb = kb0; kb < kb1; ++kb) {
+                for (int gi = 0; gi < groups && ok; ++gi) {
+                int g0, g1, b_koff;
+                group_range(p, gi, kb0, kb1, g0, g1, b_koff);
+                for (int kb = g0; kb < g1; ++kb) {
                     if (!mbar_wait(&s.empty[stage], phase ^ 1u, p.timeout_ns, p.status, 0x01,
                                    abort)) {
                         ok = false;
@@ -457,6 +487,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
                     }
                     mbar_arrive_expect_tx(&s.full[stage], Cfg::STAGE_BYTES);
                     const int kx = kb * Cfg::BK;
+                    const int kbx = (kb + b_koff) * Cfg::BK;
                     for (int i = 0; i < Cfg::NA; ++i) {
                         if (p.a_rank3)
                             tma_load_3d(s.a[stage][i], &maps.a[i], kx, tm * Cfg::BM, za, &s.full[stage]);
@@ -469,9 +500,9 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
                             uint8_t* dst = s.b[stage][i] + c * Cfg::B_CHUNK_BYTES;
                             const int nx = tn * Cfg::BN + c * Cfg::B_CHUNK_ELEMS;
                             if (p.b_rank3)
-                                tma_load_3d(dst, &maps.b[i], nx, kx, zb, &s.full[stage]);
+                                tma_load_3d(dst, &maps.b[i], nx, kbx, zb, &s.full[stage]);
                             else
-                                tma_load_2d(dst, &maps.b[i], nx, kx, &s.full[stage]);
+                                tma_load_2d(dst, &maps.b[i], nx, kbx, &s.full[stage]);
                         }
                     }
                     issued_mask |= 1u << stage;
@@ -480,6 +511,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
                         stage = 0;
                         phase ^= 1u;
                     }
+                }
                 }
             }
             if (!ok) {
@@ -498,12 +530,16 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
             uint32_t phase = 0;
             int it = 0;  // accumulator units (tile x K chunk) issued so far
             bool ok = true;
+            const int groups = max(p.oz_groups, 1);
             for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x) {
                 int zo, bz, tm, tn, kb0, kb1;
                 unit_coords(p, t, zo, bz, tm, tn, kb0, kb1);
-                const int kchunk = (Cfg::CHUNKED && p.kchunk > 0) ? p.kchunk : kb1 - kb0;
-                for (int kc0 = kb0; kc0 < kb1 && ok; kc0 += kchunk, ++it) {
-                    const int kc1 = min(kb1, kc0 + kchunk);
+                for (int gi = 0; gi < groups && ok; ++gi) {
+                int g0, g1, b_koff;
+                group_range(p, gi, kb0, kb1, g0, g1, b_koff);
+                const int kchunk = (Cfg::CHUNKED && p.kchunk > 0) ? p.kchunk : g1 - g0;
+                for (int kc0 = g0; kc0 < g1 && ok; kc0 += kchunk, ++it) {
+                    const int kc1 = min(g1, kc0 + kchunk);
                     const int buf = it % Cfg::ACC_BUFS;
                     const uint32_t acc_par = static_cast<uint32_t>((it / Cfg::ACC_BUFS) & 1);
                     if (!mbar_wait(&s.acc_empty[buf], acc_par ^ 1u, p.timeout_ns, p.status, 0x11, abort)) {
@@ -550,6 +586,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
                     }
                     if (!ok) break;
                     tc_commit(&s.acc_full[buf]);
+                }
                 }
             }
             // Every MMA issued above has completed once `drain` flips.
@@ -613,10 +650,16 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
                 }
             }
         } else {
-            for (int t = blockIdx.x; t < total_tiles; t += gridDim.x, ++it) {
+            const int groups = max(p.oz_groups, 1);
+            bool ok = true;
+            for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x) {
+                for (int gi = 0; gi < groups; ++gi, ++it) {
                 const int buf = it % Cfg::ACC_BUFS;
                 const uint32_t acc_par = static_cast<uint32_t>((it / Cfg::ACC_BUFS) & 1);
-                if (!mbar_wait(&s.acc_full[buf], acc_par, p.timeout_ns, p.status, 0x21, abort)) break;
+                if (!mbar_wait(&s.acc_full[buf], acc_par, p.timeout_ns, p.status, 0x21, abort)) {
+                    ok = false;
+                    break;
+                }
                 tc_fence_after();
                 int zo, bz, tm, tn, kb0, kb1;
                 unit_coords(p, t, zo, bz, tm, tn, kb0, kb1);
@@ -628,11 +671,12 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
 #pragma unroll
                     for (int a = 0; a < Cfg::NACC; ++a) tmem_ld_32x32b_x32(row_addr + a * Cfg::BN + c * 32, v[a]);
                     tmem_wait_ld();
-                    epilogue_store<Cfg>(p, zo, grow, tn * Cfg::BN + c * 32, v);
+                    epilogue_store<Cfg>(p, zo, grow, tn * Cfg::BN + c * 32, v, gi);
                 }
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&s.acc_empty[buf]);
+                }
             }
         }
     }

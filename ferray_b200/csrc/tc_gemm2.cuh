@@ -148,13 +148,17 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Cfg::THREADS, 1)
             int stage = 0;
             uint32_t phase = 0;
             bool ok = true;
+            const int groups = max(p.oz_groups, 1);  // fused Ozaki slice groups per tile
             for (int t = pair; t < total && ok; t += npairs) {
                 int zo, bz, tm, tn, za, zb, kb0, kb1;
                 unit_coords(p, t, zo, bz, tm, tn, kb0, kb1);
                 batch_operands(p, bz, za, zb);
                 const int row0 = tm * Cfg::BM + static_cast<int>(rank) * Cfg::CTA_M;
                 const int col0 = tn * Cfg::TILE_N + static_cast<int>(rank) * Cfg::CTA_N;
-                for (int kb = kb0; kb < kb1; ++kb) {
+                for (int gi = 0; gi < groups && ok; ++gi) {
+                int g0, g1, b_koff;
+                group_range(p, gi, kb0, kb1, g0, g1, b_koff);
+                for (int kb = g0; kb < g1; ++kb) {
                     if (!mbar_wait(&s.empty[stage], phase ^ 1u, p.timeout_ns, p.status, 0x01, abort)) {
                         ok = false;
                         break;
@@ -162,6 +166,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Cfg::THREADS, 1)
                     if (leader) mbar_arrive_expect_tx(&s.full[stage], 2 * Cfg::STAGE_BYTES);
                     const uint32_t fb = mapa_shared(smem_u32(&s.full[stage]), 0);
                     const int kx = kb * Cfg::BK;
+                    const int kbx = (kb + b_koff) * Cfg::BK;
                     for (int i = 0; i < Cfg::NA; ++i) {
                         if (p.a_rank3)
                             tma_load_3d_pair(s.a[stage][i], &maps.a[i], kx, row0, za, fb);
@@ -176,15 +181,16 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Cfg::THREADS, 1)
                             const int nx = col0 + (Cfg::COLSPLIT ? i * Cfg::BN : 0) + c * Cfg::B_CHUNK_ELEMS;
                             const CUtensorMap* mb = &maps.b[Cfg::COLSPLIT ? 0 : i];
                             if (p.b_rank3)
-                                tma_load_3d_pair(dst, mb, nx, kx, zb, fb);
+                                tma_load_3d_pair(dst, mb, nx, kbx, zb, fb);
                             else
-                                tma_load_2d_pair(dst, mb, nx, kx, fb);
+                                tma_load_2d_pair(dst, mb, nx, kbx, fb);
                         }
                     }
                     if (++stage == Cfg::STAGES) {
                         stage = 0;
                         phase ^= 1u;
                     }
+                }
                 }
             }
             if (ok) {
@@ -207,12 +213,16 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Cfg::THREADS, 1)
             uint32_t phase = 0;
             int it = 0;
             bool ok = true;
+            const int groups = max(p.oz_groups, 1);
             for (int t = pair; t < total && ok; t += npairs) {
                 int zo, bz, tm, tn, kb0, kb1;
                 unit_coords(p, t, zo, bz, tm, tn, kb0, kb1);
-                const int kchunk = (Cfg::CHUNKED && p.kchunk > 0) ? p.kchunk : kb1 - kb0;
-                for (int kc0 = kb0; kc0 < kb1 && ok; kc0 += kchunk, ++it) {
-                    const int kc1 = min(kb1, kc0 + kchunk);
+                for (int gi = 0; gi < groups && ok; ++gi) {
+                int g0, g1, b_koff;
+                group_range(p, gi, kb0, kb1, g0, g1, b_koff);
+                const int kchunk = (Cfg::CHUNKED && p.kchunk > 0) ? p.kchunk : g1 - g0;
+                for (int kc0 = g0; kc0 < g1 && ok; kc0 += kchunk, ++it) {
+                    const int kc1 = min(g1, kc0 + kchunk);
                     const int buf = it % Cfg::ACC_BUFS;
                     const uint32_t acc_par = static_cast<uint32_t>((it / Cfg::ACC_BUFS) & 1);
                     if (!mbar_wait(&s.acc_empty[buf], acc_par ^ 1u, p.timeout_ns, p.status, 0x11, abort)) {
@@ -258,6 +268,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Cfg::THREADS, 1)
                     }
                     if (!ok) break;
                     tc_commit_pair_mc(&s.acc_full[buf], 0x3);
+                }
                 }
             }
             tc_commit_pair(&s.drain);
@@ -313,10 +324,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Cfg::THREADS, 1)
                     epilogue_store<Cfg>(p, zo, grow, tn * Cfg::BN + c * 32, v);
                 }
             } else {
+                for (int gi = 0; gi < max(p.oz_groups, 1); ++gi) {
                 const int buf = it % Cfg::ACC_BUFS;
                 const uint32_t acc_par = static_cast<uint32_t>((it / Cfg::ACC_BUFS) & 1);
                 ++it;
-                if (!mbar_wait(&s.acc_full[buf], acc_par, p.timeout_ns, p.status, 0x21, abort)) break;
+                if (!mbar_wait(&s.acc_full[buf], acc_par, p.timeout_ns, p.status, 0x21, abort)) {
+                    ok = false;
+                    break;
+                }
                 tc_fence_after();
                 const uint32_t row_addr =
                     tmem + (static_cast<uint32_t>(ew * 32) << 16) + buf * Cfg::ACC_COLS;
@@ -338,12 +353,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Cfg::THREADS, 1)
 #pragma unroll
                         for (int a = 0; a < Cfg::NACC; ++a) tmem_ld_32x32b_x32(row_addr + a * Cfg::BN + c * 32, v[a]);
                         tmem_wait_ld();
-                        epilogue_store<Cfg>(p, zo, grow, tn * Cfg::BN + c * 32, v);
+                        epilogue_store<Cfg>(p, zo, grow, tn * Cfg::BN + c * 32, v, gi);
                     }
                 }
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive_cluster(mapa_shared(smem_u32(&s.acc_empty[buf]), 0));
+                }
             }
         }
     }

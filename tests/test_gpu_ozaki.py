@@ -133,3 +133,48 @@ def test_split_long_k_group_pieces(fg, oracle, m, n, k, cplx):
         assert fg.gemm_f64(m, n, k, 1.0, a, b, 0.0, c, mode="split")
     err = oracle.error_vs_dd(a, b, c)
     assert err <= (2 if cplx else 1) * k * U64 + 11 * 2.0 ** (2 - 63), err
+
+
+_PER_GROUP_SCRIPT = r"""
+import sys, numpy as np
+sys.path.insert(0, sys.argv[1])
+import ferray_b200 as fg
+d = np.load(sys.argv[2])
+a, b, cplx = d["a"], d["b"], bool(d["cplx"])
+m, k = a.shape
+n = b.shape[1]
+c = np.zeros((m, n), a.dtype)
+if cplx:
+    assert fg.gemm_c64(m, n, k, 1.5, 0.0, a, b, 0.0, 0.0, c, mode="split")
+else:
+    assert fg.gemm_f64(m, n, k, 1.5, a, b, 0.0, c, mode="split")
+np.save(sys.argv[3], c)
+"""
+
+
+@pytest.mark.parametrize("m,n,k,cplx", [(300, 257, 129, False), (513, 1000, 700, False), (200, 150, 300, True)])
+def test_fused_groups_bit_identical_to_group_launches(fg, tmp_path, m, n, k, cplx):
+    """All slice groups in one launch (the default) give the same bits as
+    one launch per group (FG_OZAKI_FUSED=0, run in a child process): the
+    FP64 epilogue adds the groups to C in the same order either way."""
+    import os
+    import subprocess
+    import sys
+    r = np.random.default_rng(m + n + k)
+    a = r.standard_normal((m, k)) * 10.0 ** r.uniform(-4, 4, (m, 1))
+    b = r.standard_normal((k, n)) * 10.0 ** r.uniform(-4, 4, (1, n))
+    if cplx:
+        a = a + 1j * r.standard_normal((m, k))
+        b = b + 1j * r.standard_normal((k, n))
+    c = np.zeros((m, n), a.dtype)
+    if cplx:
+        assert fg.gemm_c64(m, n, k, 1.5, 0.0, a, b, 0.0, 0.0, c, mode="split")
+    else:
+        assert fg.gemm_f64(m, n, k, 1.5, a, b, 0.0, c, mode="split")
+    np.savez(tmp_path / "in.npz", a=a, b=b, cplx=cplx)
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, FG_OZAKI_FUSED="0")
+    subprocess.run([sys.executable, "-c", _PER_GROUP_SCRIPT, root, str(tmp_path / "in.npz"),
+                    str(tmp_path / "out.npy")], check=True, env=env, timeout=300)
+    ref = np.load(tmp_path / "out.npy")
+    assert np.array_equal(c.view(np.uint8), ref.view(np.uint8))

@@ -52,8 +52,11 @@ def test_f16_split_scaling_far_outside_fp16_range(fg, oracle, scale_a, scale_b):
     assert fg.gemm_f32(m, n, k, 1.0, a, b, 0.0, c, mode="split_f16")
     assert fg.gemm_f32(m, n, k, 1.0, a, b, 0.0, cp)
     assert np.all(np.isfinite(c))
+    # scaling keeps the error what it is for unscaled data: the
+    # representation bound, and the same order as plain FFMA's
     e, ep = _err(oracle, a, b, c), _err(oracle, a, b, cp)
-    assert e <= 4 * ep, (e, ep)
+    assert e <= 2.0 ** -21 + k * U32, (e, ep)
+    assert e <= 8 * ep, (e, ep)
 
 
 def test_f16_split_mixed_magnitudes_zeros_and_nonfinite(fg, oracle):
@@ -105,7 +108,8 @@ def test_f16_split_complex(fg, oracle):
     assert fg.gemm_c32(m, n, k, 1.0, 0.0, a, b, 0.0, 0.0, c, mode="split_f16")
     assert fg.gemm_c32(m, n, k, 1.0, 0.0, a, b, 0.0, 0.0, cp)
     e, ep = _err(oracle, a, b, c), _err(oracle, a, b, cp)
-    assert e <= 4 * ep, (e, ep)
+    assert e <= 2.0 ** -21 + 2 * k * U32, (e, ep)
+    assert e <= 8 * ep, (e, ep)
 
 
 def test_f16_split_forced_splitk_and_tiles(fg, oracle):
@@ -115,12 +119,14 @@ def test_f16_split_forced_splitk_and_tiles(fg, oracle):
     m, n, k = 256, 256, 2048
     a = r.standard_normal((m, k)).astype(np.float32)
     b = r.standard_normal((k, n)).astype(np.float32)
-    cp = np.zeros((m, n), np.float32)
-    assert fg.gemm_f32(m, n, k, 1.0, a, b, 0.0, cp)
-    ep = _err(oracle, a, b, cp)
+    c0 = np.zeros((m, n), np.float32)
+    assert fg.gemm_f32(m, n, k, 1.0, a, b, 0.0, c0, mode="split_f16")
+    e0 = _err(oracle, a, b, c0)
+    assert e0 <= 2.0 ** -21 + k * U32
     for variant in (0, 1, 2):
         for splits in (1, 4):
             with fg.tune_forced("split_f32", variant, splits):
                 c = np.zeros((m, n), np.float32)
                 assert fg.gemm_f32(m, n, k, 1.0, a, b, 0.0, c, mode="split_f16")
-            assert _err(oracle, a, b, c) <= 2 * ep + 2.0 ** -30, (variant, splits)
+            # the same products in another tile / K order: the same error level
+            assert _err(oracle, a, b, c) <= 2 * e0, (variant, splits)
