@@ -301,7 +301,7 @@ def side_measurements(fg, L, lib, ctx, stream, n, only=""):
     if not only or only == "ozaki":
         res["ozaki_f64_c128"] = bc.ozaki_sweep(R)
     if only == "ozaki_all":
-        res["ozaki_sweep_all_slices"] = bc.ozaki_sweep(R, slices=(6, 7, 8, 9), cpu=False)
+        res["ozaki_sweep_all_slices"] = bc.ozaki_sweep(R, slices=(6, 7, 8, 9, 12, 14, 16, 17, 18, 20), cpu=False)
     if not only or only == "ragged":
         # --- ragged grouped batch, 4096 problems, dims log-uniform in [8, 512]
         dims = ragged_dims()

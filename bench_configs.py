@@ -2,15 +2,17 @@
 each, every GPU number next to its error against the double-double oracle
 and the CPU rate of ferray's restated GEMM (the oracle) on the same shape:
 
-* DGEMM f64 M = N = K = 1024, U[-1, 1), plain and Ozaki split, error vs the
-  DD oracle over the full C;
+* DGEMM f64 M = N = K = 1024, U[-1, 1), plain and Ozaki split (scheme II
+  with 16 moduli, the default, and scheme I with 9 slices), error vs the DD
+  oracle over the full C;
 * SGEMM f32 N in {256, 1024, 2048, 4096}, N(0, 1): plain FFMA, 3 x BF16
   (2 slices) and 6 x BF16 (3 slices) split;
 * CGEMM c32 N = 4096, Re and Im N(0, 1): plain, 3- and 6-product split;
 * DGEMM f64 / ZGEMM c128 at N in {2048, 4096, 8192} with exponent spread
   s in {0, 4, 8} (A = diag(10^(s u)) G diag(10^(s v)), G ~ N(0, 1),
   u, v ~ U[-1, 1]; B built the same way independently): plain FP64 vs
-  INT8-Ozaki with 8 and 9 slices, errors per spread;
+  INT8-Ozaki scheme I (8, 9 slices) and scheme II (16, 17 moduli), errors
+  per spread;
 * square i8 x i8 -> i32 at N in {1024, 4096, 8192}, bit-exact on a sample.
 
 Workloads are seeded synthetic data with the configs' shapes and value
@@ -176,7 +178,8 @@ def dgemm_1024(R):
     ref = oracle.dd_full(a, b)
     na, nb = oracle.fro(a), oracle.fro(b)
     out = {}
-    for name, mode, sl in (("plain", L.FG_MODE_PLAIN, 0), ("split_ozaki9", L.FG_MODE_SPLIT, 9)):
+    for name, mode, sl in (("plain", L.FG_MODE_PLAIN, 0), ("split_crt16", L.FG_MODE_SPLIT, 0),
+                           ("split_ozaki9", L.FG_MODE_SPLIT, 9)):
         ms = R.time(R.gemm(L.FG_F64, mode, sl, n, n, n, da.ptr, db.ptr, dc.ptr))
         err = oracle.normwise_error(dc.to_numpy(), ref, n, n, na, nb)
         out[name] = _entry(2.0 * n ** 3, ms, err)
@@ -255,9 +258,15 @@ def _spread_operand(torch, nn, spread, cplx, gen):
     return (du[:, None] * g) * dv[None, :]
 
 
-def ozaki_sweep(R, sizes=(2048, 4096, 8192), spreads=(0, 4, 8), slices=(8, 9), cpu=True):
-    """DGEMM / ZGEMM: plain FP64 (DMMA) vs INT8-Ozaki per exponent spread and
-    slice count, errors vs the DD oracle on a sampled 64 x 64 block."""
+def _oz_name(s):
+    return ("ozaki%d" if s <= 10 else "crt%d") % s
+
+
+def ozaki_sweep(R, sizes=(2048, 4096, 8192), spreads=(0, 4, 8), slices=(8, 9, 16, 17), cpu=True):
+    """DGEMM / ZGEMM: plain FP64 (DMMA) vs INT8-Ozaki per exponent spread:
+    scheme I with 8 / 9 slices ("ozaki8", "ozaki9") and scheme II with 16 /
+    17 moduli ("crt16", "crt17"); errors vs the DD oracle on a sampled
+    64 x 64 block."""
     import oracle
     torch, L = R.torch, R.L
     out = {}
@@ -280,13 +289,13 @@ def ozaki_sweep(R, sizes=(2048, 4096, 8192), spreads=(0, 4, 8), slices=(8, 9), c
                 flops = (8.0 if cplx else 2.0) * nn ** 3
                 entry = {}
                 for name, mode, sl in [("plain", L.FG_MODE_PLAIN, 0)] + \
-                        [("ozaki%d" % s, L.FG_MODE_SPLIT, s) for s in slices]:
+                        [(_oz_name(s), L.FG_MODE_SPLIT, s) for s in slices]:
                     ms = R.time(R.gemm(dt, mode, sl, nn, nn, nn, a.data_ptr(), b.data_ptr(), c.data_ptr()),
                                 min_ms=20.0)
                     got = c.index_select(0, ri).index_select(1, ci).cpu().numpy()
                     entry[name] = _entry(flops, ms, oracle.normwise_error(got, ref, nn, nn, na, nb))
                 for s in slices:
-                    e = entry["ozaki%d" % s]
+                    e = entry[_oz_name(s)]
                     e["speed_over_plain"] = round(entry["plain"]["ms"] / e["ms"], 2)
                     e["err_over_plain"] = round(e["normwise_err"] / entry["plain"]["normwise_err"], 3)
                 out["%s_%d_spread%d" % ("zgemm" if cplx else "dgemm", nn, spread)] = entry

@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <mutex>
+#include <vector>
 
 #include "ozaki_kernels.cuh"
 #include "runtime.h"
@@ -86,10 +87,10 @@ static fg_status launch_group(fg_ctx* ctx, const TcMaps& maps, TcArgs& args, cud
     return FG_OK;
 }
 
-template <int S>
-static fg_status slice_operands(const Gemm& g, bool cplx, long long Kc, long long nchunks,
-                                long long Np, int8_t* a_all, int8_t* b_all, double* rsc,
-                                double* csc, unsigned long long* cmax, unsigned long long* kmax_a,
+// Balancing exponents of the inner dimension, then the row scales of A D
+// and the column scales of D^-1 B (powers of two), shared by both schemes.
+static fg_status scale_operands(const Gemm& g, bool cplx, double* rsc, double* csc,
+                                unsigned long long* cmax, unsigned long long* kmax_a,
                                 unsigned long long* kmax_b, int* shift, cudaStream_t st) {
     const double* A = static_cast<const double*>(g.A);
     const double* B = static_cast<const double*>(g.B);
@@ -112,6 +113,20 @@ static fg_status slice_operands(const Gemm& g, bool cplx, long long Kc, long lon
     ozaki_col_max_kernel<<<cgrid, 256, 0, st>>>(B, K, N, g.ldb, cx, rows_b, shift, cmax);
     ozaki_col_scale_kernel<<<grid_for(N), 256, 0, st>>>(cmax, N, csc);
     count_launch(6);
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+template <int S>
+static fg_status slice_operands(const Gemm& g, bool cplx, long long Kc, long long nchunks,
+                                long long Np, int8_t* a_all, int8_t* b_all, double* rsc,
+                                double* csc, unsigned long long* cmax, unsigned long long* kmax_a,
+                                unsigned long long* kmax_b, int* shift, cudaStream_t st) {
+    const double* A = static_cast<const double*>(g.A);
+    const double* B = static_cast<const double*>(g.B);
+    const long long M = g.M, K = g.K, N = g.N;
+    const int cx = cplx ? 1 : 0;
+    FG_TRY(scale_operands(g, cplx, rsc, csc, cmax, kmax_a, kmax_b, shift, st));
     // Slice chunk by chunk so each chunk's digit planes are contiguous.
     for (long long c = 0; c < nchunks; ++c) {
         ozaki_slice_a_kernel<S><<<grid_for(M * Kc), 256, 0, st>>>(
@@ -119,6 +134,192 @@ static fg_status slice_operands(const Gemm& g, bool cplx, long long Kc, long lon
         ozaki_slice_b_kernel<S><<<grid_for(Kc * Np), 256, 0, st>>>(
             B, K, N, g.ldb, cx, shift, csc, b_all + c * S * Kc * Np, Kc, Np, c * Kc);
         count_launch(2);
+    }
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+// ------------------------------------------------------------ scheme II
+// Pairwise coprime moduli, largest first, each <= 256 so that a symmetric
+// residue fits int8; a call uses the first n (12..20).
+static const int kOz2Moduli[20] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227,
+                                   223, 217, 211, 199, 197, 193, 191, 181, 179, 173};
+
+// Unsigned big integer, base 2^32 limbs, least significant first: just the
+// operations the CRT constants need.
+struct BigU {
+    std::vector<uint32_t> w{1u};
+    void mul(uint32_t f) {
+        uint64_t carry = 0;
+        for (auto& x : w) {
+            const uint64_t t = static_cast<uint64_t>(x) * f + carry;
+            x = static_cast<uint32_t>(t);
+            carry = t >> 32;
+        }
+        if (carry) w.push_back(static_cast<uint32_t>(carry));
+    }
+    uint32_t divmod(uint32_t d) {  // *this /= d, returns the remainder
+        uint64_t rem = 0;
+        for (size_t i = w.size(); i-- > 0;) {
+            const uint64_t cur = (rem << 32) | w[i];
+            w[i] = static_cast<uint32_t>(cur / d);
+            rem = cur % d;
+        }
+        while (w.size() > 1 && w.back() == 0) w.pop_back();
+        return static_cast<uint32_t>(rem);
+    }
+    int bits() const {
+        int b = 32 * static_cast<int>(w.size() - 1);
+        for (uint32_t t = w.back(); t; t >>= 1) ++b;
+        return b;
+    }
+    uint64_t bits_at(int lo, int n) const {  // n <= 40 bits starting at bit lo
+        uint64_t v = 0;
+        for (int b = 0; b < n; ++b) {
+            const int q = lo + b;
+            if (q / 32 < static_cast<int>(w.size()) && ((w[q / 32] >> (q % 32)) & 1u)) v |= 1ull << b;
+        }
+        return v;
+    }
+    double to_double() const {
+        double v = 0;
+        for (size_t i = w.size(); i-- > 0;) v = v * 4294967296.0 + w[i];
+        return v;
+    }
+};
+
+static int inverse_mod(int a, int m) {  // a^-1 mod m (gcd(a, m) = 1)
+    int t = 0, nt = 1, r = m, nr = a % m;
+    while (nr) {
+        const int q = r / nr;
+        std::swap(t, nt);
+        nt -= q * t;
+        std::swap(r, nr);
+        nr -= q * r;
+    }
+    return t < 0 ? t + m : t;
+}
+
+// Constants of an n-moduli call with inner dimension K: P is the largest
+// integer precision (at most 59, so rint(x / m) in oz2_residue is off by at
+// most one) with K 2^(2P) < Mp / 4, i.e. every |C'| far from Mp / 2.
+static Oz2Consts oz2_consts(int n, long long K) {
+    Oz2Consts c{};
+    c.n = n;
+    BigU Mp;
+    for (int l = 0; l < n; ++l) Mp.mul(static_cast<uint32_t>(kOz2Moduli[l]));
+    int logk = 0;
+    while ((1ll << logk) < K) ++logk;
+    c.P = std::min(59, (Mp.bits() - 1 - logk - 2) / 2);
+    for (int l = 0; l < n; ++l) {
+        const int m = kOz2Moduli[l];
+        BigU W = Mp;
+        W.divmod(static_cast<uint32_t>(m));  // exact: Mp / m_l
+        c.m[l] = m;
+        c.inv_m[l] = 1.0 / m;
+        for (int d = 0; d < 4; ++d) c.W[l][d] = static_cast<double>(W.bits_at(40 * d, 40));
+    }
+    for (int d = 0; d < 4; ++d) c.Mc[d] = static_cast<double>(Mp.bits_at(40 * d, 40));
+    c.M_d = Mp.to_double();
+    return c;
+}
+
+static int oz2_y(int n, int l) {  // ((Mp / m_l) mod m_l)^-1 mod m_l
+    BigU Mp;
+    for (int q = 0; q < n; ++q) Mp.mul(static_cast<uint32_t>(kOz2Moduli[q]));
+    Mp.divmod(static_cast<uint32_t>(kOz2Moduli[l]));
+    const int w_mod = static_cast<int>(Mp.divmod(static_cast<uint32_t>(kOz2Moduli[l])));
+    return inverse_mod(w_mod, kOz2Moduli[l]);
+}
+
+using CfgCrt = TcCfg<KIND_I8, 256, 4, 1, 1, 1, 1, EPI_CRT>;
+using CfgCrtPair = Tc2Cfg<KIND_I8, 256, 6, 1, 1, 1, 1, EPI_CRT>;
+
+// Scheme II DGEMM / ZGEMM with n moduli (real GEMM, or the complex real
+// embedding (M x 2K)(2K x 2N) like scheme I).
+static fg_status launch_ozaki2(fg_ctx* ctx, const Gemm& g, int n, cudaStream_t st) {
+    const bool cplx = g.dtype == FG_C64;
+    const long long M = g.M, Kw = cplx ? 2 * g.K : g.K, Nw = cplx ? 2 * g.N : g.N;
+    const long long Kp = round_up(std::max<long long>(Kw, 1), 128), Np = round_up(Nw, 16);
+    const Oz2Consts c = oz2_consts(n, Kw);
+    const size_t a_bytes = static_cast<size_t>(M * n * Kp), b_bytes = static_cast<size_t>(n * Kp * Np);
+    const size_t r_bytes = static_cast<size_t>(n * M * Nw);
+    const size_t n_sc = static_cast<size_t>(g.N);
+    const size_t meta = (M + n_sc) * sizeof(double) + n_sc * sizeof(unsigned long long) +
+                        2 * g.K * sizeof(unsigned long long) + g.K * sizeof(int);
+    Scratch sc;
+    FG_TRY(sc.alloc(round_up(a_bytes, 256) + round_up(b_bytes, 256) + round_up(r_bytes, 256) + meta, st));
+    int8_t* a_all = static_cast<int8_t*>(sc.p);
+    int8_t* b_all = a_all + round_up(a_bytes, 256);
+    uint8_t* res = reinterpret_cast<uint8_t*>(b_all + round_up(b_bytes, 256));
+    double* rsc = reinterpret_cast<double*>(res + round_up(r_bytes, 256));
+    double* csc = rsc + M;
+    unsigned long long* cmax = reinterpret_cast<unsigned long long*>(csc + n_sc);
+    unsigned long long* kmax_a = cmax + n_sc;
+    unsigned long long* kmax_b = kmax_a + g.K;
+    int* shift = reinterpret_cast<int*>(kmax_b + g.K);
+    FG_TRY(scale_operands(g, cplx, rsc, csc, cmax, kmax_a, kmax_b, shift, st));
+    const double* A = static_cast<const double*>(g.A);
+    const double* B = static_cast<const double*>(g.B);
+    oz2_residue_a_kernel<<<grid_for(M * Kp), 256, 0, st>>>(A, M, g.K, g.lda, cplx ? 1 : 0, shift, rsc, a_all, Kp, c);
+    oz2_residue_b_kernel<<<grid_for(Kp * Np), 256, 0, st>>>(B, g.K, g.N, g.ldb, cplx ? 1 : 0, shift, csc, b_all, Kp, Np, c);
+    count_launch(2);
+    FG_CUDA(cudaGetLastError());
+
+    const bool pair = tune_lookup(TUNE_I8, M, Nw, Kp).variant == 2;
+    const bool fused = fused_groups();
+    const int launches = fused ? 1 : n;
+    for (int L = 0; L < launches; ++L) {
+        TcMaps maps;
+        TcArgs args{};
+        const long long kw = fused ? n * Kp : Kp;
+        {
+            uint64_t dims[2] = {static_cast<uint64_t>(kw), static_cast<uint64_t>(M)};
+            uint64_t strides[1] = {static_cast<uint64_t>(n * Kp)};
+            uint32_t box[2] = {128, 128};
+            FG_TRY(encode_map(&maps.a[0], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, a_all + (fused ? 0 : L * Kp), dims,
+                              strides, box));
+        }
+        {
+            uint64_t dims[2] = {static_cast<uint64_t>(Nw), static_cast<uint64_t>(kw)};
+            uint64_t strides[1] = {static_cast<uint64_t>(Np)};
+            uint32_t box[2] = {128, 128};
+            FG_TRY(encode_map(&maps.b[0], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, b_all + (fused ? 0 : L * Kp * Np), dims,
+                              strides, box));
+        }
+        args.M = static_cast<int>(M);
+        args.N = static_cast<int>(Nw);
+        args.K = static_cast<int>(kw);
+        args.tiles_m = static_cast<int>((M + (pair ? 255 : 127)) / (pair ? 256 : 128));
+        args.tiles_n = static_cast<int>((Nw + CfgCrt::BN - 1) / CfgCrt::BN);
+        args.k_blocks = static_cast<int>(kw / CfgCrt::BK);
+        args.batch = 1;
+        args.bdims = 1;
+        args.bshape[0] = 1;
+        args.C = res + (fused ? 0 : L * M * Nw);
+        args.ldc = Nw;
+        args.oz_crt = 1;
+        args.oz_groups = fused ? n : 1;
+        args.oz_kc_blocks = static_cast<int>(Kp / CfgCrt::BK);
+        args.crt_plane = M * Nw;
+        for (int q = 0; q < (fused ? n : 1); ++q) {
+            const int l = fused ? q : L;
+            args.crt_m[q] = kOz2Moduli[l];
+            args.crt_y[q] = oz2_y(n, l);
+        }
+        args.ops[0] = TcOp{0, 0, 0, 1, 1};
+        if (pair)
+            FG_TRY(launch_group<CfgCrtPair>(ctx, maps, args, st));
+        else
+            FG_TRY(launch_group<CfgCrt>(ctx, maps, args, st));
+    }
+    {
+        ProfScope prof("oz2_reconstruct", st);
+        oz2_reconstruct_kernel<<<grid_for(M * Nw), 256, 0, st>>>(
+            res, M, Nw, M * Nw, rsc, csc, static_cast<double*>(g.C), g.ldc, cplx ? static_cast<int>(g.N) : 0,
+            g.alpha_re, g.beta_re, c);
+        prof.stop();
+        count_launch();
     }
     FG_CUDA(cudaGetLastError());
     return FG_OK;
@@ -149,12 +350,23 @@ fg_status launch_ozaki(fg_ctx* ctx, const Gemm& g0, cudaStream_t st) {
     }
     const Gemm& g = g0;
     const bool cplx = g.dtype == FG_C64;
-    // 9 slices by default: with K balancing this keeps the normwise error well
-    // below plain FP64's for exponent spreads up to 10^8 (8 is about equal).
-    const int S = g.slices > 0 ? g.slices : 9;
-    if (S < 3 || S > 10) return set_error(FG_ERR_INVALID, "ozaki_slices must be in 3..10");
+    // Default: scheme II with 16 moduli (DGEMM 8192: 3.3-3.5x plain FP64 at
+    // 0.01-0.03x its normwise error for exponent spreads up to 10^8).
+    // Scheme I: 9 slices keep the error well below plain FP64's (8 are about
+    // equal).
+    int S = g.slices > 0 ? g.slices : 16;
+    if (S < 3 || (S > 10 && S < 12) || S > 20)
+        return set_error(FG_ERR_INVALID, "ozaki_slices must be in 3..10 (scheme I slices) or 12..20 (scheme II moduli)");
     if (g.alpha_im != 0.0 || g.beta_im != 0.0)
         return set_error(FG_ERR_UNSUPPORTED, "split ZGEMM: complex alpha/beta must be real");
+    if (S >= 12) {
+        // scheme II: one int8 GEMM per modulus, while each product's exact
+        // int32 sum holds (K 128^2 < 2^31); longer K (and empty problems)
+        // run as scheme I with 9 slices
+        if (round_up(cplx ? 2 * g.K : g.K, 128) <= 130944 && g.K > 0 && g.M > 0 && g.N > 0)
+            return launch_ozaki2(ctx, g, S, st);
+        S = 9;
+    }
     const long long M = g.M, Kw = cplx ? 2 * g.K : g.K, Nw = cplx ? 2 * g.N : g.N;
     // The operands are sliced once over the whole (padded) K; int32
     // exactness is kept per launch instead: a launch accumulates at most

@@ -255,4 +255,152 @@ __global__ void ozaki_slice_b_kernel(const double* __restrict__ B, long long K, 
     }
 }
 
+// ---------------------------------------------------------------- scheme II
+// Ozaki scheme II (Ozaki, Uchino, Imamura: integer emulation of FP64 GEMM by
+// the Chinese remainder theorem).  After the same balancing and row / column
+// scaling as the slices above, every entry becomes one integer
+//     a'_ik = rint(2^P a_ik 2^sh_k / 2^e_i),  |a'| <= 2^P,
+// exactly representable as a double (below 2^53 it is an integer, above it
+// t 2^P already is one), and likewise b'_kj with 2^-sh_k / 2^f_j.  For
+// pairwise coprime moduli m_1..m_n <= 256 with product Mp > 2 K 2^(2P), the
+// exact C' = A'B' is fixed by its residues C' mod m_l = (A' mod m_l)
+// (B' mod m_l) mod m_l: ONE int8 GEMM per modulus on symmetric residues in
+// [-128, 127] (exact int32 accumulation for K < 2^17), against the S(S+1)/2
+// slice products of scheme I.  C' is rebuilt from the residue bytes in
+// double arithmetic (oz2_reconstruct_kernel) and scaled back by 2^(e_i +
+// f_j - 2P).
+struct Oz2Consts {
+    int n, P;
+    int m[24];
+    double inv_m[24];
+    double W[24][4];  // Mp / m_l in base-2^40 digits (W[l][0] least significant)
+    double Mc[4];     // Mp in base-2^40 digits
+    double M_d;       // Mp rounded to double
+};
+
+// Symmetric residue of the integer-valued double x (|x| <= 2^61) modulo m:
+// q = rint(x / m) is off by at most one, r = x - q m is exact (fma), and at
+// most two corrections bring r into [-(m/2), m - 1 - (m/2)].
+__device__ __forceinline__ int8_t oz2_residue(double x, int m, double inv_m) {
+    const double q = rint(x * inv_m);
+    int r = static_cast<int>(fma(-q, static_cast<double>(m), x));
+    const int lo = -(m / 2), hi = lo + m - 1;
+    r += r < lo ? m : 0;
+    r += r < lo ? m : 0;
+    r -= r > hi ? m : 0;
+    r -= r > hi ? m : 0;
+    return static_cast<int8_t>(r);
+}
+
+// A residue planes: A_all[i, l*Kp + k] = a'_ik mod m_l (complex A embedded
+// as [Ar | Ai], width 2K; columns past the width are zero).
+__global__ void oz2_residue_a_kernel(const double* __restrict__ A, long long M, long long K,
+                                     long long lda, int cplx, const int* __restrict__ shift,
+                                     const double* __restrict__ scale, int8_t* __restrict__ out,
+                                     long long Kp, const __grid_constant__ Oz2Consts c) {
+    const long long W = cplx ? 2 * K : K;
+    const long long total = M * Kp;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long i = e / Kp, k = e - i * Kp;
+        double x = 0.0;
+        if (k < W) {
+            if (cplx) {
+                const long long kk = k < K ? k : k - K;
+                x = ldexp(A[2 * (i * lda + kk) + (k < K ? 0 : 1)], shift[kk]);
+            } else {
+                x = ldexp(A[i * lda + k], shift[k]);
+            }
+        }
+        double a = rint(ldexp(x * (1.0 / scale[i]), c.P));
+        if (!isfinite(a)) a = 0.0;  // the row's NaN scale marks its outputs
+        int8_t* o = out + i * (c.n * Kp) + k;
+        for (int l = 0; l < c.n; ++l) o[l * Kp] = oz2_residue(a, c.m[l], c.inv_m[l]);
+    }
+}
+
+// B residue planes: B_all[l*Kp + k, j] = b'_kj mod m_l (complex B embedded
+// as [[Br, Bi], [-Bi, Br]]).
+__global__ void oz2_residue_b_kernel(const double* __restrict__ B, long long K, long long N,
+                                     long long ldb, int cplx, const int* __restrict__ shift,
+                                     const double* __restrict__ scale, int8_t* __restrict__ out,
+                                     long long Kp, long long Np, const __grid_constant__ Oz2Consts c) {
+    const long long H = cplx ? 2 * K : K, Wn = cplx ? 2 * N : N;
+    const long long total = Kp * Np;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long k = e / Np, j = e - k * Np;
+        double x = 0.0, sc = 1.0;
+        if (k < H && j < Wn) {
+            if (cplx) {
+                const bool top = k < K, left = j < N;
+                const long long kk = top ? k : k - K, jj = left ? j : j - N;
+                const double2 v = reinterpret_cast<const double2*>(B)[kk * ldb + jj];
+                x = ldexp(top ? (left ? v.x : v.y) : (left ? -v.y : v.x), -shift[kk]);
+                sc = scale[jj];
+            } else {
+                x = ldexp(B[k * ldb + j], -shift[k]);
+                sc = scale[j];
+            }
+        }
+        double b = rint(ldexp(x * (1.0 / sc), c.P));
+        if (!isfinite(b)) b = 0.0;
+        for (int l = 0; l < c.n; ++l) out[(l * Kp + k) * Np + j] = oz2_residue(b, c.m[l], c.inv_m[l]);
+    }
+}
+
+// C from the residue bytes R[l][i, j] = (C'_ij mod m_l) y_l mod m_l:
+// S = sum_l R_l Mp/m_l is summed exactly in four base-2^40 digit sums
+// (each below 2^53), q = rint(S / Mp) (S / Mp < n, and |C'| < Mp / 4 keeps
+// it far from a tie), C' = S - q Mp digit by digit (exact), the digits are
+// balanced into [-2^39, 2^39) with exact int64 carries and C' is evaluated
+// from the top digit down (relative error about 2^-52).  Then
+// C = alpha 2^(e_i + f_j - 2P) C' (+ beta C).  Complex: embedded column
+// j < N is Re of column j, j >= N Im of column j - N (interleaved C).
+__global__ void oz2_reconstruct_kernel(const uint8_t* __restrict__ R, long long M, long long Nw,
+                                       long long plane, const double* __restrict__ rsc,
+                                       const double* __restrict__ csc, double* __restrict__ C,
+                                       long long ldc, int cplx_half, double alpha, double beta,
+                                       const __grid_constant__ Oz2Consts c) {
+    const long long total = M * Nw;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long i = e / Nw, j = e - i * Nw;
+        double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        for (int l = 0; l < c.n; ++l) {
+            const double r = static_cast<double>(R[l * plane + e]);
+            s0 = fma(r, c.W[l][0], s0);
+            s1 = fma(r, c.W[l][1], s1);
+            s2 = fma(r, c.W[l][2], s2);
+            s3 = fma(r, c.W[l][3], s3);
+        }
+        const double est = ((s3 * 0x1p120 + s2 * 0x1p80) + s1 * 0x1p40) + s0;
+        const double q = rint(est / c.M_d);
+        long long d0 = static_cast<long long>(fma(-q, c.Mc[0], s0));
+        long long d1 = static_cast<long long>(fma(-q, c.Mc[1], s1));
+        long long d2 = static_cast<long long>(fma(-q, c.Mc[2], s2));
+        long long d3 = static_cast<long long>(fma(-q, c.Mc[3], s3));
+        const long long half = 1ll << 39;
+        long long cy = (d0 + half) >> 40;
+        d0 -= cy << 40;
+        d1 += cy;
+        cy = (d1 + half) >> 40;
+        d1 -= cy << 40;
+        d2 += cy;
+        cy = (d2 + half) >> 40;
+        d2 -= cy << 40;
+        d3 += cy;
+        double x = static_cast<double>(d3);
+        x = fma(x, 0x1p40, static_cast<double>(d2));
+        x = fma(x, 0x1p40, static_cast<double>(d1));
+        x = fma(x, 0x1p40, static_cast<double>(d0));
+        const long long jc = cplx_half > 0 ? (j < cplx_half ? j : j - cplx_half) : j;
+        double y = ldexp(x, -2 * c.P) * rsc[i];
+        y = y * csc[jc];
+        double* dst = cplx_half > 0 ? C + 2 * (i * ldc + jc) + (j < cplx_half ? 0 : 1) : C + i * ldc + j;
+        const double o = alpha * y;
+        *dst = beta != 0.0 ? fma(beta, *dst, o) : o;
+    }
+}
+
 }  // namespace fg

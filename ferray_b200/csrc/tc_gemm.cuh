@@ -32,7 +32,7 @@
 namespace fg {
 
 enum : int { KIND_I8 = 0, KIND_BF16 = 1 };
-enum : int { EPI_I32 = 0, EPI_I16 = 1, EPI_F32 = 2, EPI_QMM = 3, EPI_OZAKI = 4 };
+enum : int { EPI_I32 = 0, EPI_I16 = 1, EPI_F32 = 2, EPI_QMM = 3, EPI_OZAKI = 4, EPI_CRT = 5 };
 
 constexpr int TC_MAX_OPS = 8;
 constexpr int TC_MAX_OPERANDS = 4;
@@ -122,6 +122,13 @@ struct TcArgs {
     // oz_w 2^(-7d); only the first group applies oz_beta.  The tile's C block
     // stays in L2 between its groups.
     int oz_groups, oz_d0, oz_kc_blocks, oz_S;
+    // EPI_CRT (Ozaki scheme II): group gi is the product of residue planes gi
+    // (A K blocks [gi oz_kc_blocks, (gi + 1) oz_kc_blocks), B rows the same),
+    // written as the byte ((acc mod m) y) mod m, m = crt_m[gi], y = crt_y[gi],
+    // into plane gi of C (planes crt_plane bytes apart, row pitch ldc).
+    int oz_crt;
+    int crt_m[24], crt_y[24];
+    long long crt_plane;
     TcOp ops[TC_MAX_OPS];
     DevStatus* status;
     unsigned long long timeout_ns;
@@ -166,7 +173,11 @@ __device__ __forceinline__ void unit_coords(const TcArgs& p, int t, int& zo, int
 // Without fused Ozaki groups a tile has one sub-unit, the given range.
 __device__ __forceinline__ void group_range(const TcArgs& p, int gi, int kb0, int kb1, int& g0, int& g1,
                                             int& b_koff) {
-    if (p.oz_groups > 0) {
+    if (p.oz_crt) {
+        g0 = gi * p.oz_kc_blocks;
+        g1 = g0 + p.oz_kc_blocks;
+        b_koff = 0;
+    } else if (p.oz_groups > 0) {
         const int d = p.oz_d0 - gi;
         g0 = 0;
         g1 = (d - 1) * p.oz_kc_blocks;
@@ -282,6 +293,28 @@ __device__ __forceinline__ void epilogue_store(const TcArgs& p, int bz, int grow
 #pragma unroll
             for (int j = 0; j < 32; ++j)
                 if (j < ncols) crow[j] = out[j];
+        }
+    } else if constexpr (Cfg::EPI == EPI_CRT) {
+        // exact int32 product of two residue planes -> its CRT residue byte
+        const int m = p.crt_m[oz_grp], y = p.crt_y[oz_grp];
+        uint8_t* crow = static_cast<uint8_t*>(p.C) + oz_grp * p.crt_plane + (long long)grow * p.ldc + gcol0;
+        uint32_t pk[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) pk[q] = 0;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            int r = static_cast<int32_t>(v[0][j]) % m;
+            r += r < 0 ? m : 0;
+            r = (r * y) % m;
+            pk[j / 4] |= static_cast<uint32_t>(r) << (8 * (j % 4));
+        }
+        if (ncols == 32 && (reinterpret_cast<uintptr_t>(crow) & 15) == 0) {
+            *reinterpret_cast<uint4*>(crow) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+            *reinterpret_cast<uint4*>(crow + 16) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+                if (j < ncols) crow[j] = static_cast<uint8_t>(pk[j / 4] >> (8 * (j % 4)));
         }
     } else if constexpr (Cfg::EPI == EPI_OZAKI) {
         double* cbase = static_cast<double*>(p.C) + bz * p.strideC;

@@ -259,12 +259,13 @@ fg_status fg_host_unregister(fg_ctx *ctx, void *host);
 
 /* ------------------------------------------------------------ raw GEMMs */
 /* C = alpha*A@B + beta*C, f64.  Replaces gemm_f64 (gemm/mod.rs:197-328).
- * mode SPLIT = Ozaki INT8 with `ozaki_slices` slices (0 = default 9, range 3..10). */
+ * mode SPLIT = Ozaki INT8: `ozaki_slices` 3..10 = scheme I digit slices,
+ * 12..20 = scheme II moduli, 0 = scheme II with 16 moduli (see fg_gemm). */
 fg_status fg_gemm_f64(fg_ctx *ctx, fg_mode mode, int ozaki_slices, size_t m, size_t n,
                       size_t k, double alpha, const double *a, const double *b, double beta,
                       double *c, fg_stream stream);
 /* C = alpha*A@B + beta*C, f32.  Replaces gemm_f32 (gemm/mod.rs:940-1062).
- * mode SPLIT = 3 x BF16 on tcgen05. */
+ * mode SPLIT = 3 x BF16 on tcgen05; SPLIT_F16 = 3 x FP16 of scaled operands. */
 fg_status fg_gemm_f32(fg_ctx *ctx, fg_mode mode, size_t m, size_t n, size_t k, float alpha,
                       const float *a, const float *b, float beta, float *c, fg_stream stream);
 /* Complex<f64>.  Replaces gemm_c64 (gemm/mod.rs:757-826). */
@@ -319,7 +320,11 @@ fg_status fg_quantized_matmul_noalloc(fg_ctx *ctx, size_t m, size_t n, size_t k,
 
 /* Generic strided form of all of the above (the reference's internal
  * drivers take lda/ldb/ldc: gemm/outer.rs:198-210).  `ozaki_slices` in split
- * mode: f64/c64, Ozaki INT8 slices (0 = 9); f32/c32, BF16 slices per operand,
+ * mode: f64/c64, 3..10 = Ozaki scheme I with that many INT8 digit slices per
+ * operand (S(S+1)/2 slice products), 12..20 = Ozaki scheme II with that
+ * many moduli (one INT8 product per modulus, Chinese-remainder
+ * reconstruction; K up to 130944, longer K runs scheme I with 9 slices),
+ * 0 = scheme II with 16 moduli; f32/c32, BF16 slices per operand,
  * 2 (three products, the default for 0) or 3 (six products, exact slicing of
  * f32, for FP32-level accuracy at half the speed).  alpha/beta point to a
  * scalar of the dtype's real type (two for complex: re, im); integer dtypes

@@ -1,5 +1,6 @@
 """GPU tests of the split (INT8 Ozaki) DGEMM / ZGEMM against the
-double-double oracle.
+double-double oracle: the default form (scheme II, 16 moduli; its own
+file covers other moduli counts) and scheme I with explicit slice counts.
 
 Tolerances (normwise ||C - C_ref||_F / (||A||_F ||B||_F)):
 * default (9 slices), every case: K * 2^-53, the deterministic bound a plain
@@ -41,13 +42,14 @@ def test_f64_split_bound(fg, oracle, m, n, k):
     assert err <= k * U64 + 11 * 2.0 ** (2 - 63), err
 
 
+@pytest.mark.parametrize("slices", [0, 9])
 @pytest.mark.parametrize("spread", [0, 4, 8])
-def test_f64_split_vs_plain_per_spread(fg, oracle, spread):
+def test_f64_split_vs_plain_per_spread(fg, oracle, spread, slices):
     rng = np.random.default_rng(100 + spread)
     m = n = k = 768
     a, b = spread_operands(rng, m, k, n, spread)
     cs, cp = np.zeros((m, n)), np.zeros((m, n))
-    assert fg.gemm_f64(m, n, k, 1.0, a, b, 0.0, cs, mode="split")
+    assert fg.gemm_f64(m, n, k, 1.0, a, b, 0.0, cs, mode="split", ozaki_slices=slices)
     assert fg.gemm_f64(m, n, k, 1.0, a, b, 0.0, cp, mode="plain")
     es = oracle.error_vs_dd(a, b, cs)
     ep = oracle.error_vs_dd(a, b, cp)
@@ -117,9 +119,10 @@ def test_split_matmul_batched_f64(fg):
 
 @pytest.mark.parametrize("m,n,k,cplx", [(64, 48, 15000, False), (40, 24, 7600, True)])
 def test_split_long_k_group_pieces(fg, oracle, m, n, k, cplx):
-    # 9 slices: the top slice group's concatenated K (9 x K, x2 embedded for
-    # complex) exceeds what one int32 accumulator holds exactly, so that group
-    # runs as several launches; the result keeps the default-slice bound.
+    # scheme I, 9 slices: the top slice group's concatenated K (9 x K, x2
+    # embedded for complex) exceeds what one int32 accumulator holds exactly,
+    # so that group runs as several launches; the result keeps the 9-slice
+    # bound.
     rng = np.random.default_rng(k)
     a = rng.uniform(-1, 1, (m, k))
     b = rng.uniform(-1, 1, (k, n))
@@ -127,10 +130,10 @@ def test_split_long_k_group_pieces(fg, oracle, m, n, k, cplx):
         a = a + 1j * rng.uniform(-1, 1, (m, k))
         b = b + 1j * rng.uniform(-1, 1, (k, n))
         c = np.zeros((m, n), np.complex128)
-        assert fg.gemm_c64(m, n, k, 1.0, 0.0, a, b, 0.0, 0.0, c, mode="split")
+        assert fg.gemm_c64(m, n, k, 1.0, 0.0, a, b, 0.0, 0.0, c, mode="split", ozaki_slices=9)
     else:
         c = np.zeros((m, n))
-        assert fg.gemm_f64(m, n, k, 1.0, a, b, 0.0, c, mode="split")
+        assert fg.gemm_f64(m, n, k, 1.0, a, b, 0.0, c, mode="split", ozaki_slices=9)
     err = oracle.error_vs_dd(a, b, c)
     assert err <= (2 if cplx else 1) * k * U64 + 11 * 2.0 ** (2 - 63), err
 
@@ -144,19 +147,23 @@ a, b, cplx = d["a"], d["b"], bool(d["cplx"])
 m, k = a.shape
 n = b.shape[1]
 c = np.zeros((m, n), a.dtype)
+sl = int(d["slices"])
 if cplx:
-    assert fg.gemm_c64(m, n, k, 1.5, 0.0, a, b, 0.0, 0.0, c, mode="split")
+    assert fg.gemm_c64(m, n, k, 1.5, 0.0, a, b, 0.0, 0.0, c, mode="split", ozaki_slices=sl)
 else:
-    assert fg.gemm_f64(m, n, k, 1.5, a, b, 0.0, c, mode="split")
+    assert fg.gemm_f64(m, n, k, 1.5, a, b, 0.0, c, mode="split", ozaki_slices=sl)
 np.save(sys.argv[3], c)
 """
 
 
+@pytest.mark.parametrize("slices", [9, 16])
 @pytest.mark.parametrize("m,n,k,cplx", [(300, 257, 129, False), (513, 1000, 700, False), (200, 150, 300, True)])
-def test_fused_groups_bit_identical_to_group_launches(fg, tmp_path, m, n, k, cplx):
-    """All slice groups in one launch (the default) give the same bits as
-    one launch per group (FG_OZAKI_FUSED=0, run in a child process): the
-    FP64 epilogue adds the groups to C in the same order either way."""
+def test_fused_groups_bit_identical_to_group_launches(fg, tmp_path, m, n, k, cplx, slices):
+    """All slice groups (scheme I) or all moduli (scheme II) in one launch,
+    the default, give the same bits as one launch per group / modulus
+    (FG_OZAKI_FUSED=0, run in a child process): scheme I's FP64 epilogue adds
+    the groups to C in the same order either way, and scheme II's residue
+    bytes do not depend on the launch."""
     import os
     import subprocess
     import sys
@@ -168,10 +175,10 @@ def test_fused_groups_bit_identical_to_group_launches(fg, tmp_path, m, n, k, cpl
         b = b + 1j * r.standard_normal((k, n))
     c = np.zeros((m, n), a.dtype)
     if cplx:
-        assert fg.gemm_c64(m, n, k, 1.5, 0.0, a, b, 0.0, 0.0, c, mode="split")
+        assert fg.gemm_c64(m, n, k, 1.5, 0.0, a, b, 0.0, 0.0, c, mode="split", ozaki_slices=slices)
     else:
-        assert fg.gemm_f64(m, n, k, 1.5, a, b, 0.0, c, mode="split")
-    np.savez(tmp_path / "in.npz", a=a, b=b, cplx=cplx)
+        assert fg.gemm_f64(m, n, k, 1.5, a, b, 0.0, c, mode="split", ozaki_slices=slices)
+    np.savez(tmp_path / "in.npz", a=a, b=b, cplx=cplx, slices=slices)
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     env = dict(os.environ, FG_OZAKI_FUSED="0")
     subprocess.run([sys.executable, "-c", _PER_GROUP_SCRIPT, root, str(tmp_path / "in.npz"),
