@@ -217,10 +217,14 @@ static Oz2Consts oz2_consts(int n, long long K) {
         W.divmod(static_cast<uint32_t>(m));  // exact: Mp / m_l
         c.m[l] = m;
         c.inv_m[l] = 1.0 / m;
+        c.magic[l] = static_cast<uint32_t>(((1ull << 32) + m - 1) / m);
+        c.c20[l] = static_cast<uint32_t>((1ull << 20) % m);
+        c.c40[l] = static_cast<uint32_t>((1ull << 40) % m);
         for (int d = 0; d < 4; ++d) c.W[l][d] = static_cast<double>(W.bits_at(40 * d, 40));
     }
     for (int d = 0; d < 4; ++d) c.Mc[d] = static_cast<double>(Mp.bits_at(40 * d, 40));
     c.M_d = Mp.to_double();
+    c.inv_M = 1.0 / c.M_d;
     return c;
 }
 
@@ -261,13 +265,16 @@ static fg_status launch_ozaki2(fg_ctx* ctx, const Gemm& g, int n, cudaStream_t s
     FG_TRY(scale_operands(g, cplx, rsc, csc, cmax, kmax_a, kmax_b, shift, st));
     const double* A = static_cast<const double*>(g.A);
     const double* B = static_cast<const double*>(g.B);
-    oz2_residue_a_kernel<<<grid_for(M * Kp), 256, 0, st>>>(A, M, g.K, g.lda, cplx ? 1 : 0, shift, rsc, a_all, Kp, c);
-    oz2_residue_b_kernel<<<grid_for(Kp * Np), 256, 0, st>>>(B, g.K, g.N, g.ldb, cplx ? 1 : 0, shift, csc, b_all, Kp, Np, c);
+    oz2_residue_a_kernel<<<grid_for(M * Kp / 8), 256, 0, st>>>(A, M, g.K, g.lda, cplx ? 1 : 0, shift, rsc, a_all, Kp, c);
+    oz2_residue_b_kernel<<<grid_for(Kp * Np / 8), 256, 0, st>>>(B, g.K, g.N, g.ldb, cplx ? 1 : 0, shift, csc, b_all, Kp, Np, c);
     count_launch(2);
     FG_CUDA(cudaGetLastError());
 
     const bool pair = tune_lookup(TUNE_I8, M, Nw, Kp).variant == 2;
-    const bool fused = fused_groups();
+    // one launch for all moduli up to about 24 M outputs; beyond, one launch
+    // per modulus keeps the CTAs' K positions in step for L2 reuse
+    // (DGEMM 8192: 9.9 ms against 11.2 ms fused)
+    const bool fused = fused_groups() && M * Nw <= (24ll << 20);
     const int launches = fused ? 1 : n;
     for (int L = 0; L < launches; ++L) {
         TcMaps maps;

@@ -273,6 +273,9 @@ struct Oz2Consts {
     int n, P;
     int m[24];
     double inv_m[24];
+    uint32_t magic[24];         // ceil(2^32 / m_l)
+    uint32_t c20[24], c40[24];  // 2^20 mod m_l, 2^40 mod m_l
+    double inv_M;               // 1 / Mp, for the CRT quotient
     double W[24][4];  // Mp / m_l in base-2^40 digits (W[l][0] least significant)
     double Mc[4];     // Mp in base-2^40 digits
     double M_d;       // Mp rounded to double
@@ -292,60 +295,114 @@ __device__ __forceinline__ int8_t oz2_residue(double x, int m, double inv_m) {
     return static_cast<int8_t>(r);
 }
 
+// An integer-valued double |a| <= 2^60 as a sign and three 20-bit limbs
+// (integer arithmetic from here on: one conversion per element, not one per
+// modulus).
+struct Oz2Limbs {
+    uint32_t u0, u1, u2;
+    bool neg;
+};
+
+__device__ __forceinline__ Oz2Limbs oz2_limbs(double a) {
+    const long long v = static_cast<long long>(a);  // exact: a is an integer
+    const unsigned long long u = static_cast<unsigned long long>(v < 0 ? -v : v);
+    return Oz2Limbs{static_cast<uint32_t>(u & 0xFFFFFu), static_cast<uint32_t>((u >> 20) & 0xFFFFFu),
+                    static_cast<uint32_t>(u >> 40), v < 0};
+}
+
+// Symmetric residue of the limbs' integer modulo m: x = u2 (2^40 mod m) +
+// u1 (2^20 mod m) + u0 < 2^30, x mod m by a multiply-high with
+// ceil(2^32 / m) (quotient exact or one too large) and one correction, then
+// the sign and the symmetric range [-(m/2), m - 1 - (m/2)].
+__device__ __forceinline__ uint32_t oz2_residue_limbs(const Oz2Limbs& a, uint32_t m, uint32_t magic,
+                                                      uint32_t c20, uint32_t c40) {
+    const uint32_t x = a.u2 * c40 + a.u1 * c20 + a.u0;
+    int r = static_cast<int>(x - __umulhi(x, magic) * m);
+    r += r < 0 ? static_cast<int>(m) : 0;  // r in [0, m)
+    if (a.neg) r = r ? static_cast<int>(m) - r : 0;
+    const int hi = static_cast<int>(m) - 1 - static_cast<int>(m / 2);
+    r -= r > hi ? static_cast<int>(m) : 0;
+    return static_cast<uint32_t>(r) & 0xFFu;
+}
+
+// Eight consecutive residues of one plane packed into 8 bytes.
+__device__ __forceinline__ uint2 oz2_pack8(const Oz2Limbs (&x)[8], const Oz2Consts& c, int l) {
+    const uint32_t m = static_cast<uint32_t>(c.m[l]), magic = c.magic[l], c20 = c.c20[l], c40 = c.c40[l];
+    uint32_t w[2] = {0u, 0u};
+#pragma unroll
+    for (int u = 0; u < 8; ++u) w[u / 4] |= oz2_residue_limbs(x[u], m, magic, c20, c40) << (8 * (u % 4));
+    return make_uint2(w[0], w[1]);
+}
+
 // A residue planes: A_all[i, l*Kp + k] = a'_ik mod m_l (complex A embedded
-// as [Ar | Ai], width 2K; columns past the width are zero).
+// as [Ar | Ai], width 2K; columns past the width are zero).  A thread takes
+// eight consecutive k of one row and writes 8 bytes per plane.
 __global__ void oz2_residue_a_kernel(const double* __restrict__ A, long long M, long long K,
                                      long long lda, int cplx, const int* __restrict__ shift,
                                      const double* __restrict__ scale, int8_t* __restrict__ out,
                                      long long Kp, const __grid_constant__ Oz2Consts c) {
     const long long W = cplx ? 2 * K : K;
-    const long long total = M * Kp;
+    const long long K8 = Kp / 8, total = M * K8;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
          e += (long long)gridDim.x * blockDim.x) {
-        const long long i = e / Kp, k = e - i * Kp;
-        double x = 0.0;
-        if (k < W) {
-            if (cplx) {
-                const long long kk = k < K ? k : k - K;
-                x = ldexp(A[2 * (i * lda + kk) + (k < K ? 0 : 1)], shift[kk]);
-            } else {
-                x = ldexp(A[i * lda + k], shift[k]);
+        const long long i = e / K8, k0 = (e - i * K8) * 8;
+        const double inv = 1.0 / scale[i];
+        Oz2Limbs a[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const long long k = k0 + u;
+            double x = 0.0;
+            if (k < W) {
+                if (cplx) {
+                    const long long kk = k < K ? k : k - K;
+                    x = ldexp(A[2 * (i * lda + kk) + (k < K ? 0 : 1)], shift[kk]);
+                } else {
+                    x = ldexp(A[i * lda + k], shift[k]);
+                }
             }
+            double v = rint(ldexp(x * inv, c.P));
+            if (!isfinite(v)) v = 0.0;  // the row's NaN scale marks its outputs
+            a[u] = oz2_limbs(v);
         }
-        double a = rint(ldexp(x * (1.0 / scale[i]), c.P));
-        if (!isfinite(a)) a = 0.0;  // the row's NaN scale marks its outputs
-        int8_t* o = out + i * (c.n * Kp) + k;
-        for (int l = 0; l < c.n; ++l) o[l * Kp] = oz2_residue(a, c.m[l], c.inv_m[l]);
+        int8_t* o = out + i * (c.n * Kp) + k0;
+        for (int l = 0; l < c.n; ++l) *reinterpret_cast<uint2*>(o + l * Kp) = oz2_pack8(a, c, l);
     }
 }
 
 // B residue planes: B_all[l*Kp + k, j] = b'_kj mod m_l (complex B embedded
-// as [[Br, Bi], [-Bi, Br]]).
+// as [[Br, Bi], [-Bi, Br]]).  A thread takes eight consecutive j of one row.
 __global__ void oz2_residue_b_kernel(const double* __restrict__ B, long long K, long long N,
                                      long long ldb, int cplx, const int* __restrict__ shift,
                                      const double* __restrict__ scale, int8_t* __restrict__ out,
                                      long long Kp, long long Np, const __grid_constant__ Oz2Consts c) {
     const long long H = cplx ? 2 * K : K, Wn = cplx ? 2 * N : N;
-    const long long total = Kp * Np;
+    const long long N8 = Np / 8, total = Kp * N8;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
          e += (long long)gridDim.x * blockDim.x) {
-        const long long k = e / Np, j = e - k * Np;
-        double x = 0.0, sc = 1.0;
-        if (k < H && j < Wn) {
-            if (cplx) {
-                const bool top = k < K, left = j < N;
-                const long long kk = top ? k : k - K, jj = left ? j : j - N;
-                const double2 v = reinterpret_cast<const double2*>(B)[kk * ldb + jj];
-                x = ldexp(top ? (left ? v.x : v.y) : (left ? -v.y : v.x), -shift[kk]);
-                sc = scale[jj];
-            } else {
-                x = ldexp(B[k * ldb + j], -shift[k]);
-                sc = scale[j];
+        const long long k = e / N8, j0 = (e - k * N8) * 8;
+        Oz2Limbs b[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const long long j = j0 + u;
+            double x = 0.0, sc = 1.0;
+            if (k < H && j < Wn) {
+                if (cplx) {
+                    const bool top = k < K, left = j < N;
+                    const long long kk = top ? k : k - K, jj = left ? j : j - N;
+                    const double2 v = reinterpret_cast<const double2*>(B)[kk * ldb + jj];
+                    x = ldexp(top ? (left ? v.x : v.y) : (left ? -v.y : v.x), -shift[kk]);
+                    sc = scale[jj];
+                } else {
+                    x = ldexp(B[k * ldb + j], -shift[k]);
+                    sc = scale[j];
+                }
             }
+            double v = rint(ldexp(x * (1.0 / sc), c.P));
+            if (!isfinite(v)) v = 0.0;
+            b[u] = oz2_limbs(v);
         }
-        double b = rint(ldexp(x * (1.0 / sc), c.P));
-        if (!isfinite(b)) b = 0.0;
-        for (int l = 0; l < c.n; ++l) out[(l * Kp + k) * Np + j] = oz2_residue(b, c.m[l], c.inv_m[l]);
+        for (int l = 0; l < c.n; ++l)
+            *reinterpret_cast<uint2*>(out + (l * Kp + k) * Np + j0) = oz2_pack8(b, c, l);
     }
 }
 
@@ -357,6 +414,34 @@ __global__ void oz2_residue_b_kernel(const double* __restrict__ B, long long K, 
 // from the top digit down (relative error about 2^-52).  Then
 // C = alpha 2^(e_i + f_j - 2P) C' (+ beta C).  Complex: embedded column
 // j < N is Re of column j, j >= N Im of column j - N (interleaved C).
+__device__ __forceinline__ double oz2_rebuild(double s0, double s1, double s2, double s3,
+                                              const Oz2Consts& c) {
+    const double est = ((s3 * 0x1p120 + s2 * 0x1p80) + s1 * 0x1p40) + s0;
+    const double q = rint(est * c.inv_M);
+    long long d0 = static_cast<long long>(fma(-q, c.Mc[0], s0));
+    long long d1 = static_cast<long long>(fma(-q, c.Mc[1], s1));
+    long long d2 = static_cast<long long>(fma(-q, c.Mc[2], s2));
+    long long d3 = static_cast<long long>(fma(-q, c.Mc[3], s3));
+    const long long half = 1ll << 39;
+    long long cy = (d0 + half) >> 40;
+    d0 -= cy << 40;
+    d1 += cy;
+    cy = (d1 + half) >> 40;
+    d1 -= cy << 40;
+    d2 += cy;
+    cy = (d2 + half) >> 40;
+    d2 -= cy << 40;
+    d3 += cy;
+    double x = static_cast<double>(d3);
+    x = fma(x, 0x1p40, static_cast<double>(d2));
+    x = fma(x, 0x1p40, static_cast<double>(d1));
+    return fma(x, 0x1p40, static_cast<double>(d0));
+}
+
+// One thread per output (measured faster than 4 or 8 outputs a thread:
+// the digit sums are FP64-bound and fewer registers keep more warps
+// resident).  A residue byte r becomes the double r by the exact
+// 2^52 + r - 2^52 bit trick.
 __global__ void oz2_reconstruct_kernel(const uint8_t* __restrict__ R, long long M, long long Nw,
                                        long long plane, const double* __restrict__ rsc,
                                        const double* __restrict__ csc, double* __restrict__ C,
@@ -368,37 +453,16 @@ __global__ void oz2_reconstruct_kernel(const uint8_t* __restrict__ R, long long 
         const long long i = e / Nw, j = e - i * Nw;
         double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
         for (int l = 0; l < c.n; ++l) {
-            const double r = static_cast<double>(R[l * plane + e]);
+            const double r = __hiloint2double(0x43300000, R[l * plane + e]) - 0x1p52;
             s0 = fma(r, c.W[l][0], s0);
             s1 = fma(r, c.W[l][1], s1);
             s2 = fma(r, c.W[l][2], s2);
             s3 = fma(r, c.W[l][3], s3);
         }
-        const double est = ((s3 * 0x1p120 + s2 * 0x1p80) + s1 * 0x1p40) + s0;
-        const double q = rint(est / c.M_d);
-        long long d0 = static_cast<long long>(fma(-q, c.Mc[0], s0));
-        long long d1 = static_cast<long long>(fma(-q, c.Mc[1], s1));
-        long long d2 = static_cast<long long>(fma(-q, c.Mc[2], s2));
-        long long d3 = static_cast<long long>(fma(-q, c.Mc[3], s3));
-        const long long half = 1ll << 39;
-        long long cy = (d0 + half) >> 40;
-        d0 -= cy << 40;
-        d1 += cy;
-        cy = (d1 + half) >> 40;
-        d1 -= cy << 40;
-        d2 += cy;
-        cy = (d2 + half) >> 40;
-        d2 -= cy << 40;
-        d3 += cy;
-        double x = static_cast<double>(d3);
-        x = fma(x, 0x1p40, static_cast<double>(d2));
-        x = fma(x, 0x1p40, static_cast<double>(d1));
-        x = fma(x, 0x1p40, static_cast<double>(d0));
+        const double x = oz2_rebuild(s0, s1, s2, s3, c);
         const long long jc = cplx_half > 0 ? (j < cplx_half ? j : j - cplx_half) : j;
-        double y = ldexp(x, -2 * c.P) * rsc[i];
-        y = y * csc[jc];
+        const double o = (x * (ldexp(rsc[i], -2 * c.P) * alpha)) * csc[jc];
         double* dst = cplx_half > 0 ? C + 2 * (i * ldc + jc) + (j < cplx_half ? 0 : 1) : C + i * ldc + j;
-        const double o = alpha * y;
         *dst = beta != 0.0 ? fma(beta, *dst, o) : o;
     }
 }
