@@ -57,7 +57,8 @@ def parse():
     ap.add_argument("--peaks", action="store_true",
                     help="measure library reference rates (cuBLAS via torch) for INT8, FP64, FP32")
     ap.add_argument("--side", default="",
-                    help="run one side measurement only: dgemm, i8, ragged, int, half, skinny, trsm, serving or ozaki")
+                    help="run one side measurement only: peaks, dgemm, sweep, cgemm, i8, ozaki, ozaki_all, "
+                         "split_f64, ragged, int, half, skinny, trsm or serving")
     return ap.parse_args()
 
 
@@ -300,6 +301,20 @@ def side_measurements(fg, L, lib, ctx, stream, n, only=""):
         res["i8_square"] = bc.i8_square(R, int8_peak=int8_peak)
     if not only or only == "ozaki":
         res["ozaki_f64_c128"] = bc.ozaki_sweep(R)
+    if only == "split_f64":
+        # one size: the default split DGEMM (Ozaki scheme II, 16 moduli) vs
+        # plain at N = n, N(0, 1) operands generated on the device
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(SEED)
+        a = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=gen)
+        b = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=gen)
+        c = torch.empty_like(a)
+        d = {}
+        for name, mode in (("plain", L.FG_MODE_PLAIN), ("split", L.FG_MODE_SPLIT)):
+            ms = R.time(R.gemm(L.FG_F64, mode, 0, n, n, n, a.data_ptr(), b.data_ptr(), c.data_ptr()), min_ms=10.0)
+            d[name] = {"tflops": round(2.0 * n ** 3 / ms / 1e9, 2), "ms": round(ms, 4)}
+        res["split_f64_%d" % n] = d
+        del a, b, c
     if only == "ozaki_all":
         res["ozaki_sweep_all_slices"] = bc.ozaki_sweep(R, slices=(6, 7, 8, 9, 12, 14, 16, 17, 18, 20), cpu=False)
     if not only or only == "ragged":
