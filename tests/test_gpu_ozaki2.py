@@ -4,7 +4,7 @@ the product rebuilt by the Chinese remainder theorem) against the
 double-double oracle.
 
 The integer operands carry P bits below each balanced row / column maximum,
-P = min(59, floor((log2 Mp - ceil(log2 K) - 3) / 2)) for the moduli product
+P = min(59, floor((floor(log2 Mp) - ceil(log2 K) - 2) / 2)) for the moduli product
 Mp; entries within 2^(53 - P) of their row maximum are exact.  Tolerances
 (normwise ||C - C_ref||_F / (||A||_F ||B||_F)):
 * 16 or more moduli (P >= 55 up to K = 8192): no worse than 2x the plain
