@@ -58,7 +58,7 @@ def parse():
                     help="measure library reference rates (cuBLAS via torch) for INT8, FP64, FP32")
     ap.add_argument("--side", default="",
                     help="run one side measurement only: peaks, dgemm, sweep, cgemm, i8, ozaki, ozaki_all, "
-                         "split_f64, ragged, int, half, skinny, trsm or serving")
+                         "split_f64, ragged, ragged_i8, int, half, skinny, trsm or serving")
     return ap.parse_args()
 
 
@@ -317,6 +317,23 @@ def side_measurements(fg, L, lib, ctx, stream, n, only=""):
         del a, b, c
     if only == "ozaki_all":
         res["ozaki_sweep_all_slices"] = bc.ozaki_sweep(R, slices=(6, 7, 8, 9, 12, 14, 16, 17, 18, 20), cpu=False)
+    if only == "ragged_i8":
+        # the i8 ragged batch alone: one grouped plan replayed (profiling)
+        dims = ragged_dims()
+        bufs, tab = [], (L.fg_problem * len(dims))()
+        for i, (m, nn, k) in enumerate(dims):
+            ta = torch.randint(-100, 100, (int(m * k),), dtype=torch.int8, device="cuda")
+            tb = torch.randint(-100, 100, (int(k * nn),), dtype=torch.int8, device="cuda")
+            tc = torch.zeros(int(m * nn), dtype=torch.int32, device="cuda")
+            bufs.append((ta, tb, tc))
+            tab[i] = L.fg_problem(int(m), int(nn), int(k), ta.data_ptr(), tb.data_ptr(), tc.data_ptr(),
+                                  int(k), int(nn), int(nn))
+        h = C.c_void_p()
+        assert lib.fg_grouped_plan_create(ctx.handle, L.FG_I8, 0, tab, len(dims), sh, C.byref(h)) == 0
+        ms = _time_calls(torch, stream, lambda: lib.fg_grouped_plan_run(h, sh), 5, 2)
+        lib.fg_grouped_plan_destroy(h)
+        res["ragged_i8"] = {"grouped_ms": round(ms, 4)}
+        del bufs
     if not only or only == "ragged":
         # --- ragged grouped batch, 4096 problems, dims log-uniform in [8, 512]
         dims = ragged_dims()

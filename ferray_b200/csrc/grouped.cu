@@ -234,7 +234,7 @@ fg_status grouped_job_bind(GroupedJob* j, void* dev_base, void* host_stage) {
     for (int x : order) {
         const GroupedProblem& g = j->probs[x];
         for (int tm = 0; tm < g.tiles_m; ++tm)
-            for (int tn = 0; tn < g.tiles_n; ++tn) htiles[t++] = TileRec{x, tm, tn, 0};
+            for (int tn = 0; tn < g.tiles_n; ++tn) htiles[t++] = TileRec{x, tm, tn, g.k_blocks};
     }
     const TileRec* dtiles = reinterpret_cast<const TileRec*>(dbase + o_tiles);
     CUtensorMap* hmaps = reinterpret_cast<CUtensorMap*>(hbase + o_maps);

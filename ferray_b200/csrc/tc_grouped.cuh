@@ -29,10 +29,12 @@ struct GroupedProblem {
     int tile;              // plain FP32 batches: square tile edge, 64 or 32
 };
 
-// Per global tile: problem index, tile row, tile column (written by the host
-// with the problem table, so a tile costs one load instead of a search).
+// Per global tile: problem index, tile row, tile column and the problem's K
+// blocks (written by the host with the problem table, so a tile costs one
+// 16-byte load instead of a search; the producer and the MMA issuer need
+// nothing else).
 struct TileRec {
-    int problem, tm, tn, pad;
+    int problem, tm, tn, kb;
 };
 
 struct GroupedArgs {
@@ -64,19 +66,36 @@ __device__ __forceinline__ void grouped_store(const GroupedArgs& g, const Groupe
     const int col = col0 + lane;
     const int rows = min(32, pr.M - row0);
     if (col < pr.N) {
-        for (int r = 0; r < rows; ++r) {
-            const long long off = (long long)(row0 + r) * pr.ldc + col;
-            if constexpr (Cfg::EPI == EPI_I32) {
-                int32_t* p = static_cast<int32_t*>(pr.C) + off;
-                uint32_t w = stg[r][lane];
-                if (g.accumulate) w += static_cast<uint32_t>(*p);
-                *p = static_cast<int32_t>(w);
-            } else {
-                float* p = static_cast<float*>(pr.C) + off;
-                float o = g.alpha * __uint_as_float(stg[r][lane]);
-                if (g.beta != 0.f) o = fmaf(g.beta, *p, o);
-                *p = o;
+        // unrolled with predicates: all shared-memory reads (and the reads
+        // of C for accumulate / beta) are issued before the first store, so
+        // they overlap instead of costing one round trip per row
+        uint32_t w[32];
+#pragma unroll
+        for (int r = 0; r < 32; ++r) w[r] = stg[r][lane];
+        const long long ldc = pr.ldc;
+        if constexpr (Cfg::EPI == EPI_I32) {
+            int32_t* p = static_cast<int32_t*>(pr.C) + (long long)row0 * ldc + col;
+            if (g.accumulate) {
+#pragma unroll
+                for (int r = 0; r < 32; ++r)
+                    if (r < rows) w[r] += static_cast<uint32_t>(p[r * ldc]);
             }
+#pragma unroll
+            for (int r = 0; r < 32; ++r)
+                if (r < rows) p[r * ldc] = static_cast<int32_t>(w[r]);
+        } else {
+            float* p = static_cast<float*>(pr.C) + (long long)row0 * ldc + col;
+            float o[32];
+#pragma unroll
+            for (int r = 0; r < 32; ++r) o[r] = g.alpha * __uint_as_float(w[r]);
+            if (g.beta != 0.f) {
+#pragma unroll
+                for (int r = 0; r < 32; ++r)
+                    if (r < rows) o[r] = fmaf(g.beta, p[r * ldc], o[r]);
+            }
+#pragma unroll
+            for (int r = 0; r < 32; ++r)
+                if (r < rows) p[r * ldc] = o[r];
         }
     }
     __syncwarp();
@@ -97,7 +116,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
     // thread and the four epilogue warps read them in order
     constexpr int SLOTS = 16;
     __shared__ uint64_t sched_full[SLOTS], sched_empty[SLOTS];
-    __shared__ long long sched_tile[SLOTS];
+    __shared__ int4 sched_rec[SLOTS];  // the tile's TileRec; problem < 0 ends the walk
 
     if (threadIdx.x == 0) {
         for (int i = 0; i < SLOTS; ++i) {
@@ -135,32 +154,32 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
             bool ok = true;
             int slot = 0;
             uint32_t sph = 0;
-            long long t = static_cast<long long>(atomicAdd(g.tile_counter, 1ull));
+            // Two claims ahead: while the loads of tile t0 are issued, the
+            // record of t1 is already in flight and t2 is being claimed, so
+            // no global round trip sits between two tiles' loads.
+            const long long total = g.total_tiles;
+            const TileRec none{-1, 0, 0, 0};
+            long long t0 = static_cast<long long>(atomicAdd(g.tile_counter, 1ull));
+            long long t1 = t0 < total ? static_cast<long long>(atomicAdd(g.tile_counter, 1ull)) : t0;
+            TileRec r0 = t0 < total ? g.tiles[t0] : none;
             while (ok) {
                 // publish the claimed tile (or the end marker) to the other roles
                 if (!mbar_wait(&sched_empty[slot], sph ^ 1u, g.timeout_ns, g.status, 0x35, abort)) {
                     ok = false;
                     break;
                 }
-                sched_tile[slot] = t;
+                sched_rec[slot] = make_int4(r0.problem, r0.tm, r0.tn, r0.kb);
                 mbar_arrive(&sched_full[slot]);
                 if (++slot == SLOTS) {
                     slot = 0;
                     sph ^= 1u;
                 }
-                if (t >= g.total_tiles) break;
-                const TileRec tr = g.tiles[t];
-                const int pi = tr.problem, tm = tr.tm, tn = tr.tn;
-                const GroupedProblem pr = g.problems[pi];
+                if (t0 >= total) break;
+                const long long t2 = t1 < total ? static_cast<long long>(atomicAdd(g.tile_counter, 1ull)) : t1;
+                const TileRec r1 = t1 < total ? g.tiles[t1] : none;  // used after this tile's loads
+                const int pi = r0.problem, tm = r0.tm, tn = r0.tn;
                 const CUtensorMap* mp = g.maps + (long long)pi * NMAPS;
-                const long long t_next = static_cast<long long>(atomicAdd(g.tile_counter, 1ull));
-                if (t_next < g.total_tiles) {
-                    const int pn = g.tiles[t_next].problem;
-                    if (pn != pi)
-                        for (int i = 0; i < NMAPS; ++i) tma_prefetch_desc(g.maps + (long long)pn * NMAPS + i);
-                }
-                t = t_next;
-                for (int kb = 0; kb < pr.k_blocks; ++kb) {
+                for (int kb = 0; kb < r0.kb; ++kb) {
                     if (!mbar_wait(&s.empty[stage], phase ^ 1u, g.timeout_ns, g.status, 0x31, abort)) {
                         ok = false;
                         break;
@@ -182,6 +201,11 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
                         phase ^= 1u;
                     }
                 }
+                if (r1.problem >= 0 && r1.problem != pi)
+                    for (int i = 0; i < NMAPS; ++i) tma_prefetch_desc(g.maps + (long long)r1.problem * NMAPS + i);
+                t0 = t1;
+                t1 = t2;
+                r0 = r1;
             }
             if (!ok) {
                 for (int i = 0; i < Cfg::STAGES; ++i) {
@@ -204,15 +228,14 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
                     ok = false;
                     break;
                 }
-                const long long t = sched_tile[slot];
+                const int4 rec = sched_rec[slot];
                 mbar_arrive(&sched_empty[slot]);
                 if (++slot == SLOTS) {
                     slot = 0;
                     sph ^= 1u;
                 }
-                if (t >= g.total_tiles) break;
-                const int pi = g.tiles[t].problem;
-                const int kblocks = g.problems[pi].k_blocks;
+                if (rec.x < 0) break;
+                const int kblocks = rec.w;
                 const int kchunk = (Cfg::CHUNKED && g.kchunk > 0) ? g.kchunk : max(kblocks, 1);
                 for (int kc0 = 0; kc0 < max(kblocks, 1) && ok; kc0 += kchunk, ++it) {
                     const int kc1 = min(kblocks, kc0 + kchunk);
@@ -280,18 +303,17 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
                 ok = false;
                 break;
             }
-            const long long t = sched_tile[slot];
+            const int4 rec = sched_rec[slot];
             __syncwarp();
             if (lane == 0) mbar_arrive(&sched_empty[slot]);
             if (++slot == SLOTS) {
                 slot = 0;
                 sph ^= 1u;
             }
-            if (t >= g.total_tiles) break;
-            const TileRec tr = g.tiles[t];
-            const int tm = tr.tm, tn = tr.tn;
-            const GroupedProblem pr = g.problems[tr.problem];
-            const int kblocks = max(pr.k_blocks, 1);
+            if (rec.x < 0) break;
+            const int tm = rec.y, tn = rec.z;
+            const GroupedProblem pr = g.problems[rec.x];
+            const int kblocks = max(rec.w, 1);
             const int kchunk = (Cfg::CHUNKED && g.kchunk > 0) ? g.kchunk : kblocks;
             float run[Cfg::CHUNKED ? Cfg::BN : 1];
             if constexpr (Cfg::CHUNKED) {
