@@ -49,7 +49,11 @@ size_t request_bytes(const fg_request& r) {
         if (r.mode != FG_MODE_PLAIN && (r.dtype == FG_F32 || r.dtype == FG_C32))
             scratch = (r.dtype == FG_C32 ? 4 : 1) * 2 * 2 * (r.m * r.k + r.k * r.n) * 2;
         else if (r.mode != FG_MODE_PLAIN && (r.dtype == FG_F64 || r.dtype == FG_C64))
-            scratch = (r.dtype == FG_C64 ? 4 : 1) * 9 * (r.m * r.k + r.k * r.n + 32 * (r.m + r.n));
+            // default split: Ozaki scheme II with 16 moduli -> 16 int8 residue
+            // planes of A, B and of the result bytes (x4 for the complex
+            // embedding), plus scales
+            scratch = (r.dtype == FG_C64 ? 4 : 1) * 16 * (r.m * r.k + r.k * r.n + r.m * r.n) +
+                      32 * (r.m + r.n + r.k);
         else if (r.dtype == FG_I16)
             scratch = 2 * (r.m * r.k + r.k * r.n) + 64 * (r.m + r.n);
         else if (r.dtype == FG_I8 || r.dtype == FG_U8I8)
