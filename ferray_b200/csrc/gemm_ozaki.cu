@@ -237,7 +237,7 @@ static int oz2_y(int n, int l) {  // ((Mp / m_l) mod m_l)^-1 mod m_l
 }
 
 using CfgCrt = TcCfg<KIND_I8, 256, 4, 1, 1, 1, 1, EPI_CRT>;
-using CfgCrtPair = Tc2Cfg<KIND_I8, 256, 6, 1, 1, 1, 1, EPI_CRT>;
+using CfgCrtPair = Tc2Cfg<KIND_I8, 256, 7, 1, 1, 1, 1, EPI_CRT>;
 
 // Scheme II DGEMM / ZGEMM with n moduli (real GEMM, or the complex real
 // embedding (M x 2K)(2K x 2N) like scheme I).

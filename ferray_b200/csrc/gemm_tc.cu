@@ -25,7 +25,7 @@ using namespace fg;
 using CfgI8 = TcCfg<KIND_I8, 256, 4, 1, 1, 1, 1, EPI_I32>;
 using CfgI8n128 = TcCfg<KIND_I8, 128, 6, 1, 1, 1, 1, EPI_I32>;
 // 256 x 256 tiles on CTA pairs (cta_group::2), 6 stages of 32 KB per CTA.
-using CfgI8Pair = Tc2Cfg<KIND_I8, 256, 6, 1, 1, 1, 1, EPI_I32>;
+using CfgI8Pair = Tc2Cfg<KIND_I8, 256, 7, 1, 1, 1, 1, EPI_I32>;
 // 256 x 512 tiles on CTA pairs: one A tile feeds two N = 256 MMAs into two
 // TMEM accumulators (all 512 columns, single-buffered); 4 stages of 48 KB.
 using CfgI8PairW = Tc2Cfg<KIND_I8, 256, 4, 1, 2, 2, 2, EPI_I32, 0, 1>;
