@@ -399,12 +399,19 @@ def gemm_batched_strided(dtype, batch, m, n, k, a, stride_a, b, stride_b, c, str
     ctx.sync()
 
 
+def _ptr(x):
+    """Device address of a DeviceArray or a raw pointer (int-like or None)."""
+    if _is_dev(x):
+        return x.ptr
+    return None if x is None else int(x)
+
+
 def _table(problems):
     tab = (L.fg_problem * len(problems))()
     for i, p in enumerate(problems):
         m, n, k, a, b, c = p[:6]
-        tab[i] = L.fg_problem(m, n, k, a.ptr if _is_dev(a) else a, b.ptr if _is_dev(b) else b,
-                              c.ptr if _is_dev(c) else c, k, n, n)
+        lda, ldb, ldc = p[6:9] if len(p) >= 9 else (k, n, n)
+        tab[i] = L.fg_problem(m, n, k, _ptr(a), _ptr(b), _ptr(c), lda, ldb, ldc)
     return tab
 
 
@@ -722,11 +729,18 @@ def shard_requests(dims, world, rank, weights=None):
     return _shard(dims, weights, world, rank, L.FG_SHARD_ONLINE)
 
 
+def _grouped_dtype(dtype):
+    d = np.dtype(dtype)
+    return L.FG_I8 if d == np.int8 else L.FG_U8I8 if d == np.uint8 else L.FG_F32
+
+
 def gemm_grouped(problems, dtype=np.float32, mode=PLAIN):
     """One persistent grouped launch over ragged problems
-    [(m, n, k, A, B, C), ...] (DeviceArrays or raw device pointers)."""
+    [(m, n, k, A, B, C), ...] or [(m, n, k, A, B, C, lda, ldb, ldc), ...]
+    (DeviceArrays or raw device pointers; leading dimensions in elements,
+    default k, n, n).  dtype int8: i8 x i8; uint8: u8 x i8; float32."""
     ctx = default_context()
-    dt = L.FG_I8 if np.dtype(dtype) == np.int8 else L.FG_F32
+    dt = _grouped_dtype(dtype)
     tab = _table(problems)
     check(ctx._lib.fg_gemm_grouped(ctx.handle, dt, _mode(mode), tab, len(problems), None),
           "grouped")
@@ -738,7 +752,7 @@ class GroupedPlan:
 
     def __init__(self, problems, dtype=np.float32, mode=PLAIN):
         self.ctx = default_context()
-        dt = L.FG_I8 if np.dtype(dtype) == np.int8 else L.FG_F32
+        dt = _grouped_dtype(dtype)
         self._tab = _table(problems)
         h = C.c_void_p()
         check(self.ctx._lib.fg_grouped_plan_create(self.ctx.handle, dt, _mode(mode), self._tab,

@@ -91,3 +91,96 @@ def test_grouped_k_zero_and_empty(fg):
     assert np.all(c.to_numpy() == 0.0)
     assert np.max(np.abs(c2.to_numpy() - a2.to_numpy() @ b2.to_numpy())) < 1e-4
     fg.gemm_grouped([], dtype=np.float32)
+
+
+def _placed(rng, dims, esize, aligned_every=4):
+    """Operand placements inside one device buffer: per problem a byte offset
+    and leading dimensions.  Every `aligned_every`-th problem gets 16-byte
+    offsets and leading dimensions (TMA reads it); the others get odd offsets
+    and padded leading dimensions (the loader warps read them)."""
+    out, cur = [], 0
+    for i, (m, n, k) in enumerate(dims):
+        if i % aligned_every == 0:
+            k16, n16 = -(-k // 16) * 16, -(-n // 16) * 16
+            lda, ldb = k16 + 16 * int(rng.integers(0, 2)), n16 + 16 * int(rng.integers(0, 2))
+            oa = -(-cur // 16) * 16
+        else:
+            lda, ldb = k + int(rng.integers(0, 5)), n + int(rng.integers(0, 5))
+            oa = cur + int(rng.integers(1, 16)) * (1 if esize == 1 else 0) + esize * int(rng.integers(1, 4))
+        ob = oa + esize * m * lda
+        ob = -(-ob // 16) * 16 + (0 if i % aligned_every == 0 else esize * int(rng.integers(1, 4)))
+        cur = ob + esize * k * ldb + 64
+        out.append((oa, ob, lda, ldb))
+    return out, cur
+
+
+@pytest.mark.parametrize("dtype", [np.int8, np.uint8])
+def test_grouped_i8_offsets_and_padding(fg, dtype):
+    """i8 / u8 x i8 problems at unaligned offsets with padded leading
+    dimensions (loader warps), mixed in one launch with 16-byte-aligned ones
+    (TMA), padded output rows too: bit-exact against int64 products."""
+    rng = np.random.default_rng(21)
+    dims = ragged_dims(rng, 40, 1, 300)
+    dims = np.vstack([dims, [[1, 1, 1], [130, 3, 260], [5, 129, 17], [256, 256, 256]]])
+    place, total = _placed(rng, dims, 1)
+    buf = np.full(total, 0x5A, np.uint8)  # padding bytes must not leak into results
+    want, outs = [], []
+    for (m, n, k), (oa, ob, lda, ldb) in zip(dims, place):
+        a = rng.integers(0, 256, (m, k), dtype=np.uint8)
+        b = rng.integers(0, 256, (k, n), dtype=np.uint8)
+        for r in range(m):
+            buf[oa + r * lda: oa + r * lda + k] = a[r]
+        for r in range(k):
+            buf[ob + r * ldb: ob + r * ldb + n] = b[r]
+        av = a.astype(np.int64) if dtype == np.uint8 else a.view(np.int8).astype(np.int64)
+        want.append((av @ b.view(np.int8).astype(np.int64)).astype(np.int32))
+    dbuf = fg.DeviceArray.from_numpy(buf)
+    probs = []
+    for (m, n, k), (oa, ob, lda, ldb) in zip(dims, place):
+        ldc = n + int(rng.integers(0, 3))
+        dc = fg.DeviceArray.from_numpy(np.full((m, ldc), -7, np.int32))
+        outs.append((dc, n))
+        probs.append((int(m), int(n), int(k), dbuf.ptr + oa, dbuf.ptr + ob, dc.ptr, lda, ldb, ldc))
+    fg.gemm_grouped(probs, dtype=dtype)
+    for (dc, n), w in zip(outs, want):
+        got = dc.to_numpy()
+        np.testing.assert_array_equal(got[:, :n], w)
+        assert np.all(got[:, n:] == -7), "store past the row end"
+
+
+def test_grouped_split_offsets_and_padding(fg, oracle):
+    """Split-f32 problems whose operands sit at 4-byte (not 16-byte) offsets
+    with padded leading dimensions: within tolerance of the DD oracle, and
+    bit-identical to the same problems from contiguous buffers (the loader
+    warps read both, so placement must not change a bit)."""
+    rng = np.random.default_rng(22)
+    dims = ragged_dims(rng, 24, 1, 300)
+    dims = np.vstack([dims, [[1, 1, 1], [130, 3, 260], [5, 129, 17]]])
+    place, total = _placed(rng, dims, 4, aligned_every=3)
+    buf = np.full(total // 4 + 16, np.nan, np.float32)  # padding must not leak
+    host, probs, probs_c, outs = [], [], [], []
+    for (m, n, k), (oa, ob, lda, ldb) in zip(dims, place):
+        a = rng.standard_normal((m, k)).astype(np.float32)
+        b = rng.standard_normal((k, n)).astype(np.float32)
+        for r in range(m):
+            buf[oa // 4 + r * lda: oa // 4 + r * lda + k] = a[r]
+        for r in range(k):
+            buf[ob // 4 + r * ldb: ob // 4 + r * ldb + n] = b[r]
+        host.append((a, b))
+    dbuf = fg.DeviceArray.from_numpy(buf)
+    keep = []
+    for (m, n, k), (oa, ob, lda, ldb), (a, b) in zip(dims, place, host):
+        dc = fg.DeviceArray((m, n), np.float32)
+        probs.append((int(m), int(n), int(k), dbuf.ptr + oa, dbuf.ptr + ob, dc.ptr, lda, ldb, int(n)))
+        da, db = fg.DeviceArray.from_numpy(a), fg.DeviceArray.from_numpy(b)
+        dc2 = fg.DeviceArray((m, n), np.float32)
+        keep += [da, db]
+        probs_c.append((int(m), int(n), int(k), da, db, dc2))
+        outs.append((dc, dc2))
+    fg.gemm_grouped(probs, dtype=np.float32, mode="split")
+    fg.gemm_grouped(probs_c, dtype=np.float32, mode="split")
+    for (m, n, k), (dc, dc2), (a, b) in zip(dims, outs, host):
+        got = dc.to_numpy()
+        assert np.array_equal(got.view(np.uint32), dc2.to_numpy().view(np.uint32)), (m, n, k)
+        err = oracle.error_vs_dd(a, b, got)
+        assert err <= 2.0 ** -15 + k * U32, (m, n, k, err)
