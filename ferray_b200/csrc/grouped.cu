@@ -1,18 +1,17 @@
 // grouped.cu -- fg_gemm_grouped and prepared grouped plans (CUDA graphs).
 //
 // Lowering of a host problem table:
-//  * dtype FG_I8 / FG_U8I8: tcgen05 kind::i8 grouped kernel; operands that
-//    meet the TMA 16-byte rule (pointer and leading dimension) are read by
-//    TMA, the others are staged by the kernel itself (granule copies and
-//    shift warps), all in place -- no copy pass;
-//  * dtype FG_F32, mode SPLIT: split_prep_kernel cuts every operand into
-//    bf16 hi/lo planes in an arena (one pass); tcgen05 kind::f16 grouped
-//    kernel, three products, K-chunked FP32 accumulation;
+//  * dtype FG_I8 / FG_U8I8: tcgen05 kind::i8 grouped kernel; operands whose
+//    pointer or leading dimension breaks the TMA 16-byte rule are copied into
+//    a 16-byte-pitched arena by the prep launch, the rest are read in place;
+//  * dtype FG_F32, mode SPLIT: the prep launch splits every operand into bf16
+//    hi/lo planes in the arena; tcgen05 kind::f16 grouped kernel, three
+//    products, K-chunked FP32 accumulation;
 //  * dtype FG_F32, mode PLAIN: persistent FFMA grouped kernel.
 // Tiles are numbered deepest problem first and handed out by the kernels'
-// device-side scheduler (an atomic tile counter, zeroed before every
-// launch).  A plan keeps the tables and arena resident and replays the
-// counter reset, split pass and grouped launch from a CUDA graph.
+// device-side scheduler (an atomic tile counter, zeroed before every launch).
+// A plan keeps the tables and arena resident and replays the counter reset,
+// prep and grouped launches from a CUDA graph.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -29,12 +28,8 @@ using namespace fg;
 
 namespace {
 
-// The i8 kernel's stage count leaves room for its raw slots (grouped_smem_bytes).
-using CfgGroupedI8 = TcCfg<KIND_I8, 128, 3, 1, 1, 1, 1, EPI_I32>;
+using CfgGroupedI8 = TcCfg<KIND_I8, 128, 6, 1, 1, 1, 1, EPI_I32>;
 using CfgGroupedBf16 = TcCfg<KIND_BF16, 128, 3, 2, 2, 1, 3, EPI_F32, 1>;
-// 227 KB per block, less the kernel's static shared memory (about 19 KB)
-static_assert(grouped_smem_bytes<CfgGroupedI8>() + 20 * 1024 <= 232448, "i8 grouped kernel shared memory");
-static_assert(grouped_smem_bytes<CfgGroupedBf16>() + 20 * 1024 <= 232448, "split grouped kernel shared memory");
 
 long long rup(long long x, long long a) { return (x + a - 1) / a * a; }
 
@@ -44,7 +39,7 @@ fg_status set_smem_attr() {
     static cudaError_t err = cudaSuccess;
     std::call_once(once, [] {
         err = cudaFuncSetAttribute(tc_grouped_kernel<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   static_cast<int>(grouped_smem_bytes<Cfg>()));
+                                   static_cast<int>(tc_smem_bytes<Cfg>()));
     });
     if (err != cudaSuccess) return fgrt::cuda_error(err, "cudaFuncSetAttribute(grouped)");
     return FG_OK;
@@ -56,8 +51,7 @@ fg_status set_smem_attr() {
 // tiling, layout sizes); bind() fixes the device base address, encodes the
 // TMA descriptors and writes the tables into a host image laid out exactly
 // like the front of the device region; launch() copies that image with one
-// async memcpy and issues the split pass (split form) and the grouped
-// kernel on a stream.
+// async memcpy and issues the prep and grouped kernels on a stream.
 struct fgrt::GroupedJob {
     fg_ctx* ctx = nullptr;
     fg_dtype dtype = FG_F32;
@@ -65,9 +59,7 @@ struct fgrt::GroupedJob {
     int kind = 0;  // 0 = FFMA, 1 = i8 tensor, 2 = bf16x3 tensor
     struct Opnd {
         const void* src = nullptr;
-        long long ld = 0;          // leading dimension TMA reads (elements)
-        long long off0 = -1, off1 = -1;  // split form: hi / lo planes in the arena
-        bool gen = false;          // i8: staged by the kernel (no TMA descriptor)
+        long long off0 = -1, off1 = -1, ld = 0;
     };
     struct Zero {
         void* c;
@@ -78,7 +70,7 @@ struct fgrt::GroupedJob {
     std::vector<Opnd> oa, ob;
     std::vector<Zero> zeros;
     long long total_tiles = 0;
-    long long arena = 0;  // split form: bytes of bf16 planes
+    long long arena = 0;
     int nseg = 0;
     size_t sz_probs = 0, sz_maps = 0, sz_ptrs = 0, sz_segs = 0, sz_tiles = 0;
     static constexpr size_t sz_sched = 256;  // the tile scheduler's counter
@@ -87,7 +79,7 @@ struct fgrt::GroupedJob {
     const void* host = nullptr;
     GroupedArgs targs{};
     SimtGroupedArgs sargs{};
-    SplitSeg* d_segs = nullptr;
+    PrepSeg* d_segs = nullptr;
     unsigned long long* d_counter = nullptr;
     size_t host_bytes() const { return sz_probs + sz_maps + sz_ptrs + sz_segs + sz_tiles + sz_sched; }
     size_t dev_bytes() const { return host_bytes() + static_cast<size_t>(arena); }
@@ -144,6 +136,7 @@ fg_status grouped_job_build(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, const fg_
     j->probs.resize(np);
     j->oa.resize(np);
     j->ob.resize(np);
+    int nseg = 0;
     for (int x = 0; x < np; ++x) {
         const fg_problem& q = table[order[x]];
         j->probs_in[x] = q;
@@ -166,20 +159,28 @@ fg_status grouped_job_build(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, const fg_
         j->total_tiles += (long long)g.tiles_m * g.tiles_n;
         g.C = q.c;
         g.ldc = q.ldc;
-        g.A = q.a;
-        g.B = q.b;
-        g.lda = q.lda;
-        g.ldb = q.ldb;
         auto& oa = j->oa[x];
         auto& ob = j->ob[x];
         oa.src = q.a;
         ob.src = q.b;
-        oa.ld = q.lda;
-        ob.ld = q.ldb;
         if (j->kind == 1) {
             g.k_blocks = static_cast<int>((q.k + 127) / 128);
-            oa.gen = (reinterpret_cast<uintptr_t>(q.a) & 15) || (q.lda % 16);
-            ob.gen = (reinterpret_cast<uintptr_t>(q.b) & 15) || (q.ldb % 16);
+            if ((reinterpret_cast<uintptr_t>(q.a) & 15) || (q.lda % 16)) {
+                oa.ld = rup(q.k, 16);
+                oa.off0 = j->arena;
+                j->arena = rup(j->arena + oa.ld * q.m, 256);
+                ++nseg;
+            } else {
+                oa.ld = q.lda;
+            }
+            if ((reinterpret_cast<uintptr_t>(q.b) & 15) || (q.ldb % 16)) {
+                ob.ld = rup(q.n, 16);
+                ob.off0 = j->arena;
+                j->arena = rup(j->arena + ob.ld * q.k, 256);
+                ++nseg;
+            } else {
+                ob.ld = q.ldb;
+            }
         } else if (j->kind == 2) {
             g.k_blocks = static_cast<int>((q.k + 63) / 64);
             oa.ld = rup(q.k, 8);
@@ -192,19 +193,20 @@ fg_status grouped_job_build(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, const fg_
             j->arena = rup(j->arena + 2 * ob.ld * q.k, 256);
             ob.off1 = j->arena;
             j->arena = rup(j->arena + 2 * ob.ld * q.k, 256);
-            j->nseg += 2;
+            nseg += 2;
         } else {
             g.k_blocks = static_cast<int>((q.k + 15) / 16);
+            oa.ld = q.lda;
+            ob.ld = q.ldb;
         }
     }
-    // TMA descriptors: i8 A and B per problem (slots of staged operands stay
-    // zero); split form hi / lo planes of A and B
-    const int nmaps = j->kind == 1 ? 2 : j->kind == 2 ? 4 : 0;
+    j->nseg = nseg;
+    const int nmaps = j->kind == 2 ? 4 : 2;
     const size_t npp = static_cast<size_t>(std::max(np, 1));
     j->sz_probs = rup(sizeof(GroupedProblem) * npp, 256);
-    j->sz_maps = nmaps ? rup(sizeof(CUtensorMap) * nmaps * npp, 256) : 0;
+    j->sz_maps = j->kind == 0 ? 0 : rup(sizeof(CUtensorMap) * nmaps * npp, 256);
     j->sz_ptrs = j->kind == 0 ? rup((2 * sizeof(void*) + 2 * sizeof(long long)) * npp, 256) : 0;
-    j->sz_segs = rup(sizeof(SplitSeg) * std::max(j->nseg, 1), 256);
+    j->sz_segs = rup(sizeof(PrepSeg) * std::max(nseg, 1), 256);
     j->sz_tiles = rup(sizeof(TileRec) * static_cast<size_t>(std::max<long long>(j->total_tiles, 1)), 256);
     return FG_OK;
 }
@@ -231,44 +233,40 @@ fg_status grouped_job_bind(GroupedJob* j, void* dev_base, void* host_stage) {
     long long t = 0;
     for (int x : order) {
         const GroupedProblem& g = j->probs[x];
-        const int kb = g.k_blocks | (((j->oa[x].gen ? TILE_GEN_A : 0) | (j->ob[x].gen ? TILE_GEN_B : 0))
-                                     << TILE_GEN_SHIFT);
-        const fg_problem& q = j->probs_in[x];
         for (int tm = 0; tm < g.tiles_m; ++tm)
-            for (int tn = 0; tn < g.tiles_n; ++tn)
-                htiles[t++] = TileRec{x, tm, tn, kb, q.a, q.b, q.lda, q.ldb, g.M, g.N, g.K, 0};
+            for (int tn = 0; tn < g.tiles_n; ++tn) htiles[t++] = TileRec{x, tm, tn, g.k_blocks};
     }
     const TileRec* dtiles = reinterpret_cast<const TileRec*>(dbase + o_tiles);
     CUtensorMap* hmaps = reinterpret_cast<CUtensorMap*>(hbase + o_maps);
-    if (j->kind == 1) {
-        std::memset(hmaps, 0, j->sz_maps);
-        for (int x = 0; x < np; ++x) {
-            const fg_problem& q = j->probs_in[x];
-            const auto& oa = j->oa[x];
-            const auto& ob = j->ob[x];
+    PrepSeg* hsegs = reinterpret_cast<PrepSeg*>(hbase + o_segs);
+    int si = 0;
+    for (int x = 0; x < np; ++x) {
+        const fg_problem& q = j->probs_in[x];
+        const auto& oa = j->oa[x];
+        const auto& ob = j->ob[x];
+        if (j->kind == 1) {
+            const void* pa = q.a;
+            const void* pb = q.b;
+            if (oa.off0 >= 0) {
+                pa = d_arena + oa.off0;
+                hsegs[si++] = PrepSeg{q.a, const_cast<void*>(pa), nullptr, q.m, q.k, q.lda, oa.ld, 0, 0};
+            }
+            if (ob.off0 >= 0) {
+                pb = d_arena + ob.off0;
+                hsegs[si++] = PrepSeg{q.b, const_cast<void*>(pb), nullptr, q.k, q.n, q.ldb, ob.ld, 0, 0};
+            }
+            uint64_t da[2] = {(uint64_t)q.k, (uint64_t)q.m}, sa[1] = {(uint64_t)oa.ld};
+            uint64_t db[2] = {(uint64_t)q.n, (uint64_t)q.k}, sb[1] = {(uint64_t)ob.ld};
             uint32_t box[2] = {128, 128};
-            if (!oa.gen) {
-                uint64_t da[2] = {(uint64_t)q.k, (uint64_t)q.m}, sa[1] = {(uint64_t)oa.ld};
-                FG_TRY(encode_map(&hmaps[2 * x], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, q.a, da, sa, box));
-            }
-            if (!ob.gen) {
-                uint64_t db[2] = {(uint64_t)q.n, (uint64_t)q.k}, sb[1] = {(uint64_t)ob.ld};
-                FG_TRY(encode_map(&hmaps[2 * x + 1], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, q.b, db, sb, box));
-            }
-        }
-    } else if (j->kind == 2) {
-        SplitSeg* hsegs = reinterpret_cast<SplitSeg*>(hbase + o_segs);
-        int si = 0;
-        for (int x = 0; x < np; ++x) {
-            const fg_problem& q = j->probs_in[x];
-            const auto& oa = j->oa[x];
-            const auto& ob = j->ob[x];
-            auto* ah = reinterpret_cast<__nv_bfloat16*>(d_arena + oa.off0);
-            auto* al = reinterpret_cast<__nv_bfloat16*>(d_arena + oa.off1);
-            auto* bh = reinterpret_cast<__nv_bfloat16*>(d_arena + ob.off0);
-            auto* bl = reinterpret_cast<__nv_bfloat16*>(d_arena + ob.off1);
-            hsegs[si++] = SplitSeg{static_cast<const float*>(q.a), ah, al, q.m, q.k, q.lda, oa.ld};
-            hsegs[si++] = SplitSeg{static_cast<const float*>(q.b), bh, bl, q.k, q.n, q.ldb, ob.ld};
+            FG_TRY(encode_map(&hmaps[2 * x], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, pa, da, sa, box));
+            FG_TRY(encode_map(&hmaps[2 * x + 1], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, pb, db, sb, box));
+        } else if (j->kind == 2) {
+            void* ah = d_arena + oa.off0;
+            void* al = d_arena + oa.off1;
+            void* bh = d_arena + ob.off0;
+            void* bl = d_arena + ob.off1;
+            hsegs[si++] = PrepSeg{q.a, ah, al, q.m, q.k, q.lda, oa.ld, 0, 1};
+            hsegs[si++] = PrepSeg{q.b, bh, bl, q.k, q.n, q.ldb, ob.ld, 0, 1};
             uint64_t da[2] = {(uint64_t)q.k, (uint64_t)q.m}, sa[1] = {(uint64_t)(2 * oa.ld)};
             uint64_t db[2] = {(uint64_t)q.n, (uint64_t)q.k}, sb[1] = {(uint64_t)(2 * ob.ld)};
             uint32_t boxa[2] = {64, 128}, boxb[2] = {64, 64};
@@ -302,12 +300,12 @@ fg_status grouped_job_bind(GroupedJob* j, void* dev_base, void* host_stage) {
         j->sargs.alpha = 1.f;
         j->sargs.beta = 0.f;
     }
-    j->d_segs = reinterpret_cast<SplitSeg*>(dbase + o_segs);
+    j->d_segs = reinterpret_cast<PrepSeg*>(dbase + o_segs);
     j->targs = GroupedArgs{};
     j->targs.problems = reinterpret_cast<const GroupedProblem*>(dbase);
     j->targs.tiles = dtiles;
     j->targs.tile_counter = j->d_counter;
-    j->targs.maps = j->sz_maps ? reinterpret_cast<const CUtensorMap*>(dbase + o_maps) : nullptr;
+    j->targs.maps = reinterpret_cast<const CUtensorMap*>(dbase + o_maps);
     j->targs.count = np;
     j->targs.total_tiles = j->total_tiles;
     j->targs.alpha = 1.f;
@@ -341,8 +339,8 @@ static fg_status grouped_job_kernels(GroupedJob* j, cudaStream_t st) {
         count_launch();
     }
     if (j->nseg > 0) {
-        ProfScope prof("grouped_split_prep", st);
-        split_prep_kernel<<<std::min(j->nseg, 65535), 256, 0, st>>>(j->d_segs, j->nseg);
+        ProfScope prof("grouped_prep", st);
+        grouped_prep_kernel<<<std::min(j->nseg, 65535), 256, 0, st>>>(j->d_segs, j->nseg, 0);
         prof.stop();
         count_launch();
     }
@@ -358,13 +356,11 @@ static fg_status grouped_job_kernels(GroupedJob* j, cudaStream_t st) {
         prof.stop();
     } else if (j->kind == 1) {
         ProfScope prof("tc_grouped_i8", st);
-        tc_grouped_kernel<CfgGroupedI8>
-            <<<grid, LoaderCfg<CfgGroupedI8>::THREADS, grouped_smem_bytes<CfgGroupedI8>(), st>>>(j->targs);
+        tc_grouped_kernel<CfgGroupedI8><<<grid, CfgGroupedI8::THREADS, tc_smem_bytes<CfgGroupedI8>(), st>>>(j->targs);
         prof.stop();
     } else {
         ProfScope prof("tc_grouped_3xbf16", st);
-        tc_grouped_kernel<CfgGroupedBf16>
-            <<<grid, LoaderCfg<CfgGroupedBf16>::THREADS, grouped_smem_bytes<CfgGroupedBf16>(), st>>>(j->targs);
+        tc_grouped_kernel<CfgGroupedBf16><<<grid, CfgGroupedBf16::THREADS, tc_smem_bytes<CfgGroupedBf16>(), st>>>(j->targs);
         prof.stop();
     }
     count_launch();
