@@ -376,87 +376,155 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
 }
 
 // ------------------------------------------------------------------ prep
-// One launch over a list of segments: copy a byte matrix into a 16-byte-
-// pitched buffer (op 0) or split an f32 matrix into bf16 hi/lo planes (op 1).
-// Work is one destination row per warp: the warp finds its segment once
-// (binary search over the segments' first rows) and its lanes stride over
-// the row, so loads and stores are coalesced along the row.
+// One launch over a list of segments, one per operand that TMA cannot read
+// as it is: op 0 copies a byte matrix whose pointer or leading dimension
+// breaks the TMA 16-byte rule into a 16-byte-pitched buffer (i8); op 1 cuts
+// an f32 matrix into bf16 hi = bf16(x) and lo = bf16(x - hi) planes (round
+// to nearest even; the split form).  Bytes / elements past a row's end
+// become 0.  Source rows are read as the aligned 16-byte granules that hold
+// them (a granule is read only when it holds a byte of the row, so every
+// read stays on memory the row occupies) and shifted into place in
+// registers, so each thread issues one to three 16-byte loads per 16-byte
+// output chunk, PREP_ILP chunks per thread per pass with every load issued
+// before the first store.
 struct PrepSeg {
     const void* src;
     void* dst0;
     void* dst1;
     long long rows, cols, ld_src, ld_dst;  // elements
-    long long start;                       // first global row of this segment
+    long long start;                       // unused (kept for the table layout)
     int op;
 };
 
-// One 16-byte destination chunk of segment row r at byte / element offset c.
-__device__ __forceinline__ void prep_chunk(const PrepSeg& sg, long long r, long long c) {
-    if (sg.op == 0) {
-        // 16 bytes of an unaligned row from the one or two aligned 16-byte
-        // granules that hold them: a granule is read only when it holds a
-        // byte of the row, so every read stays on memory the row occupies.
-        // Bytes past the row end become 0.
-        const uint8_t* src = static_cast<const uint8_t*>(sg.src) + r * sg.ld_src + c;
-        const long long valid = sg.cols - c;  // bytes of the row from c on
-        unsigned long long o0 = 0, o1 = 0;
-        if (valid > 0) {
-            const uintptr_t a = reinterpret_cast<uintptr_t>(src);
-            const uintptr_t base = a & ~static_cast<uintptr_t>(15);
-            const int sh = static_cast<int>(a - base);
-            const ulonglong2 w0 = __ldg(reinterpret_cast<const ulonglong2*>(base));
-            ulonglong2 w1 = make_ulonglong2(0ull, 0ull);
-            if (sh + valid > 16) w1 = __ldg(reinterpret_cast<const ulonglong2*>(base + 16));
-            const bool hi = sh >= 8;
-            const unsigned long long x0 = hi ? w0.y : w0.x, x1 = hi ? w1.x : w0.y, x2 = hi ? w1.y : w1.x;
-            const int sb = (sh & 7) * 8;
-            o0 = sb ? (x0 >> sb) | (x1 << (64 - sb)) : x0;
-            o1 = sb ? (x1 >> sb) | (x2 << (64 - sb)) : x1;
-            if (valid < 16) {
-                o1 = valid <= 8 ? 0ull : (o1 & ((1ull << (8 * (valid - 8))) - 1));
-                if (valid < 8) o0 &= (1ull << (8 * valid)) - 1;
-            }
-        }
-        *reinterpret_cast<ulonglong2*>(static_cast<uint8_t*>(sg.dst0) + r * sg.ld_dst + c) = make_ulonglong2(o0, o1);
-    } else {
-        const float* src = static_cast<const float*>(sg.src) + r * sg.ld_src;
-        __align__(16) __nv_bfloat16 h[8], l[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const float x = c + j < sg.cols ? __ldg(src + c + j) : 0.f;
-            h[j] = __float2bfloat16_rn(x);
-            l[j] = __float2bfloat16_rn(x - __bfloat162float(h[j]));
-        }
-        *reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(sg.dst0) + r * sg.ld_dst + c) =
-            *reinterpret_cast<const uint4*>(h);
-        *reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(sg.dst1) + r * sg.ld_dst + c) =
-            *reinterpret_cast<const uint4*>(l);
+constexpr int PREP_ILP = 2;  // output chunks per thread per pass, loads issued first
+
+// op 0: 16 bytes of a row starting at byte address p, `valid` of them in
+// the row (valid <= 0: none).
+struct PrepBytes {
+    ulonglong2 w0, w1;
+    int sh;
+    int valid;
+};
+__device__ __forceinline__ PrepBytes prep_load_bytes(const uint8_t* p, long long valid) {
+    PrepBytes g;
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    const uintptr_t base = a & ~static_cast<uintptr_t>(15);
+    g.sh = static_cast<int>(a - base);
+    g.valid = static_cast<int>(valid < 0 ? 0 : valid > 16 ? 16 : valid);
+    g.w0 = make_ulonglong2(0ull, 0ull);
+    g.w1 = make_ulonglong2(0ull, 0ull);
+    if (g.valid > 0) g.w0 = __ldg(reinterpret_cast<const ulonglong2*>(base));
+    if (g.valid > 0 && g.sh + g.valid > 16) g.w1 = __ldg(reinterpret_cast<const ulonglong2*>(base + 16));
+    return g;
+}
+__device__ __forceinline__ ulonglong2 prep_shift_bytes(const PrepBytes& g) {
+    if (g.valid <= 0) return make_ulonglong2(0ull, 0ull);
+    const bool hi = g.sh >= 8;
+    const unsigned long long x0 = hi ? g.w0.y : g.w0.x, x1 = hi ? g.w1.x : g.w0.y, x2 = hi ? g.w1.y : g.w1.x;
+    const int sb = (g.sh & 7) * 8;
+    unsigned long long o0 = sb ? (x0 >> sb) | (x1 << (64 - sb)) : x0;
+    unsigned long long o1 = sb ? (x1 >> sb) | (x2 << (64 - sb)) : x1;
+    if (g.valid < 16) {
+        o1 = g.valid <= 8 ? 0ull : (o1 & ((1ull << (8 * (g.valid - 8))) - 1));
+        if (g.valid < 8) o0 &= (1ull << (8 * g.valid)) - 1;
     }
+    return make_ulonglong2(o0, o1);
 }
 
-static __global__ void grouped_prep_kernel(const PrepSeg* __restrict__ segs, int nseg,
-                                           long long total_rows) {
+// op 1: 8 floats of a row starting at p (4-byte aligned), `valid` of them
+// in the row, from the two or three aligned granules that hold them.
+struct PrepFloats {
+    float4 g0, g1, g2;
+    int q;  // floats into the first granule
+    int valid;
+};
+__device__ __forceinline__ PrepFloats prep_load_floats(const float* p, long long valid) {
+    PrepFloats g;
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    const uintptr_t base = a & ~static_cast<uintptr_t>(15);
+    g.q = static_cast<int>(a - base) >> 2;
+    g.valid = static_cast<int>(valid < 0 ? 0 : valid > 8 ? 8 : valid);
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4* gp = reinterpret_cast<const float4*>(base);
+    g.g0 = g.valid > 0 ? __ldg(gp) : z;
+    g.g1 = g.valid > 0 && g.q + g.valid > 4 ? __ldg(gp + 1) : z;
+    g.g2 = g.valid > 0 && g.q > 0 && g.q + g.valid > 8 ? __ldg(gp + 2) : z;
+    return g;
+}
+__device__ __forceinline__ void prep_split_floats(const PrepFloats& g, uint4& hi, uint4& lo) {
+    const float w[12] = {g.g0.x, g.g0.y, g.g0.z, g.g0.w, g.g1.x, g.g1.y, g.g1.z, g.g1.w,
+                         g.g2.x, g.g2.y, g.g2.z, g.g2.w};
+    float v[11], f[8];
+#pragma unroll
+    for (int k = 0; k < 11; ++k) v[k] = (g.q & 1) ? w[k + 1] : w[k];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const float x = (g.q & 2) ? v[k + 2] : v[k];
+        f[k] = k < g.valid ? x : 0.f;
+    }
+    uint32_t h[4], l[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const __nv_bfloat162 hv = __floats2bfloat162_rn(f[2 * e], f[2 * e + 1]);
+        const __nv_bfloat162 lv = __floats2bfloat162_rn(f[2 * e] - __low2float(hv), f[2 * e + 1] - __high2float(hv));
+        h[e] = *reinterpret_cast<const uint32_t*>(&hv);
+        l[e] = *reinterpret_cast<const uint32_t*>(&lv);
+    }
+    hi = make_uint4(h[0], h[1], h[2], h[3]);
+    lo = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
+static __global__ void __launch_bounds__(256) grouped_prep_kernel(const PrepSeg* __restrict__ segs, int nseg,
+                                                                  long long total_rows) {
     // One block per segment (grid-stride over segments).  The block's threads
     // take the segment's 16-byte destination chunks (destination pitch is a
-    // multiple of 16 bytes) in row-major order, so rows shorter than a warp's
-    // reach still keep every lane busy; consecutive lanes write consecutive
-    // chunks.  Out-of-row bytes become 0.
+    // multiple of 16 bytes) in row-major order, PREP_ILP per thread per pass
+    // with all loads issued before the first store, so rows shorter than a
+    // warp's reach still keep every lane busy and each thread keeps several
+    // loads in flight; consecutive lanes write consecutive chunks.
     (void)total_rows;
     for (int si = blockIdx.x; si < nseg; si += gridDim.x) {
         const PrepSeg sg = segs[si];
-        const long long per = sg.op == 0 ? 16 : 8;  // elements per chunk
-        const long long cpr = sg.ld_dst / per;      // chunks per row
+        const unsigned per = sg.op == 0 ? 16u : 8u;                   // elements per chunk
+        const unsigned cpr = static_cast<unsigned>(sg.ld_dst / per);  // chunks per row
         const long long total = sg.rows * cpr;
-        if (total < (1LL << 31)) {
-            const unsigned ucpr = static_cast<unsigned>(cpr);
-            for (unsigned idx = threadIdx.x; idx < static_cast<unsigned>(total); idx += blockDim.x) {
-                const unsigned r = idx / ucpr;
-                prep_chunk(sg, r, static_cast<long long>(idx - r * ucpr) * per);
+        for (long long pass = 0; pass < total; pass += static_cast<long long>(PREP_ILP) * blockDim.x) {
+            long long r[PREP_ILP], c[PREP_ILP];
+#pragma unroll
+            for (int q = 0; q < PREP_ILP; ++q) {
+                const long long idx = pass + threadIdx.x + static_cast<long long>(q) * blockDim.x;
+                r[q] = -1;
+                c[q] = 0;
+                if (idx < total) {
+                    r[q] = idx / cpr;
+                    c[q] = (idx - r[q] * cpr) * per;
+                }
             }
-        } else {
-            for (long long idx = threadIdx.x; idx < total; idx += blockDim.x) {
-                const long long r = idx / cpr;
-                prep_chunk(sg, r, (idx - r * cpr) * per);
+            if (sg.op == 0) {
+                PrepBytes g[PREP_ILP];
+#pragma unroll
+                for (int q = 0; q < PREP_ILP; ++q)
+                    g[q] = prep_load_bytes(static_cast<const uint8_t*>(sg.src) + (r[q] < 0 ? 0 : r[q] * sg.ld_src + c[q]),
+                                           r[q] < 0 ? 0 : sg.cols - c[q]);
+#pragma unroll
+                for (int q = 0; q < PREP_ILP; ++q)
+                    if (r[q] >= 0)
+                        *reinterpret_cast<ulonglong2*>(static_cast<uint8_t*>(sg.dst0) + r[q] * sg.ld_dst + c[q]) =
+                            prep_shift_bytes(g[q]);
+            } else {
+                PrepFloats g[PREP_ILP];
+#pragma unroll
+                for (int q = 0; q < PREP_ILP; ++q)
+                    g[q] = prep_load_floats(static_cast<const float*>(sg.src) + (r[q] < 0 ? 0 : r[q] * sg.ld_src + c[q]),
+                                            r[q] < 0 ? 0 : sg.cols - c[q]);
+#pragma unroll
+                for (int q = 0; q < PREP_ILP; ++q) {
+                    if (r[q] < 0) continue;
+                    uint4 hi, lo;
+                    prep_split_floats(g[q], hi, lo);
+                    *reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(sg.dst0) + r[q] * sg.ld_dst + c[q]) = hi;
+                    *reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(sg.dst1) + r[q] * sg.ld_dst + c[q]) = lo;
+                }
             }
         }
     }
