@@ -340,7 +340,10 @@ static fg_status grouped_job_kernels(GroupedJob* j, cudaStream_t st) {
     }
     if (j->nseg > 0) {
         ProfScope prof("grouped_prep", st);
-        grouped_prep_kernel<<<std::min(j->nseg, 65535), 256, 0, st>>>(j->d_segs, j->nseg, 0);
+        if (j->kind == 1)
+            grouped_prep_kernel<0><<<std::min(j->nseg, 65535), 256, 0, st>>>(j->d_segs, j->nseg, 0);
+        else
+            grouped_prep_kernel<1><<<std::min(j->nseg, 65535), 256, 0, st>>>(j->d_segs, j->nseg, 0);
         prof.stop();
         count_launch();
     }

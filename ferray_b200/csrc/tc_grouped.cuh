@@ -385,8 +385,8 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
 // them (a granule is read only when it holds a byte of the row, so every
 // read stays on memory the row occupies) and shifted into place in
 // registers, so each thread issues one to three 16-byte loads per 16-byte
-// output chunk, PREP_ILP chunks per thread per pass with every load issued
-// before the first store.
+// output chunk, prep_ilp() chunks per thread per pass with every load
+// issued before the first store.
 struct PrepSeg {
     const void* src;
     void* dst0;
@@ -396,7 +396,13 @@ struct PrepSeg {
     int op;
 };
 
-constexpr int PREP_ILP = 2;  // output chunks per thread per pass, loads issued first
+// output chunks per thread per pass (loads issued first): the byte copy
+// keeps one (more registers would halve occupancy and it was measured
+// slower), the split two
+template <int OP>
+constexpr int prep_ilp() {
+    return OP == 0 ? 1 : 2;
+}
 
 // op 0: 16 bytes of a row starting at byte address p, `valid` of them in
 // the row (valid <= 0: none).
@@ -474,8 +480,12 @@ __device__ __forceinline__ void prep_split_floats(const PrepFloats& g, uint4& hi
     lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
+// OP: every segment of a launch has the same op (a plan is all i8 or all
+// split), so each op gets its own instantiation and register budget.
+template <int OP>
 static __global__ void __launch_bounds__(256) grouped_prep_kernel(const PrepSeg* __restrict__ segs, int nseg,
                                                                   long long total_rows) {
+    constexpr int PREP_ILP = prep_ilp<OP>();
     // One block per segment (grid-stride over segments).  The block's threads
     // take the segment's 16-byte destination chunks (destination pitch is a
     // multiple of 16 bytes) in row-major order, PREP_ILP per thread per pass
@@ -485,7 +495,7 @@ static __global__ void __launch_bounds__(256) grouped_prep_kernel(const PrepSeg*
     (void)total_rows;
     for (int si = blockIdx.x; si < nseg; si += gridDim.x) {
         const PrepSeg sg = segs[si];
-        const unsigned per = sg.op == 0 ? 16u : 8u;                   // elements per chunk
+        const unsigned per = OP == 0 ? 16u : 8u;                      // elements per chunk
         const unsigned cpr = static_cast<unsigned>(sg.ld_dst / per);  // chunks per row
         const long long total = sg.rows * cpr;
         for (long long pass = 0; pass < total; pass += static_cast<long long>(PREP_ILP) * blockDim.x) {
@@ -496,11 +506,17 @@ static __global__ void __launch_bounds__(256) grouped_prep_kernel(const PrepSeg*
                 r[q] = -1;
                 c[q] = 0;
                 if (idx < total) {
-                    r[q] = idx / cpr;
-                    c[q] = (idx - r[q] * cpr) * per;
+                    if (total < (1LL << 31)) {  // 32-bit division where it fits
+                        const unsigned u = static_cast<unsigned>(idx), ur = u / cpr;
+                        r[q] = ur;
+                        c[q] = static_cast<long long>(u - ur * cpr) * per;
+                    } else {
+                        r[q] = idx / cpr;
+                        c[q] = (idx - r[q] * cpr) * per;
+                    }
                 }
             }
-            if (sg.op == 0) {
+            if constexpr (OP == 0) {
                 PrepBytes g[PREP_ILP];
 #pragma unroll
                 for (int q = 0; q < PREP_ILP; ++q)
