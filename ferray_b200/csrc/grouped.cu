@@ -72,7 +72,8 @@ struct fgrt::GroupedJob {
     long long total_tiles = 0;
     long long arena = 0;
     int nseg = 0;
-    size_t sz_probs = 0, sz_maps = 0, sz_ptrs = 0, sz_segs = 0, sz_tiles = 0;
+    int njobs = 0;  // prep launch blocks: segments cut at PREP_JOB_CHUNKS chunks
+    size_t sz_probs = 0, sz_maps = 0, sz_ptrs = 0, sz_segs = 0, sz_jobs = 0, sz_tiles = 0;
     static constexpr size_t sz_sched = 256;  // the tile scheduler's counter
     // bound state
     void* dev = nullptr;
@@ -80,8 +81,9 @@ struct fgrt::GroupedJob {
     GroupedArgs targs{};
     SimtGroupedArgs sargs{};
     PrepSeg* d_segs = nullptr;
+    PrepJob* d_jobs = nullptr;
     unsigned long long* d_counter = nullptr;
-    size_t host_bytes() const { return sz_probs + sz_maps + sz_ptrs + sz_segs + sz_tiles + sz_sched; }
+    size_t host_bytes() const { return sz_probs + sz_maps + sz_ptrs + sz_segs + sz_jobs + sz_tiles + sz_sched; }
     size_t dev_bytes() const { return host_bytes() + static_cast<size_t>(arena); }
 };
 
@@ -170,6 +172,7 @@ fg_status grouped_job_build(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, const fg_
                 oa.off0 = j->arena;
                 j->arena = rup(j->arena + oa.ld * q.m, 256);
                 ++nseg;
+                j->njobs += static_cast<int>((q.m * (oa.ld / 16) + PREP_JOB_CHUNKS - 1) / PREP_JOB_CHUNKS);
             } else {
                 oa.ld = q.lda;
             }
@@ -178,6 +181,7 @@ fg_status grouped_job_build(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, const fg_
                 ob.off0 = j->arena;
                 j->arena = rup(j->arena + ob.ld * q.k, 256);
                 ++nseg;
+                j->njobs += static_cast<int>((q.k * (ob.ld / 16) + PREP_JOB_CHUNKS - 1) / PREP_JOB_CHUNKS);
             } else {
                 ob.ld = q.ldb;
             }
@@ -194,6 +198,8 @@ fg_status grouped_job_build(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, const fg_
             ob.off1 = j->arena;
             j->arena = rup(j->arena + 2 * ob.ld * q.k, 256);
             nseg += 2;
+            j->njobs += static_cast<int>((q.m * (oa.ld / 8) + PREP_JOB_CHUNKS - 1) / PREP_JOB_CHUNKS +
+                                         (q.k * (ob.ld / 8) + PREP_JOB_CHUNKS - 1) / PREP_JOB_CHUNKS);
         } else {
             g.k_blocks = static_cast<int>((q.k + 15) / 16);
             oa.ld = q.lda;
@@ -207,6 +213,7 @@ fg_status grouped_job_build(fg_ctx* ctx, fg_dtype dtype, fg_mode mode, const fg_
     j->sz_maps = j->kind == 0 ? 0 : rup(sizeof(CUtensorMap) * nmaps * npp, 256);
     j->sz_ptrs = j->kind == 0 ? rup((2 * sizeof(void*) + 2 * sizeof(long long)) * npp, 256) : 0;
     j->sz_segs = rup(sizeof(PrepSeg) * std::max(nseg, 1), 256);
+    j->sz_jobs = rup(sizeof(PrepJob) * static_cast<size_t>(std::max(j->njobs, 1)), 256);
     j->sz_tiles = rup(sizeof(TileRec) * static_cast<size_t>(std::max<long long>(j->total_tiles, 1)), 256);
     return FG_OK;
 }
@@ -217,7 +224,7 @@ fg_status grouped_job_bind(GroupedJob* j, void* dev_base, void* host_stage) {
     char* dbase = static_cast<char*>(dev_base);
     char* hbase = static_cast<char*>(host_stage);
     const size_t o_maps = j->sz_probs, o_ptrs = o_maps + j->sz_maps, o_segs = o_ptrs + j->sz_ptrs;
-    const size_t o_tiles = o_segs + j->sz_segs, o_sched = o_tiles + j->sz_tiles;
+    const size_t o_jobs = o_segs + j->sz_segs, o_tiles = o_jobs + j->sz_jobs, o_sched = o_tiles + j->sz_tiles;
     char* d_arena = dbase + j->host_bytes();
     std::memset(hbase + o_sched, 0, j->sz_sched);
     j->d_counter = reinterpret_cast<unsigned long long*>(dbase + o_sched);
@@ -276,6 +283,19 @@ fg_status grouped_job_bind(GroupedJob* j, void* dev_base, void* host_stage) {
             FG_TRY(encode_map(&hmaps[4 * x + 3], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, bl, db, sb, boxb));
         }
     }
+    {
+        // block jobs: each segment cut into runs of at most PREP_JOB_CHUNKS chunks
+        PrepJob* hjobs = reinterpret_cast<PrepJob*>(hbase + o_jobs);
+        int ji = 0;
+        for (int k = 0; k < si; ++k) {
+            const PrepSeg& sg = hsegs[k];
+            const long long n = sg.rows * (sg.ld_dst / (sg.op == 0 ? 16 : 8));
+            for (long long c0 = 0; c0 < n && ji < j->njobs; c0 += PREP_JOB_CHUNKS)
+                hjobs[ji++] = PrepJob{k, 0, c0, std::min(n, c0 + PREP_JOB_CHUNKS)};
+        }
+        if (ji != j->njobs || si != j->nseg) return set_error(FG_ERR_INVALID, "grouped plan: prep table mismatch");
+    }
+    j->d_jobs = reinterpret_cast<PrepJob*>(dbase + o_jobs);
     if (j->kind == 0) {
         const void** pa = reinterpret_cast<const void**>(hbase + o_ptrs);
         const void** pb = pa + npp;
@@ -340,10 +360,11 @@ static fg_status grouped_job_kernels(GroupedJob* j, cudaStream_t st) {
     }
     if (j->nseg > 0) {
         ProfScope prof("grouped_prep", st);
+        const int blocks = std::min(j->njobs, 1 << 20);
         if (j->kind == 1)
-            grouped_prep_kernel<0><<<std::min(j->nseg, 65535), 256, 0, st>>>(j->d_segs, j->nseg, 0);
+            grouped_prep_kernel<0><<<blocks, 256, 0, st>>>(j->d_segs, j->d_jobs, j->njobs);
         else
-            grouped_prep_kernel<1><<<std::min(j->nseg, 65535), 256, 0, st>>>(j->d_segs, j->nseg, 0);
+            grouped_prep_kernel<1><<<blocks, 256, 0, st>>>(j->d_segs, j->d_jobs, j->njobs);
         prof.stop();
         count_launch();
     }

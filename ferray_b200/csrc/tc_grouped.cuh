@@ -480,25 +480,34 @@ __device__ __forceinline__ void prep_split_floats(const PrepFloats& g, uint4& hi
     lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
+// A block job: chunks [c0, c1) of one segment.  Segments longer than
+// PREP_JOB_CHUNKS chunks are cut into several jobs (host-built table), so
+// the largest operands do not leave one block working long after the rest.
+struct PrepJob {
+    int seg, pad;
+    long long c0, c1;
+};
+constexpr long long PREP_JOB_CHUNKS = 4096;
+
 // OP: every segment of a launch has the same op (a plan is all i8 or all
 // split), so each op gets its own instantiation and register budget.
 template <int OP>
-static __global__ void __launch_bounds__(256) grouped_prep_kernel(const PrepSeg* __restrict__ segs, int nseg,
-                                                                  long long total_rows) {
+static __global__ void __launch_bounds__(256) grouped_prep_kernel(const PrepSeg* __restrict__ segs,
+                                                                  const PrepJob* __restrict__ jobs, int njobs) {
     constexpr int PREP_ILP = prep_ilp<OP>();
-    // One block per segment (grid-stride over segments).  The block's threads
-    // take the segment's 16-byte destination chunks (destination pitch is a
-    // multiple of 16 bytes) in row-major order, PREP_ILP per thread per pass
-    // with all loads issued before the first store, so rows shorter than a
-    // warp's reach still keep every lane busy and each thread keeps several
-    // loads in flight; consecutive lanes write consecutive chunks.
-    (void)total_rows;
-    for (int si = blockIdx.x; si < nseg; si += gridDim.x) {
-        const PrepSeg sg = segs[si];
+    // One block per job (grid-stride over jobs).  The block's threads take
+    // the job's 16-byte destination chunks (destination pitch is a multiple
+    // of 16 bytes) in row-major order, PREP_ILP per thread per pass with all
+    // loads issued before the first store, so rows shorter than a warp's
+    // reach still keep every lane busy and each thread keeps several loads in
+    // flight; consecutive lanes write consecutive chunks.
+    for (int ji = blockIdx.x; ji < njobs; ji += gridDim.x) {
+        const PrepJob jb = jobs[ji];
+        const PrepSeg sg = segs[jb.seg];
         const unsigned per = OP == 0 ? 16u : 8u;                      // elements per chunk
         const unsigned cpr = static_cast<unsigned>(sg.ld_dst / per);  // chunks per row
-        const long long total = sg.rows * cpr;
-        for (long long pass = 0; pass < total; pass += static_cast<long long>(PREP_ILP) * blockDim.x) {
+        const long long total = jb.c1;
+        for (long long pass = jb.c0; pass < total; pass += static_cast<long long>(PREP_ILP) * blockDim.x) {
             long long r[PREP_ILP], c[PREP_ILP];
 #pragma unroll
             for (int q = 0; q < PREP_ILP; ++q) {
