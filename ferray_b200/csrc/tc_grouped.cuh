@@ -396,12 +396,11 @@ struct PrepSeg {
     int op;
 };
 
-// output chunks per thread per pass (loads issued first): the byte copy
-// keeps one (more registers would halve occupancy and it was measured
-// slower), the split two
+// output chunks per thread per pass (loads issued first): one for both ops
+// -- two halved the blocks per SM (registers) and were measured slower
 template <int OP>
 constexpr int prep_ilp() {
-    return OP == 0 ? 1 : 2;
+    return 1;
 }
 
 // op 0: 16 bytes of a row starting at byte address p, `valid` of them in
