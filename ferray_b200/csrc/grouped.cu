@@ -332,7 +332,9 @@ fg_status grouped_job_bind(GroupedJob* j, void* dev_base, void* host_stage) {
     j->targs.beta = 0.f;
     j->targs.status = j->ctx->d_status;
     j->targs.timeout_ns = 4000000000ull;
-    j->targs.kchunk = 2;
+    // split form: K blocks (64 values each) per TMEM accumulation chunk, as
+    // in the single-problem split GEMM
+    j->targs.kchunk = 4;
     if (j->kind == 1) {
         j->targs.ops[0] = TcOp{0, 0, 0, j->dtype == FG_I8 ? 1 : 0, 1};
         FG_TRY(set_smem_attr<CfgGroupedI8>());
