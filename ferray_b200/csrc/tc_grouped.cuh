@@ -55,13 +55,18 @@ struct GroupedArgs {
 
 // Stores one warp's 32 rows x 32 columns: lane l holds row row0 + l.  The
 // block goes through a padded shared-memory tile so that the global stores
-// (and the reads of C for accumulate / beta) are 128-byte row segments.
+// (and the reads of C for accumulate / beta) are 128-byte row segments.  The
+// tile's rows are 36 words apart: each lane writes its row as eight 16-byte
+// stores (banks 4l + 4q: no conflict within a quarter warp) and each lane
+// then reads one column (banks 4r + l: no conflict).
+constexpr int EPI_PITCH = 36;
 template <class Cfg>
 __device__ __forceinline__ void grouped_store(const GroupedArgs& g, const GroupedProblem& pr, int row0,
-                                              int col0, const uint32_t (&v)[32], uint32_t (*stg)[33],
+                                              int col0, const uint32_t (&v)[32], uint32_t (*stg)[EPI_PITCH],
                                               int lane) {
 #pragma unroll
-    for (int j = 0; j < 32; ++j) stg[lane][j] = v[j];
+    for (int q = 0; q < 8; ++q)
+        *reinterpret_cast<uint4*>(&stg[lane][4 * q]) = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
     __syncwarp();
     const int col = col0 + lane;
     const int rows = min(32, pr.M - row0);
@@ -292,8 +297,8 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
         }
     } else {
         const int ew = warp & 3;
-        __shared__ uint32_t epi_stage[4][32][33];
-        uint32_t (*stg)[33] = epi_stage[ew];
+        __shared__ __align__(16) uint32_t epi_stage[4][32][EPI_PITCH];
+        uint32_t (*stg)[EPI_PITCH] = epi_stage[ew];
         int it = 0;
         bool ok = true;
         int slot = 0;
@@ -342,12 +347,20 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
                 } else {
                     // chunks past the problem's last row / column hold nothing
                     const int nch = row0 < pr.M ? min(Cfg::BN / 32, (pr.N - tn * Cfg::BN + 31) / 32) : 0;
+                    // two chunks in flight: chunk c + 1 is read out of TMEM
+                    // while chunk c goes to memory
+                    uint32_t va[32], vb[32];
+                    if (nch > 0) tmem_ld_32x32b_x32(row_addr, va);
 #pragma unroll 1
-                    for (int c = 0; c < nch; ++c) {
-                        uint32_t v[32];
-                        tmem_ld_32x32b_x32(row_addr + c * 32, v);
+                    for (int c = 0; c < nch; c += 2) {
                         tmem_wait_ld();
-                        grouped_store<Cfg>(g, pr, row0, tn * Cfg::BN + c * 32, v, stg, lane);
+                        if (c + 1 < nch) tmem_ld_32x32b_x32(row_addr + (c + 1) * 32, vb);
+                        grouped_store<Cfg>(g, pr, row0, tn * Cfg::BN + c * 32, va, stg, lane);
+                        if (c + 1 < nch) {
+                            tmem_wait_ld();
+                            if (c + 2 < nch) tmem_ld_32x32b_x32(row_addr + (c + 2) * 32, va);
+                            grouped_store<Cfg>(g, pr, row0, tn * Cfg::BN + (c + 1) * 32, vb, stg, lane);
+                        }
                     }
                 }
                 tc_fence_before();
