@@ -264,8 +264,10 @@ fg_status grouped_job_bind(GroupedJob* j, void* dev_base, void* host_stage) {
             }
             uint64_t da[2] = {(uint64_t)q.k, (uint64_t)q.m}, sa[1] = {(uint64_t)oa.ld};
             uint64_t db[2] = {(uint64_t)q.n, (uint64_t)q.k}, sb[1] = {(uint64_t)ob.ld};
-            uint32_t box[2] = {128, 128};
-            FG_TRY(encode_map(&hmaps[2 * x], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, pa, da, sa, box));
+            // A in 8-row boxes (the kernel spreads them over the accumulator's
+            // lane quadrants), B in 128 x 128 boxes
+            uint32_t boxa[2] = {128, 8}, box[2] = {128, 128};
+            FG_TRY(encode_map(&hmaps[2 * x], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, pa, da, sa, boxa));
             FG_TRY(encode_map(&hmaps[2 * x + 1], CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, pb, db, sb, box));
         } else if (j->kind == 2) {
             void* ah = d_arena + oa.off0;
@@ -276,7 +278,7 @@ fg_status grouped_job_bind(GroupedJob* j, void* dev_base, void* host_stage) {
             hsegs[si++] = PrepSeg{q.b, bh, bl, q.k, q.n, q.ldb, ob.ld, 0, 1};
             uint64_t da[2] = {(uint64_t)q.k, (uint64_t)q.m}, sa[1] = {(uint64_t)(2 * oa.ld)};
             uint64_t db[2] = {(uint64_t)q.n, (uint64_t)q.k}, sb[1] = {(uint64_t)(2 * ob.ld)};
-            uint32_t boxa[2] = {64, 128}, boxb[2] = {64, 64};
+            uint32_t boxa[2] = {64, 8}, boxb[2] = {64, 64};  // A in 8-row boxes (row spreading)
             FG_TRY(encode_map(&hmaps[4 * x + 0], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, ah, da, sa, boxa));
             FG_TRY(encode_map(&hmaps[4 * x + 1], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, al, da, sa, boxa));
             FG_TRY(encode_map(&hmaps[4 * x + 2], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, bh, db, sb, boxb));

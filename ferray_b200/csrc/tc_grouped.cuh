@@ -53,7 +53,20 @@ struct GroupedArgs {
 };
 
 
-// Stores one warp's 32 rows x 32 columns: lane l holds row row0 + l.  The
+// Row spreading: the producer loads a tile's A rows as sixteen 8-row TMA
+// boxes, source rows 8i .. 8i + 7 into shared-memory rows 32 (i % 4) +
+// 8 (i / 4) (each box is one 1024-byte 128B-swizzle atom, so the layout is
+// the canonical one with the rows permuted).  Accumulator row p -- TMEM lane
+// p, read by epilogue warp p / 32 -- then holds tile row
+// 32 ((p % 32) / 8) + 8 (p / 32) + p % 8, so a tile's first 32 rows are
+// shared by all four epilogue warps instead of all landing on the first
+// (ragged tiles are mostly short: M averages about 121).
+__device__ __forceinline__ int spread_row(int ew, int lane) {
+    return 32 * (lane >> 3) + 8 * ew + (lane & 7);
+}
+
+// Stores one warp's 32 rows x 32 columns: lane l holds tile row
+// spread_row(ew, l) of the tile starting at row `base`.  The
 // block goes through a padded shared-memory tile so that the global stores
 // (and the reads of C for accumulate / beta) are 128-byte row segments.  The
 // tile's rows are 36 words apart: each lane writes its row as eight 16-byte
@@ -61,7 +74,7 @@ struct GroupedArgs {
 // then reads one column (banks 4r + l: no conflict).
 constexpr int EPI_PITCH = 36;
 template <class Cfg>
-__device__ __forceinline__ void grouped_store(const GroupedArgs& g, const GroupedProblem& pr, int row0,
+__device__ __forceinline__ void grouped_store(const GroupedArgs& g, const GroupedProblem& pr, int base, int ew,
                                               int col0, const uint32_t (&v)[32], uint32_t (*stg)[EPI_PITCH],
                                               int lane) {
 #pragma unroll
@@ -69,7 +82,9 @@ __device__ __forceinline__ void grouped_store(const GroupedArgs& g, const Groupe
         *reinterpret_cast<uint4*>(&stg[lane][4 * q]) = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
     __syncwarp();
     const int col = col0 + lane;
-    const int rows = min(32, pr.M - row0);
+    // row r of the staged block is tile row spread_row(ew, r) = 8 ew + rel(r)
+    const int lim = pr.M - base - 8 * ew;  // rel(r) < lim: the row exists
+#define FG_REL(r) (32 * ((r) >> 3) + ((r) & 7))
     if (col < pr.N) {
         // unrolled with predicates: all shared-memory reads (and the reads
         // of C for accumulate / beta) are issued before the first store, so
@@ -79,30 +94,31 @@ __device__ __forceinline__ void grouped_store(const GroupedArgs& g, const Groupe
         for (int r = 0; r < 32; ++r) w[r] = stg[r][lane];
         const long long ldc = pr.ldc;
         if constexpr (Cfg::EPI == EPI_I32) {
-            int32_t* p = static_cast<int32_t*>(pr.C) + (long long)row0 * ldc + col;
+            int32_t* p = static_cast<int32_t*>(pr.C) + (long long)(base + 8 * ew) * ldc + col;
             if (g.accumulate) {
 #pragma unroll
                 for (int r = 0; r < 32; ++r)
-                    if (r < rows) w[r] += static_cast<uint32_t>(p[r * ldc]);
+                    if (FG_REL(r) < lim) w[r] += static_cast<uint32_t>(p[FG_REL(r) * ldc]);
             }
 #pragma unroll
             for (int r = 0; r < 32; ++r)
-                if (r < rows) p[r * ldc] = static_cast<int32_t>(w[r]);
+                if (FG_REL(r) < lim) p[FG_REL(r) * ldc] = static_cast<int32_t>(w[r]);
         } else {
-            float* p = static_cast<float*>(pr.C) + (long long)row0 * ldc + col;
+            float* p = static_cast<float*>(pr.C) + (long long)(base + 8 * ew) * ldc + col;
             float o[32];
 #pragma unroll
             for (int r = 0; r < 32; ++r) o[r] = g.alpha * __uint_as_float(w[r]);
             if (g.beta != 0.f) {
 #pragma unroll
                 for (int r = 0; r < 32; ++r)
-                    if (r < rows) o[r] = fmaf(g.beta, p[r * ldc], o[r]);
+                    if (FG_REL(r) < lim) o[r] = fmaf(g.beta, p[FG_REL(r) * ldc], o[r]);
             }
 #pragma unroll
             for (int r = 0; r < 32; ++r)
-                if (r < rows) p[r * ldc] = o[r];
+                if (FG_REL(r) < lim) p[FG_REL(r) * ldc] = o[r];
         }
     }
+#undef FG_REL
     __syncwarp();
 }
 
@@ -191,8 +207,13 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
                     }
                     mbar_arrive_expect_tx(&s.full[stage], Cfg::STAGE_BYTES);
                     const int kx = kb * Cfg::BK;
+                    // A as sixteen 8-row boxes, spread over the accumulator's
+                    // lane quadrants (spread_row)
                     for (int i = 0; i < Cfg::NA; ++i)
-                        tma_load_2d(s.a[stage][i], mp + i, kx, tm * Cfg::BM, &s.full[stage]);
+#pragma unroll
+                        for (int bx = 0; bx < Cfg::BM / 8; ++bx)
+                            tma_load_2d(s.a[stage][i] + (32 * (bx & 3) + 8 * (bx >> 2)) * Cfg::BK_BYTES, mp + i, kx,
+                                        tm * Cfg::BM + 8 * bx, &s.full[stage]);
                     for (int i = 0; i < Cfg::NB; ++i) {
 #pragma unroll
                         for (int c = 0; c < Cfg::B_CHUNKS; ++c)
@@ -325,7 +346,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
 #pragma unroll
                 for (int j = 0; j < Cfg::BN; ++j) run[j] = 0.f;
             }
-            const int row0 = tm * Cfg::BM + ew * 32;
+            const int base = tm * Cfg::BM;  // this warp's rows: base + spread_row(ew, lane)
             for (int kc0 = 0; kc0 < kblocks; kc0 += kchunk, ++it) {
                 const int buf = it % Cfg::ACC_BUFS;
                 const uint32_t acc_par = static_cast<uint32_t>((it / Cfg::ACC_BUFS) & 1);
@@ -346,7 +367,7 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
                     }
                 } else {
                     // chunks past the problem's last row / column hold nothing
-                    const int nch = row0 < pr.M ? min(Cfg::BN / 32, (pr.N - tn * Cfg::BN + 31) / 32) : 0;
+                    const int nch = base + 8 * ew < pr.M ? min(Cfg::BN / 32, (pr.N - tn * Cfg::BN + 31) / 32) : 0;
                     // two chunks in flight: chunk c + 1 is read out of TMEM
                     // while chunk c goes to memory
                     uint32_t va[32], vb[32];
@@ -355,11 +376,11 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
                     for (int c = 0; c < nch; c += 2) {
                         tmem_wait_ld();
                         if (c + 1 < nch) tmem_ld_32x32b_x32(row_addr + (c + 1) * 32, vb);
-                        grouped_store<Cfg>(g, pr, row0, tn * Cfg::BN + c * 32, va, stg, lane);
+                        grouped_store<Cfg>(g, pr, base, ew, tn * Cfg::BN + c * 32, va, stg, lane);
                         if (c + 1 < nch) {
                             tmem_wait_ld();
                             if (c + 2 < nch) tmem_ld_32x32b_x32(row_addr + (c + 2) * 32, va);
-                            grouped_store<Cfg>(g, pr, row0, tn * Cfg::BN + (c + 1) * 32, vb, stg, lane);
+                            grouped_store<Cfg>(g, pr, base, ew, tn * Cfg::BN + (c + 1) * 32, vb, stg, lane);
                         }
                     }
                 }
@@ -374,7 +395,8 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
                     uint32_t v[32];
 #pragma unroll
                     for (int j = 0; j < 32; ++j) v[j] = __float_as_uint(run[c * 32 + j]);
-                    grouped_store<Cfg>(g, pr, row0, tn * Cfg::BN + c * 32, v, stg, lane);
+                    if (base + 8 * ew < pr.M)
+                        grouped_store<Cfg>(g, pr, base, ew, tn * Cfg::BN + c * 32, v, stg, lane);
                 }
             }
         }
