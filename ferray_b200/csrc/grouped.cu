@@ -256,11 +256,11 @@ fg_status grouped_job_bind(GroupedJob* j, void* dev_base, void* host_stage) {
             const void* pb = q.b;
             if (oa.off0 >= 0) {
                 pa = d_arena + oa.off0;
-                hsegs[si++] = PrepSeg{q.a, const_cast<void*>(pa), nullptr, q.m, q.k, q.lda, oa.ld, 0, 0};
+                hsegs[si++] = PrepSeg{q.a, const_cast<void*>(pa), nullptr, q.m, q.k, q.lda, oa.ld, 0};
             }
             if (ob.off0 >= 0) {
                 pb = d_arena + ob.off0;
-                hsegs[si++] = PrepSeg{q.b, const_cast<void*>(pb), nullptr, q.k, q.n, q.ldb, ob.ld, 0, 0};
+                hsegs[si++] = PrepSeg{q.b, const_cast<void*>(pb), nullptr, q.k, q.n, q.ldb, ob.ld, 0};
             }
             uint64_t da[2] = {(uint64_t)q.k, (uint64_t)q.m}, sa[1] = {(uint64_t)oa.ld};
             uint64_t db[2] = {(uint64_t)q.n, (uint64_t)q.k}, sb[1] = {(uint64_t)ob.ld};
@@ -274,8 +274,8 @@ fg_status grouped_job_bind(GroupedJob* j, void* dev_base, void* host_stage) {
             void* al = d_arena + oa.off1;
             void* bh = d_arena + ob.off0;
             void* bl = d_arena + ob.off1;
-            hsegs[si++] = PrepSeg{q.a, ah, al, q.m, q.k, q.lda, oa.ld, 0, 1};
-            hsegs[si++] = PrepSeg{q.b, bh, bl, q.k, q.n, q.ldb, ob.ld, 0, 1};
+            hsegs[si++] = PrepSeg{q.a, ah, al, q.m, q.k, q.lda, oa.ld, 1};
+            hsegs[si++] = PrepSeg{q.b, bh, bl, q.k, q.n, q.ldb, ob.ld, 1};
             uint64_t da[2] = {(uint64_t)q.k, (uint64_t)q.m}, sa[1] = {(uint64_t)(2 * oa.ld)};
             uint64_t db[2] = {(uint64_t)q.n, (uint64_t)q.k}, sb[1] = {(uint64_t)(2 * ob.ld)};
             uint32_t boxa[2] = {64, 8}, boxb[2] = {64, 64};  // A in 8-row boxes (row spreading)

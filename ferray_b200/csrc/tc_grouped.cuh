@@ -420,23 +420,19 @@ __global__ void __launch_bounds__(Cfg::THREADS, 1)
 // them (a granule is read only when it holds a byte of the row, so every
 // read stays on memory the row occupies) and shifted into place in
 // registers, so each thread issues one to three 16-byte loads per 16-byte
-// output chunk, prep_ilp() chunks per thread per pass with every load
-// issued before the first store.
+// output chunk, PREP_ILP chunks per thread per pass with every load issued
+// before the first store.
 struct PrepSeg {
     const void* src;
     void* dst0;
     void* dst1;
     long long rows, cols, ld_src, ld_dst;  // elements
-    long long start;                       // unused (kept for the table layout)
     int op;
 };
 
 // output chunks per thread per pass (loads issued first): one for both ops
 // -- two halved the blocks per SM (registers) and were measured slower
-template <int OP>
-constexpr int prep_ilp() {
-    return 1;
-}
+constexpr int PREP_ILP = 1;
 
 // op 0: 16 bytes of a row starting at byte address p, `valid` of them in
 // the row (valid <= 0: none).
@@ -528,7 +524,6 @@ constexpr long long PREP_JOB_CHUNKS = 4096;
 template <int OP>
 static __global__ void __launch_bounds__(256) grouped_prep_kernel(const PrepSeg* __restrict__ segs,
                                                                   const PrepJob* __restrict__ jobs, int njobs) {
-    constexpr int PREP_ILP = prep_ilp<OP>();
     // One block per job (grid-stride over jobs).  The block's threads take
     // the job's 16-byte destination chunks (destination pitch is a multiple
     // of 16 bytes) in row-major order, PREP_ILP per thread per pass with all
