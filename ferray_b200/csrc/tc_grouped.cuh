@@ -9,12 +9,16 @@
 // on a counter (zeroed before every launch), so CTAs that drew short tiles
 // come back for more and the heavy tiles go first (dynamic
 // longest-processing-time order).  The producer passes each claimed tile
-// index to the CTA's MMA and epilogue roles through a small ring of
+// record to the CTA's MMA and epilogue roles through a small ring of
 // shared-memory slots guarded by mbarriers, so all three roles of
 // tc_gemm.cuh (TMA producer, MMA issuer, epilogue) walk the same sequence;
-// a tile index past the end tells them to stop.  The producer claims one
-// tile ahead and prefetches that tile's tensor maps while the current one
-// loads.
+// a record past the end tells them to stop.  The producer claims two tiles
+// ahead and prefetches the next tile's tensor maps while the current one
+// loads.  Operands TMA cannot read as they are (i8 rows that break its
+// 16-byte rule, the split form's f32 operands) are rewritten once by
+// grouped_prep_kernel into an arena before the launch.  A is loaded as
+// 8-row boxes spread over the accumulator's lane quadrants (spread_row), so
+// short tiles keep all four epilogue warps busy.
 #pragma once
 #include "tc_gemm.cuh"
 

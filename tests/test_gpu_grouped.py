@@ -97,7 +97,7 @@ def _placed(rng, dims, esize, aligned_every=4):
     """Operand placements inside one device buffer: per problem a byte offset
     and leading dimensions.  Every `aligned_every`-th problem gets 16-byte
     offsets and leading dimensions (TMA reads it); the others get odd offsets
-    and padded leading dimensions (the loader warps read them)."""
+    and padded leading dimensions (the prep pass re-pitches those)."""
     out, cur = [], 0
     for i, (m, n, k) in enumerate(dims):
         if i % aligned_every == 0:
@@ -117,7 +117,7 @@ def _placed(rng, dims, esize, aligned_every=4):
 @pytest.mark.parametrize("dtype", [np.int8, np.uint8])
 def test_grouped_i8_offsets_and_padding(fg, dtype):
     """i8 / u8 x i8 problems at unaligned offsets with padded leading
-    dimensions (loader warps), mixed in one launch with 16-byte-aligned ones
+    dimensions (re-pitched by the prep pass), mixed in one launch with 16-byte-aligned ones
     (TMA), padded output rows too: bit-exact against int64 products."""
     rng = np.random.default_rng(21)
     dims = ragged_dims(rng, 40, 1, 300)
@@ -151,8 +151,8 @@ def test_grouped_i8_offsets_and_padding(fg, dtype):
 def test_grouped_split_offsets_and_padding(fg, oracle):
     """Split-f32 problems whose operands sit at 4-byte (not 16-byte) offsets
     with padded leading dimensions: within tolerance of the DD oracle, and
-    bit-identical to the same problems from contiguous buffers (the loader
-    warps read both, so placement must not change a bit)."""
+    bit-identical to the same problems from contiguous buffers (the split
+    pass reads both, so placement must not change a bit)."""
     rng = np.random.default_rng(22)
     dims = ragged_dims(rng, 24, 1, 300)
     dims = np.vstack([dims, [[1, 1, 1], [130, 3, 260], [5, 129, 17]]])
