@@ -184,3 +184,34 @@ def test_grouped_split_offsets_and_padding(fg, oracle):
         assert np.array_equal(got.view(np.uint32), dc2.to_numpy().view(np.uint32)), (m, n, k)
         err = oracle.error_vs_dd(a, b, got)
         assert err <= 2.0 ** -15 + k * U32, (m, n, k, err)
+
+
+@pytest.mark.parametrize("dtype,mode", [(np.int8, "plain"), (np.float32, "split")])
+def test_grouped_row_spread_boundaries(fg, oracle, dtype, mode):
+    """Tile heights at every boundary of the kernels' row spreading (A rows
+    loaded as 8-row boxes spread over the four accumulator lane quadrants,
+    each epilogue warp storing rows 8 w + 32 j + r): M around 8, 32, 64, 96,
+    128 and past one tile, with ragged N and K.  i8 exact; split f32 within
+    the DD tolerance; rows of C outside the product are left alone."""
+    rng = np.random.default_rng(23)
+    ms = [1, 7, 8, 9, 31, 32, 33, 63, 64, 65, 96, 97, 127, 128, 129, 255, 257]
+    dims = np.array([[m, int(rng.integers(1, 200)), int(rng.integers(1, 300))] for m in ms])
+    probs, host = make_problems(fg, rng, dims, dtype)
+    # C one row taller than the product, guard row filled: the extra row must survive
+    guarded = []
+    for (m, n, k, da, db, dc) in probs:
+        fill = np.full((m + 1, n), -9 if dtype == np.int8 else np.float32(-9.5),
+                       np.int32 if dtype == np.int8 else np.float32)
+        g = fg.DeviceArray.from_numpy(fill)
+        guarded.append((m, n, k, da, db, g))
+    fg.gemm_grouped(guarded, dtype=dtype, mode=mode)
+    for (m, n, k, da, db, g), (a, b) in zip(guarded, host):
+        got = g.to_numpy()
+        assert np.all(got[m] == (-9 if dtype == np.int8 else np.float32(-9.5))), (m, n, k)
+        got = got[:m]
+        if dtype == np.int8:
+            want = (a.astype(np.int64) @ b.astype(np.int64)).astype(np.int32)
+            np.testing.assert_array_equal(got, want)
+        else:
+            err = oracle.error_vs_dd(a, b, got)
+            assert err <= 2.0 ** -15 + k * U32, (m, n, k, err)
