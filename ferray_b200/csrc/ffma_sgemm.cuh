@@ -7,10 +7,10 @@
 // A is first transposed into a packed K x Mp scratch (Mp = M rounded up to
 // 4, zero padded), so both operand tiles are rows of 16-byte chunks that
 // `cp.async.cg` copies global -> shared without passing through registers,
-// in a 4-stage ring of BK = 16 (one __syncthreads per K block).  The freed
-// registers and the deeper ring keep the FFMA pipe fed (in a standalone
-// B200 timing of the same kernel: 53 TFLOP/s at 8192^3 against 36.8 for the
-// register-staged kernel).
+// in a 3-stage ring of BK = 32 (one __syncthreads per K block; 101 KB, two
+// CTAs per SM).  The freed registers and the ring keep the FFMA pipe fed
+// (B200, 8192^3: 52.9 TFLOP/s, against 52.0 for a 4-stage ring of BK = 16
+// on the same box and 36.8 for the register-staged kernel).
 // B is read in place when it is 16-byte aligned with ldb and N multiples of
 // 4, otherwise from a packed copy (pitch Np = N rounded up to 4).
 #pragma once
@@ -22,7 +22,7 @@
 namespace fg {
 
 struct FfmaCfg {
-    static constexpr int BM = 128, BN = 128, BK = 16, STAGES = 4, THREADS = 256, PAD = 4;
+    static constexpr int BM = 128, BN = 128, BK = 32, STAGES = 3, THREADS = 256, PAD = 4;
     static constexpr int AS = BK * (BM + PAD), BS = BK * (BN + PAD);  // floats per stage
     static constexpr size_t SMEM = size_t(STAGES) * (AS + BS) * sizeof(float);
 };
