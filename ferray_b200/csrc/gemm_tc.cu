@@ -72,8 +72,10 @@ static unsigned long long kTimeoutNs = 4000000000ull;  // 4 s per wait
 
 // Row tiles per raster group of the persistent tile walk: FG_RASTER when
 // set, else 16 for the plain i8 CTA-pair kernel and 8 for the rest (B200,
-// 8192^3, same box: i8 3.10-3.12 POPS at 16 against 3.00-3.03 at 8; the
-// 3xBF16 pair kernel 479 TFLOP/s at 8 against 435-469 at 16).
+// 8192^3, same box: i8 3.10-3.16 POPS at 16 against 3.00-3.05 at 8; the
+// 3xBF16 pair kernel 479 TFLOP/s at 8 against 435-469 at 16, bf16 x bf16
+// 1193 against 1130; the scheme II products and the quantized GEMM within
+// noise of each other).
 static int raster_env() {
     static int v = [] {
         const char* e = getenv("FG_RASTER");
