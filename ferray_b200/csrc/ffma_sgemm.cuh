@@ -194,7 +194,7 @@ static __global__ void __launch_bounds__(FfmaCfg::THREADS, 2)
 // kernels at equal split-K.  With few rows the work per B element is small,
 // so the host splits K to fill the GPU.
 struct FfmaSkinnyCfg {
-    static constexpr int BM = 32, BN = 256, BK = 16, STAGES = 4, THREADS = 256, PAD = 4;
+    static constexpr int BM = 32, BN = 256, BK = 32, STAGES = 3, THREADS = 256, PAD = 4;
     static constexpr int AS = BK * (BM + PAD), BS = BK * (BN + PAD);
     static constexpr size_t SMEM = size_t(STAGES) * (AS + BS) * sizeof(float);
 };
@@ -221,7 +221,8 @@ static __global__ void __launch_bounds__(FfmaSkinnyCfg::THREADS, 2)
     const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     const int kblocks = (K + BK - 1) / BK;
-    constexpr int A_CH = BK * BM / 4;                  // 128 chunks: threads 0..127 take one
+    constexpr int A_CH = BK * BM / 4;                  // 256 chunks: every thread takes one
+    static_assert(A_CH <= Cfg::THREADS, "one A chunk per thread at most");
     constexpr int B_CH = BK * BN / 4 / Cfg::THREADS;   // 4 chunks a thread
 
     auto load = [&](int stage, int kb) {
